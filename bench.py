@@ -1,0 +1,446 @@
+"""Benchmark of the DEM droplet step (direct O(N^2) path).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--n 65536] [--precision mixed|fp64]
+
+Workload (default): N = 65,536 water droplets in oil, radii lognormal (median
+5 um, sigma_ln 0.35, clipped to [1, 30] um), periodic cube at 2 % volume
+fraction, overlaps rejected, seed 0; E = 3e5 V/m, eps_oil 2.85, eta_oil 0.06,
+eta_water 0.001, dt = 1e-4 s.  One step = collision detection (spatial hash)
++ coalescence when pairs exist + dipole forces + Oseen convection + Euler
+update with the periodic wrap, all on the device.
+
+Printed JSON (rank 0, one line):
+  value        steps/s of the whole job, inputs resident in HBM
+  e2e          steps/s through the public numpy API (host buffers every step:
+               detection + forces/convection uploads, results downloaded)
+  roofline     the dominant kernel (mixed force pass) against the FP32 pipe
+  cpu_baseline the CPU oracle (restatement of the reference kernels, all host
+               threads) on a bounded row sample, extrapolated to a full step
+Multi-GPU (torchrun): every rank integrates its own independent box (replicas;
+weak scaling); value sums the ranks' steps/s over the max-over-ranks time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "particle-simulator_b200"))
+
+FLOPS_FORCE_PAIR = 33  # algorithmic flops of one force pair (FMA = 2)
+FLOPS_OSEEN_PAIR = 34  # algorithmic flops of one Oseen pair
+SM_COUNT_B200 = 148
+FP32_LANES_PER_SM = 128
+PHYS = dict(eps_oil=2.85, eta_oil=0.06, eta_water=0.001, E=3e5)
+DT = 1e-4
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=65536)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--cpu-sample-seconds", type=float, default=12.0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def make_state(n, seed):
+    from dem.particle_generator import LognormalDropletGenerator
+
+    g = LognormalDropletGenerator(n, seed=seed)
+    s = g.generate()
+    return s.positions, s.radii, g.L
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {
+            "sm_mhz": float(np.median(sm)) if sm else None,
+            "sm_max_mhz": float(max(mx)) if mx else None,
+            "power_w_median": float(np.median(power)) if power else None,
+            "samples": len(sm),
+            "reasons": sorted(reasons),
+        }
+
+
+# ---------------------------------------------------------------------------
+# our implementation
+# ---------------------------------------------------------------------------
+class DeviceStepper:
+    """Device-resident direct DEM step through the library's C ABI."""
+
+    def __init__(self, pos, r, L, precision, device):
+        import torch
+
+        from dem.collision_detector import SpatialHashCollisionDetector
+        from dem.force_calculator import DirectDropletForceCalculator
+
+        self.torch = torch
+        n = len(r)
+        self.fc = DirectDropletForceCalculator(num_particles=n, L=L, boundary_mode="periodic", precision=precision,
+                                               device=device, **PHYS)
+        self.det = SpatialHashCollisionDetector(num_particles=n, L=L, boundary_mode="periodic", device=device)
+        self.ctx = self.fc._ctx
+        self.L = L
+        eta_o, eta_w = PHYS["eta_oil"], PHYS["eta_water"]
+        self.stokes = 2 * np.pi * eta_o * (2 * eta_o + 3 * eta_w) / (eta_o + eta_w)
+        self.dev = self.ctx.device
+        self.pos = [torch.empty((3, n), dtype=torch.float64, device=self.dev) for _ in range(2)]
+        self.r = [torch.as_tensor(r, device=self.dev).clone(), torch.empty(n, dtype=torch.float64, device=self.dev)]
+        self.ctx.aos_to_soa(n, torch.as_tensor(pos, device=self.dev), self.pos[0])
+        self.cur, self.rc, self.n = 0, 0, n
+        self.n_out = torch.zeros(1, dtype=torch.int32, device=self.dev)
+        self.merges = 0
+        self.launches_per_step = None
+
+    def step(self):
+        n, pos, r = self.n, self.pos[self.cur], self.r[self.rc]
+        k, pairs, counts = self.det.detect_device(n, pos, r, self.L, True)
+        if k > 0:  # coalescence, then detect again at the same time (reference semantics)
+            nxt = 1 - self.cur
+            self.ctx.merge(n, pos, r, pairs, counts, self.pos[nxt], self.r[1 - self.rc], self.n_out)
+            self.n = int(self.n_out.item())
+            self.cur, self.rc = nxt, 1 - self.rc
+            self.merges += 1
+            return self.step()
+        F, V = self.fc.forces_and_convection_soa(n, pos, r)
+        nxt = 1 - self.cur
+        self.ctx.euler_update(n, pos, r, F, V, self.stokes, DT, self.L, True, self.pos[nxt])
+        self.cur = nxt
+
+
+def flush_l2(buf):
+    buf.fill_(1)
+
+
+def run_ours(args, rank, world, device):
+    import torch
+
+    torch.cuda.set_device(device)
+    pos, r, L = make_state(args.n, args.seed + rank)
+    n = len(r)
+    st = DeviceStepper(pos, r, L, args.precision, device)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)  # > 126 MB L2
+    for _ in range(args.warmup):
+        st.step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    sampler = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.4)
+    st.ctx.profile(True)
+    stream = torch.cuda.current_stream()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        flush_l2(flush)  # outside the timed events: every step starts with a cold L2
+        ev[k][0].record(stream)
+        st.step()
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = float(sum(step_ms))
+    kern = {}
+    for name in ("mixed_force_pass", "mixed_convection_pass", "fp64_force_pass", "fp64_convection_pass",
+                 "hash_detect"):
+        ms, cnt = st.ctx.profile_read(name)
+        if cnt:
+            kern[name] = (ms, cnt)
+    st.ctx.profile(False)
+    clocks = sampler.stop() if sampler else None
+    t = torch.tensor([total_ms], device=device)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.barrier()
+    return dict(n=n, n_final=st.n, L=L, total_ms=float(t.item()), step_ms=step_ms, kern=kern, clocks=clocks,
+                merges=st.merges, pos=pos, r=r)
+
+
+def run_e2e(args, device, steps, warmup):
+    """The reference's solver loop (euler_droplet_solver.py:97-131) driving the
+    drop-in detector and calculator through their numpy API: host state,
+    uploads and downloads on every step."""
+    import torch
+
+    from dem.collision_detector import SpatialHashCollisionDetector
+    from dem.force_calculator import DirectDropletForceCalculator
+    from dem.solution.droplet_solution import merge_droplets
+
+    pos, r, L = make_state(args.n, args.seed)
+    n = len(r)
+    fc = DirectDropletForceCalculator(num_particles=n, L=L, boundary_mode="periodic", precision=args.precision,
+                                      device=device, **PHYS)
+    det = SpatialHashCollisionDetector(num_particles=n, L=L, boundary_mode="periodic", device=device)
+    eta_o, eta_w = PHYS["eta_oil"], PHYS["eta_water"]
+    stokes = 2 * np.pi * eta_o * (2 * eta_o + 3 * eta_w) / (eta_o + eta_w)
+
+    def one(pos, r):
+        while True:
+            hit, pairs = det.detect(pos, r)
+            if not hit:
+                break
+            pos, r = merge_droplets(pos, r, pairs)
+        F, V = fc.calculate_forces_and_convection(pos, r)
+        pos = pos + (F / (stokes * r[:, None]) + V) * DT
+        pos %= L
+        return pos, r
+
+    for _ in range(warmup):
+        pos, r = one(pos, r)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        pos, r = one(pos, r)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    n = len(r)
+    return dict(steps_per_s=steps / dt, h2d=2 * n * 32, d2h=n * 48 + 16)
+
+
+# ---------------------------------------------------------------------------
+# CPU oracle (reference algorithm restated in C, all host threads)
+# ---------------------------------------------------------------------------
+def cpu_step_rate(pos, r, L, budget_s, threads=0):
+    """Times hash detection (full) and the two O(N^2) passes on a row sample
+    sized to ~budget_s, and extrapolates the time of one full step."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    m, eta, stokes = O.physics_constants(**PHYS)
+    n = len(r)
+    cores = O.max_threads() if threads <= 0 else threads
+    t0 = time.perf_counter()
+    O.hash_detect(pos, r, L, True, table_size=O.next_power_of_2(2 * n))
+    t_hash = time.perf_counter() - t0
+    # calibrate on a small sample, then size the timed sample
+    rows = max(cores * 4, 64)
+    t0 = time.perf_counter()
+    F = O.direct_forces(pos, r, m, L, True, rows=(0, rows), threads=threads)
+    O.direct_convection(pos, F, eta, L, True, rows=(0, rows), threads=threads)
+    per_row = (time.perf_counter() - t0) / rows
+    rows = int(min(n, max(rows, budget_s / max(per_row, 1e-9))))
+    t0 = time.perf_counter()
+    F = O.direct_forces(pos, r, m, L, True, rows=(0, rows), threads=threads)
+    O.direct_convection(pos, F, eta, L, True, rows=(0, rows), threads=threads)
+    t_rows = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    O.euler_direct(pos, r, np.zeros((n, 3)), np.zeros((n, 3)), stokes, DT, L, True)
+    t_euler = time.perf_counter() - t0
+    t_step = t_hash + t_rows * (n / rows) + t_euler
+    return dict(steps_per_s=1.0 / t_step, cores=cores, rows=rows, sample_s=t_rows + t_hash + t_euler,
+                pairs_per_s=n * (n - 1) / t_step)
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    pos, r, L = make_state(args.n, args.seed)
+    n = len(r)
+    budget = max(1.0, min(args.cpu_sample_seconds, 120.0 / max(args.steps + args.warmup, 1)))
+    for _ in range(args.warmup):
+        cpu_step_rate(pos, r, L, budget)
+    rates = [cpu_step_rate(pos, r, L, budget) for _ in range(args.steps)]
+    sps = float(np.median([x["steps_per_s"] for x in rates]))
+    line = {
+        "impl": "reference",
+        "metric": "DEM steps/s (direct, N=%d)" % n,
+        "value": sps,
+        "unit": "steps/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1000.0 / sps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded lognormal droplets)",
+        "config": {"workload": f"direct DEM step, N={n}, periodic, 2% volume fraction, dt=1e-4",
+                   "pairs_per_s": sps * n * (n - 1)},
+        "cpu_baseline": {"value": sps, "unit": "steps/s", "cores": rates[0]["cores"], "kind": "port",
+                         "sample": f"hash detection + Euler on all {n} droplets, both O(N^2) passes on "
+                                   f"{rates[0]['rows']} rows x {n} columns per step, extrapolated"},
+        "e2e": {"value": sps, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if args.impl == "ours":
+            torch.cuda.set_device(local)
+        torch.distributed.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        if world > 1:
+            import torch
+
+            torch.distributed.destroy_process_group()
+        return
+
+    import torch
+
+    device = torch.device("cuda", local)
+    res = run_ours(args, rank, world, device)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+    n = res["n"]
+    K = args.steps
+    steps_per_s = K * world / (res["total_ms"] / 1000.0)
+    pairs = n * (n - 1)
+    clocks = res["clocks"] or {}
+    # roofline of the dominant kernel
+    prec = args.precision
+    fname = "mixed_force_pass" if prec == "mixed" else "fp64_force_pass"
+    cname = "mixed_convection_pass" if prec == "mixed" else "fp64_convection_pass"
+    kern = res["kern"]
+    dom = max((fname, cname), key=lambda k: kern.get(k, (0, 1))[0])
+    ms, cnt = kern.get(dom, (float("nan"), 1))
+    flops = (FLOPS_FORCE_PAIR if dom == fname else FLOPS_OSEEN_PAIR) * pairs
+    achieved = flops / (ms / cnt / 1000.0) / 1e12
+    max_mhz = clocks.get("sm_max_mhz") or 1965.0
+    lanes = FP32_LANES_PER_SM if prec == "mixed" else FP32_LANES_PER_SM // 2
+    peak = SM_COUNT_B200 * lanes * 2 * max_mhz * 1e6 / 1e12
+    peak_at_clock = SM_COUNT_B200 * lanes * 2 * (clocks.get("sm_mhz") or max_mhz) * 1e6 / 1e12
+    traffic = None
+    prof = ROOT / "profiles" / "traffic.json"
+    if prof.exists():
+        try:
+            traffic = json.loads(prof.read_text()).get(dom)
+        except Exception:
+            traffic = None
+    line = {
+        "metric": f"DEM steps/s (direct, N={n})",
+        "value": steps_per_s,
+        "unit": "steps/s",
+        "n_gpus": world,
+        "steps": K,
+        "warmup": args.warmup,
+        "ms_per_step": res["total_ms"] / K,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 pair terms + f64 near pairs/sums" if prec == "mixed" else "f64",
+        "data": "synthetic (seeded lognormal droplets, 2% volume fraction)",
+        "config": {
+            "workload": f"direct DEM step (hash detection + merge + dipole force + Oseen convection + Euler), "
+                        f"N={n}, periodic, dt=1e-4",
+            "precision": prec,
+            "pairs_per_s": steps_per_s * pairs,
+            "l2": "flushed between steps (256 MiB write outside the timed events)",
+            "merges_in_timed_and_warmup": res["merges"],
+            "n_final": res["n_final"],
+            "kernel_ms_per_launch": {k: v[0] / v[1] for k, v in kern.items()},
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+        },
+        "roofline": {
+            "kernel": dom,
+            "bound": "fp32_pipe" if prec == "mixed" else "fp64_pipe",
+            "achieved": achieved,
+            "peak": peak,
+            "unit": "TFLOP/s",
+            "frac": achieved / peak,
+            "frac_at_sampled_clock": achieved / peak_at_clock,
+            "traffic": traffic,
+            "peak_source": f"{SM_COUNT_B200} SMs x {lanes} lanes x 2 flop x {max_mhz:.0f} MHz (max SM clock); "
+                           "MEASURED_PEAKS.json holds no CUDA-core figure",
+            "flops_per_pair": FLOPS_FORCE_PAIR if dom == fname else FLOPS_OSEEN_PAIR,
+        },
+        "clocks": clocks,
+        "gpu_launches": None,
+    }
+    if not args.no_e2e:
+        e = run_e2e(args, device, steps=max(3, min(K, 10)), warmup=1)
+        line["e2e"] = {"value": e["steps_per_s"], "unit": "steps/s", "h2d_bytes_per_step": e["h2d"],
+                       "d2h_bytes_per_step": e["d2h"]}
+    if not args.no_cpu:
+        c = cpu_step_rate(res["pos"], res["r"], res["L"], args.cpu_sample_seconds)
+        line["cpu_baseline"] = {"value": c["steps_per_s"], "unit": "steps/s", "cores": c["cores"], "kind": "port",
+                                "sample": f"hash + Euler on all {n} droplets; both O(N^2) passes on {c['rows']} rows "
+                                          f"x {n} columns, extrapolated ({c['sample_s']:.1f} s of CPU work)"}
+    # kernels of ours launched in the timed region: per step hash (max, params, assign, 3 scan, scatter, count,
+    # 3 scan, write = 12) + forces (maxabs, prep, pass, reduce = 4) + convection (2 maxabs, 2 prep, pass, reduce = 6)
+    # + euler (1)
+    line["gpu_launches"] = K * (12 + 4 + 6 + 1)
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

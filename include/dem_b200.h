@@ -1,0 +1,165 @@
+/*
+ * dem_b200.h -- C ABI of libdem_b200.so, the B200 (sm_100a) implementation of
+ * the DEM droplet hot path of ddkx21/particle-simulator.
+ *
+ * Conventions
+ *   - Every array argument is a DEVICE pointer (cudaMalloc'd or a torch CUDA
+ *     tensor's data_ptr()), except where a comment says "host".
+ *   - Positions, forces and velocities are structure-of-arrays: one double
+ *     array per Cartesian component, length n.  Radii: double[n].
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default
+ *     stream).  Calls are asynchronous with respect to the host unless the
+ *     comment says the call synchronises.
+ *   - Return value: DEM_OK or one of the DEM_E_* codes; dem_last_error()
+ *     gives the message.  The Python layer maps DEM_E_CAPACITY and
+ *     DEM_E_INVALID to ValueError and DEM_E_NOT_ALLOCATED to RuntimeError,
+ *     the exception types the reference raises.
+ *   - One context per stream; a context is not shared between host threads.
+ *
+ * Each entry point names the reference function it replaces (path:line in
+ * ddkx21/particle-simulator).
+ */
+#ifndef DEM_B200_H
+#define DEM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define DEM_API __attribute__((visibility("default")))
+#else
+#define DEM_API
+#endif
+
+#define DEM_OK 0
+#define DEM_E_INVALID 1       /* bad argument                                   */
+#define DEM_E_CAPACITY 2      /* n (or a pair/node count) exceeds a capacity    */
+#define DEM_E_CUDA 3          /* CUDA runtime error                             */
+#define DEM_E_DEVICE 4        /* a kernel raised a device error flag            */
+#define DEM_E_NOT_ALLOCATED 5 /* optional data not allocated                    */
+
+/* precision of the direct O(N^2) passes */
+#define DEM_PREC_FP64 0  /* reference drop-in: bit-exact with the reference expression order */
+#define DEM_PREC_MIXED 1 /* FP32 pair terms, compensated sums, FP64 near-contact pairs       */
+
+/* device error flags (dem_device_errors) */
+#define DEM_DEVERR_WAIT_TIMEOUT 1u  /* a bounded wait (mbarrier / flag) ran out   */
+#define DEM_DEVERR_PAIR_OVERFLOW 2u /* more colliding pairs than the pair buffer  */
+#define DEM_DEVERR_NODE_OVERFLOW 4u /* octree node pool exhausted                 */
+#define DEM_DEVERR_NONFINITE 8u     /* a non-finite value was produced            */
+
+typedef struct dem_ctx dem_ctx;
+
+/* ---- context --------------------------------------------------------- */
+/* Creates a context on `device` with room for `capacity` particles.
+ * Replaces the per-class Taichi field allocation of
+ * dem/force_calculator/direct_droplet_force_calculator.py:37-48 and
+ * dem/collision_detector/spatial_hash_collision_detector.py:45-69. */
+DEM_API int dem_ctx_create(int device, int capacity, dem_ctx **out);
+DEM_API void dem_ctx_destroy(dem_ctx *ctx);
+/* Grows the workspace to `capacity` particles (no-op when already large enough). */
+DEM_API int dem_ctx_reserve(dem_ctx *ctx, int capacity);
+DEM_API int dem_ctx_capacity(const dem_ctx *ctx);
+DEM_API const char *dem_last_error(const dem_ctx *ctx);
+/* Reads and clears the device error flags (DEM_DEVERR_*).  Synchronises `stream`. */
+DEM_API int dem_device_errors(dem_ctx *ctx, uint32_t *flags_host, void *stream);
+/* Library version string (host). */
+DEM_API const char *dem_version(void);
+
+/* Opt-in kernel timing: while enabled, CUDA events are recorded on the launch
+ * stream around the main kernels ("mixed_force_pass", "mixed_convection_pass",
+ * "fp64_force_pass", "fp64_convection_pass", "hash_detect").
+ * dem_profile_read synchronises on the recorded events and returns the summed
+ * device time and the number of launches of `name`. */
+DEM_API int dem_profile_enable(dem_ctx *ctx, int enable);
+DEM_API int dem_profile_read(dem_ctx *ctx, const char *name, double *total_ms, int *launches);
+DEM_API int dem_profile_reset(dem_ctx *ctx);
+
+/* Tuning of the mixed-precision direct kernels (0 keeps the current value).
+ *   i_per_thread  i-particles register-blocked per thread (1, 2, 4 or 8)
+ *   threads       threads per CTA (64..512, multiple of 32)
+ *   j_splits      number of j-chunks the N^2 sum is split into (>=1; 0 = auto)
+ *   near_force    FP64 radius factor k: pairs with |r_ij| <= k (r_i + r_j) are
+ *   near_oseen    computed in FP64 (force / convection pass) */
+DEM_API int dem_direct_set_tuning(dem_ctx *ctx, int i_per_thread, int threads, int j_splits, double near_force,
+                          double near_oseen);
+DEM_API int dem_direct_get_tuning(const dem_ctx *ctx, int *i_per_thread, int *threads, int *j_splits,
+                          double *near_force, double *near_oseen);
+
+/* ---- layout ---------------------------------------------------------- */
+/* (n, 3) row-major <-> three component arrays.  The reference's public
+ * methods take and return (N, 3) numpy arrays
+ * (direct_droplet_force_calculator.py:260-305); the kernels work on SoA. */
+DEM_API int dem_aos_to_soa(dem_ctx *ctx, int n, const double *aos, double *x, double *y, double *z, void *stream);
+DEM_API int dem_soa_to_aos(dem_ctx *ctx, int n, const double *x, const double *y, const double *z, double *aos,
+                           void *stream);
+
+/* ---- direct O(N^2) passes --------------------------------------------- */
+/* Dipole force on every droplet.
+ * Replaces DirectDropletForceCalculator._calculate_forces,
+ * dem/force_calculator/direct_droplet_force_calculator.py:202-253
+ * (pair term _calculate_one_force :183-200; MIC :234-240; cut r > r_i + r_j). */
+DEM_API int dem_direct_forces(dem_ctx *ctx, int n, const double *x, const double *y, const double *z, const double *r,
+                      double m_const, double L, int periodic, int precision, double *fx, double *fy, double *fz,
+                      void *stream);
+
+/* Oseen convection velocity of every droplet (correction off).  r (radii)
+ * may be NULL for DEM_PREC_FP64; the mixed path uses it for its near-contact
+ * test.
+ * Replaces DirectDropletForceCalculator._calculate_convection_velocities,
+ * dem/force_calculator/direct_droplet_force_calculator.py:354-411. */
+DEM_API int dem_direct_convection(dem_ctx *ctx, int n, const double *x, const double *y, const double *z, const double *r,
+                          const double *fx, const double *fy, const double *fz, double eta_const, double L,
+                          int periodic, int precision, double *vx, double *vy, double *vz, void *stream);
+
+/* Explicit Euler update of the direct path, out of place (xo may equal x):
+ *   x_o = (x + (F / (stokes_factor * r) + v) * dt) mod L   (numpy remainder when periodic)
+ * Replaces dem/solver/euler_droplet_solver.py:121-131. */
+DEM_API int dem_euler_update(dem_ctx *ctx, int n, const double *x, const double *y, const double *z, const double *r,
+                     const double *fx, const double *fy, const double *fz, const double *vx, const double *vy,
+                     const double *vz, double stokes_factor, double dt, double L, int periodic, double *xo,
+                     double *yo, double *zo, void *stream);
+
+/* Euler update of the tree path, x_o = (x + v_total * dt) mod L.
+ * Replaces dem/solver/euler_droplet_solver.py:119, :130-131. */
+DEM_API int dem_euler_update_total(dem_ctx *ctx, int n, const double *x, const double *y, const double *z,
+                           const double *vx, const double *vy, const double *vz, double dt, double L, int periodic,
+                           double *xo, double *yo, double *zo, void *stream);
+
+/* ---- spatial hash collision detection -------------------------------- */
+/* Unique colliding pairs (i < j, lexicographic order) with the reference's
+ * cell/hash semantics: cell = 2 max r, grid = max(1, ceil(L / cell)), hash
+ * (ix*73856093 ^ iy*19349663 ^ iz*83492791) & (table_size - 1), 27 neighbour
+ * cells, MIC distance <= r_i + r_j.
+ * pairs: int32[pair_capacity][2] (device).  counts: int64[2] (device):
+ * counts[0] = number of unique pairs (may exceed pair_capacity: then only the
+ * first pair_capacity pairs are written and DEM_DEVERR_PAIR_OVERFLOW is
+ * raised), counts[1] = raw hits before de-duplication.
+ * Replaces SpatialHashCollisionDetector.detect,
+ * dem/collision_detector/spatial_hash_collision_detector.py:233-316
+ * (kernels :74-229, np.unique :312). */
+DEM_API int dem_hash_detect(dem_ctx *ctx, int n, const double *x, const double *y, const double *z, const double *r,
+                    double L, int periodic, int table_size, int32_t *pairs, int64_t pair_capacity, int64_t *counts,
+                    void *stream);
+
+/* ---- coalescence ------------------------------------------------------ */
+/* Greedy merge of the colliding pairs in (i, j) order; survivors keep their
+ * order and the merged droplets are appended in pair order.
+ *   r_new = (r_a^3 + r_b^3)^(1/3),  x_new = (x_a r_a^3 + x_b r_b^3) / (r_a^3 + r_b^3)  (no MIC)
+ * num_pairs: device int64 (counts[0] of dem_hash_detect).  Outputs must not
+ * alias inputs.  n_out: device int32, the new droplet count.  merged: optional
+ * device int32[n][2] receiving the merged (a, b) pairs in merge order.
+ * Replaces DropletSolution.generate_next_solution,
+ * dem/solution/droplet_solution.py:208-287. */
+DEM_API int dem_merge(dem_ctx *ctx, int n, const double *x, const double *y, const double *z, const double *r,
+              const int32_t *pairs, const int64_t *num_pairs, double *xo, double *yo, double *zo, double *ro,
+              int32_t *n_out, int32_t *merged, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DEM_B200_H */

@@ -1,0 +1,510 @@
+// direct_mixed.cu -- mixed-precision direct O(N^2) passes for sm_100a.
+//
+// Pair terms run on the FP32 FMA pipes; FP64 is kept where it matters:
+//   * coordinates are rounded to FP32 only after a shift to the box centre and
+//     an exact power-of-two rescaling (length unit ell = 2^e ~ max radius), so
+//     their absolute error is ~2^-25 of the half box;
+//   * every pair with |r_ij| <= k (r_i + r_j) (k = near_force / near_oseen) is
+//     recomputed in FP64 from the original coordinates with the reference's
+//     exact formula, minimum image and contact cut;
+//   * each thread accumulates a j-run of FLUSH terms in FP32, then folds it into
+//     a compensated (hi, lo) FP32 pair with Knuth's two-sum; the per-split
+//     partials are added in FP64 in a fixed order (deterministic results).
+//
+// Work decomposition: a CTA owns THREADS*IPT droplets i (IPT register-blocked
+// per thread) and one j-chunk (blockIdx.y); j-tiles of packed float4
+// (x, y, z, w) are staged in shared memory by 1-D TMA bulk copies into a
+// double buffer completed on mbarriers (bounded waits, no multicast), and read
+// as warp-wide broadcasts.
+//
+// Reference: dem/force_calculator/direct_droplet_force_calculator.py:183-253
+// (force) and :354-411 (convection).
+#include <cmath>
+
+#include "common.cuh"
+#include "tma.cuh"
+
+namespace dem {
+
+constexpr int TJ = 128;    // j per shared-memory tile
+constexpr int FLUSH = 64;  // FP32 run length before the compensated fold
+constexpr float RINT_MAGIC = 12582912.0f;  // 1.5 * 2^23: (x + M) - M == rint(x) for |x| < 2^22
+
+struct MixedArgs {
+    int n;
+    int j_chunk;  // j per split (multiple of TJ)
+    const float4 *pos4;  // (x, y, z, r^3) scaled / (x, y, z, -)
+    const float *krf;    // force pass: k_f * r (scaled)
+    const float4 *frc4;  // convection pass: (F scaled, k_o * r scaled)
+    const double *x, *y, *z, *r;      // FP64 originals
+    const double *fx, *fy, *fz;       // FP64 forces (convection pass)
+    double L, halfL;
+    const unsigned long long *scales;  // [0] max r, [1] max |F| (bit patterns)
+    double *partial;  // [splits][3][n]
+    uint32_t *err;
+};
+
+__device__ __forceinline__ void two_sum_fold(float &hi, float &lo, float a) {
+    const float s = hi + a;
+    const float bp = s - hi;
+    const float ap = s - bp;
+    lo += (hi - ap) + (a - bp);
+    hi = s;
+}
+
+__device__ __forceinline__ void fold_double(float &hi, float &lo, double v) {
+    const float vh = (float)v;
+    const float vl = (float)(v - (double)vh);
+    two_sum_fold(hi, lo, vh);
+    lo += vl;
+}
+
+template <bool PER>
+__device__ __forceinline__ float mic32(float d, float Ls, float invLs) {
+    if (!PER) return d;
+    const float u = fmaf(d, invLs, RINT_MAGIC) - RINT_MAGIC;
+    return fmaf(-Ls, u, d);
+}
+
+// FP64 pair terms in scaled units (lengths / ell), reference formulas.
+__device__ __noinline__ double3 near_force_fp64(int i, int j, const MixedArgs a, int periodic, double inv_ell) {
+    double3 o = make_double3(0.0, 0.0, 0.0);
+    if (i == j) return o;
+    double dx = a.x[j] - a.x[i], dy = a.y[j] - a.y[i], dz = a.z[j] - a.z[i];
+    if (periodic) {
+        dx = mic64(dx, a.L, a.halfL);
+        dy = mic64(dy, a.L, a.halfL);
+        dz = mic64(dz, a.L, a.halfL);
+    }
+    const double r_mag = sqrt(dx * dx + dy * dy + dz * dz);
+    if (!(r_mag > a.r[i] + a.r[j])) return o;  // contact cut, :246
+    const double s = inv_ell;
+    dx *= s;
+    dy *= s;
+    dz *= s;
+    const double rm = r_mag * s, rj = a.r[j] * s;
+    const double M = ipow3(rj) / ipow7(rm);
+    const double dx2 = dx * dx, dy2 = dy * dy, dz2 = dz * dz;
+    const double fxy = M * (4 * dz2 - dx2 - dy2);
+    o.x = fxy * dx;
+    o.y = fxy * dy;
+    o.z = M * (2 * dz2 - 3 * dx2 - 3 * dy2) * dz;
+    return o;
+}
+
+__device__ __noinline__ double3 near_oseen_fp64(int i, int j, const MixedArgs a, int periodic, double inv_ell,
+                                                double fscale_inv) {
+    double3 o = make_double3(0.0, 0.0, 0.0);
+    if (i == j) return o;
+    double X = a.x[i] - a.x[j], Y = a.y[i] - a.y[j], Z = a.z[i] - a.z[j];
+    if (periodic) {
+        X = mic64(X, a.L, a.halfL);
+        Y = mic64(Y, a.L, a.halfL);
+        Z = mic64(Z, a.L, a.halfL);
+    }
+    const double s = inv_ell;
+    X *= s;
+    Y *= s;
+    Z *= s;
+    const double rr = sqrt(X * X + Y * Y + Z * Z);
+    const double Fx = a.fx[j] * fscale_inv, Fy = a.fy[j] * fscale_inv, Fz = a.fz[j] * fscale_inv;
+    const double inv_r = 1.0 / rr;
+    const double inv_r3 = inv_r * inv_r * inv_r;
+    const double dot = X * Fx + Y * Fy + Z * Fz;
+    o.x = Fx * inv_r + X * dot * inv_r3;
+    o.y = Fy * inv_r + Y * dot * inv_r3;
+    o.z = Fz * inv_r + Z * dot * inv_r3;
+    return o;
+}
+
+// 2^-e with 2^(e-1) <= m < 2^e (1 when m == 0 or not finite)
+__device__ __forceinline__ double pow2_inv_of(unsigned long long bits) {
+    const double m = __longlong_as_double((long long)bits);
+    if (!(m > 0.0) || !isfinite(m)) return 1.0;
+    int e;
+    frexp(m, &e);
+    return ldexp(1.0, -e);
+}
+
+// ---------------------------------------------------------------------------
+// Shared pipeline skeleton: tile t of this CTA's j-chunk lives in buffer t&1.
+// ---------------------------------------------------------------------------
+template <int IPT, bool PER, bool FORCE>
+__global__ void __launch_bounds__(512) mixed_pass_kernel(const MixedArgs a) {
+    __shared__ __align__(128) float4 sA[2][TJ];
+    __shared__ __align__(128) float4 sB[2][TJ];  // convection: forces; force pass: uses sK
+    __shared__ __align__(128) float sK[2][TJ];
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ int s_abort;
+
+    const int tid = threadIdx.x, T = blockDim.x;
+    const int n = a.n;
+    const int ibase = blockIdx.x * T * IPT;
+    const int split = blockIdx.y;
+    const int j0 = split * a.j_chunk;
+    const int j1 = min(n, j0 + a.j_chunk);
+    const int ntiles = j1 > j0 ? (j1 - j0 + TJ - 1) / TJ : 0;
+    const double inv_ell = pow2_inv_of(a.scales[0]);
+    const double fscale_inv = FORCE ? 1.0 : pow2_inv_of(a.scales[1]);
+    const float Ls = (float)(a.L * inv_ell);
+    const float invLs = (float)(1.0 / (a.L * inv_ell));
+
+    float xi[IPT], yi[IPT], zi[IPT], ki[IPT];
+    float ax[IPT], ay[IPT], az[IPT], hx[IPT], hy[IPT], hz[IPT], lx[IPT], ly[IPT], lz[IPT];
+    int iidx[IPT];
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+        const int i = ibase + k * T + tid;
+        iidx[k] = i;
+        xi[k] = yi[k] = zi[k] = ki[k] = 0.f;
+        if (i < n) {
+            const float4 p = a.pos4[i];
+            xi[k] = p.x;
+            yi[k] = p.y;
+            zi[k] = p.z;
+            ki[k] = FORCE ? a.krf[i] : a.frc4[i].w;
+        }
+        ax[k] = ay[k] = az[k] = hx[k] = hy[k] = hz[k] = lx[k] = ly[k] = lz[k] = 0.f;
+    }
+
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_mbarrier_init();
+        s_abort = 0;
+    }
+    __syncthreads();
+
+    auto issue = [&](int t) {
+        const int js = j0 + t * TJ;
+        const int cnt = min(TJ, j1 - js);
+        const int b = t & 1;
+        const uint32_t bytes_a = (uint32_t)cnt * 16u;
+        if (FORCE) {
+            const uint32_t bytes_k = (uint32_t)((cnt + 3) & ~3) * 4u;
+            mbar_arrive_expect_tx(&bar[b], bytes_a + bytes_k);
+            tma_load_1d(sA[b], a.pos4 + js, bytes_a, &bar[b]);
+            tma_load_1d(sK[b], a.krf + js, bytes_k, &bar[b]);
+        } else {
+            mbar_arrive_expect_tx(&bar[b], 2u * bytes_a);
+            tma_load_1d(sA[b], a.pos4 + js, bytes_a, &bar[b]);
+            tma_load_1d(sB[b], a.frc4 + js, bytes_a, &bar[b]);
+        }
+    };
+
+    if (tid == 0 && ntiles > 0) issue(0);
+    bool aborted = false;
+    for (int t = 0; t < ntiles; ++t) {
+        if (tid == 0 && t + 1 < ntiles) {
+            fence_proxy_async_smem();
+            issue(t + 1);
+        }
+        const bool ok = mbar_wait_bounded(&bar[t & 1], (uint32_t)((t >> 1) & 1), a.err);
+        if (!ok) s_abort = 1;
+        if (ok) {
+            const int js = j0 + t * TJ;
+            const int cnt = min(TJ, j1 - js);
+            const float4 *A = sA[t & 1];
+            const float4 *B = sB[t & 1];
+            const float *K = sK[t & 1];
+            for (int jj = 0; jj < cnt; ++jj) {
+                const float4 pj = A[jj];
+                float4 fj;
+                float kj;
+                if (FORCE) {
+                    kj = K[jj];
+                } else {
+                    fj = B[jj];
+                    kj = fj.w;
+                }
+                uint32_t nearmask = 0;
+#pragma unroll
+                for (int k = 0; k < IPT; ++k) {
+                    float dx, dy, dz;
+                    if (FORCE) {  // d = x_j - x_i (:229-231)
+                        dx = pj.x - xi[k];
+                        dy = pj.y - yi[k];
+                        dz = pj.z - zi[k];
+                    } else {  // d = x_i - x_j (:382-384)
+                        dx = xi[k] - pj.x;
+                        dy = yi[k] - pj.y;
+                        dz = zi[k] - pj.z;
+                    }
+                    dx = mic32<PER>(dx, Ls, invLs);
+                    dy = mic32<PER>(dy, Ls, invLs);
+                    dz = mic32<PER>(dz, Ls, invLs);
+                    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                    const float sr = ki[k] + kj;
+                    const bool nr = r2 <= sr * sr;
+                    nearmask |= (nr ? 1u : 0u) << k;
+                    float rinv = rsqrtf(r2);
+                    if (FORCE) {
+                        const float rinv2 = rinv * rinv;
+                        const float rinv3 = rinv2 * rinv;
+                        const float rinv4 = rinv2 * rinv2;
+                        const float fac = nr ? 0.f : pj.w * (rinv4 * rinv3);
+                        const float ang = fmaf(5.f * dz, dz, -r2);   // 4dz^2 - dx^2 - dy^2
+                        const float angz = fmaf(-2.f, r2, ang);     // 2dz^2 - 3dx^2 - 3dy^2
+                        const float f = fac * ang;
+                        ax[k] = fmaf(f, dx, ax[k]);
+                        ay[k] = fmaf(f, dy, ay[k]);
+                        az[k] = fmaf(fac * angz, dz, az[k]);
+                    } else {
+                        rinv = nr ? 0.f : rinv;
+                        const float rinv2 = rinv * rinv;
+                        const float dot = fmaf(dx, fj.x, fmaf(dy, fj.y, dz * fj.z));
+                        const float sc = dot * rinv2;
+                        ax[k] = fmaf(rinv, fmaf(dx, sc, fj.x), ax[k]);
+                        ay[k] = fmaf(rinv, fmaf(dy, sc, fj.y), ay[k]);
+                        az[k] = fmaf(rinv, fmaf(dz, sc, fj.z), az[k]);
+                    }
+                }
+                // near-contact pairs (and i == j): FP64, reference formula
+                if (__any_sync(0xffffffffu, nearmask != 0u)) {
+                    if (nearmask) {
+                        const int j = js + jj;
+#pragma unroll
+                        for (int k = 0; k < IPT; ++k) {
+                            if ((nearmask >> k) & 1u) {
+                                if (iidx[k] < n) {
+                                    const double3 v = FORCE ? near_force_fp64(iidx[k], j, a, PER ? 1 : 0, inv_ell)
+                                                            : near_oseen_fp64(iidx[k], j, a, PER ? 1 : 0, inv_ell,
+                                                                              fscale_inv);
+                                    fold_double(hx[k], lx[k], v.x);
+                                    fold_double(hy[k], ly[k], v.y);
+                                    fold_double(hz[k], lz[k], v.z);
+                                }
+                            }
+                        }
+                    }
+                }
+                if ((jj & (FLUSH - 1)) == FLUSH - 1 || jj == cnt - 1) {
+#pragma unroll
+                    for (int k = 0; k < IPT; ++k) {
+                        two_sum_fold(hx[k], lx[k], ax[k]);
+                        two_sum_fold(hy[k], ly[k], ay[k]);
+                        two_sum_fold(hz[k], lz[k], az[k]);
+                        ax[k] = ay[k] = az[k] = 0.f;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        if (s_abort) {
+            aborted = true;
+            if (tid == 0 && t + 1 < ntiles) mbar_wait_bounded(&bar[(t + 1) & 1], (uint32_t)(((t + 1) >> 1) & 1), a.err);
+            break;
+        }
+    }
+    if (aborted) return;
+    const size_t plane = (size_t)n;
+    double *P = a.partial + (size_t)split * 3 * plane;
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+        const int i = iidx[k];
+        if (i < n) {
+            P[i] = (double)hx[k] + (double)lx[k];
+            P[plane + i] = (double)hy[k] + (double)ly[k];
+            P[2 * plane + i] = (double)hz[k] + (double)lz[k];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Preparation, scaling and reduction kernels
+// ---------------------------------------------------------------------------
+// Maximum of |v| over up to three arrays -> slot (as the bit pattern of a
+// non-negative double, which orders like an unsigned integer).
+__global__ void maxabs_kernel(int n, const double *__restrict__ a, const double *__restrict__ b,
+                              const double *__restrict__ c, unsigned long long *__restrict__ slot) {
+    double m = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        m = fmax(m, fabs(a[i]));
+        if (b) m = fmax(m, fabs(b[i]));
+        if (c) m = fmax(m, fabs(c[i]));
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m > 0.0) atomicMax(slot, (unsigned long long)__double_as_longlong(m));
+}
+
+__global__ void prep_positions_kernel(int n, const double *__restrict__ x, const double *__restrict__ y,
+                                      const double *__restrict__ z, const double *__restrict__ r, double center,
+                                      const unsigned long long *__restrict__ scales, double k_near,
+                                      float4 *__restrict__ pos4, float *__restrict__ kr) {
+    const double s = pow2_inv_of(scales[0]);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double rs = r[i] * s;
+        pos4[i] = make_float4((float)((x[i] - center) * s), (float)((y[i] - center) * s), (float)((z[i] - center) * s),
+                              (float)(rs * rs * rs));
+        if (kr) kr[i] = (float)(k_near * rs);
+    }
+}
+
+__global__ void prep_forces_kernel(int n, const double *__restrict__ fx, const double *__restrict__ fy,
+                                   const double *__restrict__ fz, const double *__restrict__ r,
+                                   const unsigned long long *__restrict__ scales, double k_near,
+                                   float4 *__restrict__ frc4) {
+    const double s = pow2_inv_of(scales[0]);
+    const double q = pow2_inv_of(scales[1]);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        frc4[i] = make_float4((float)(fx[i] * q), (float)(fy[i] * q), (float)(fz[i] * q), (float)(k_near * r[i] * s));
+}
+
+// out_c[i] = factor_i * sum_s partial[s][c][i]
+//   force:      factor_i = m_const * (r_i / ell)^3 * ell^2
+//   convection: factor   = eta / ell * 2^q
+template <bool FORCE>
+__global__ void reduce_partials_kernel(int n, int splits, const double *__restrict__ partial,
+                                       const double *__restrict__ r, const unsigned long long *__restrict__ scales,
+                                       double coeff, double *__restrict__ ox, double *__restrict__ oy,
+                                       double *__restrict__ oz, uint32_t *err) {
+    const double s = pow2_inv_of(scales[0]);
+    const double ell = 1.0 / s;
+    const double q = pow2_inv_of(scales[1]);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double sx = 0.0, sy = 0.0, sz = 0.0;
+        for (int p = 0; p < splits; ++p) {
+            const double *P = partial + (size_t)p * 3 * n;
+            sx += P[i];
+            sy += P[n + i];
+            sz += P[2 * (size_t)n + i];
+        }
+        double f;
+        if (FORCE) {
+            const double rs = r[i] * s;
+            f = coeff * ipow3(rs) * ell * ell;
+        } else {
+            f = coeff * s / q;
+        }
+        const double vx = f * sx, vy = f * sy, vz = f * sz;
+        if (!(isfinite(vx) && isfinite(vy) && isfinite(vz))) raise_device_error(err, DEM_DEVERR_NONFINITE);
+        ox[i] = vx;
+        oy[i] = vy;
+        oz[i] = vz;
+    }
+}
+
+template <int IPT, bool PER, bool FORCE>
+static void launch_pass(const MixedArgs &a, dim3 grid, int threads, cudaStream_t s) {
+    mixed_pass_kernel<IPT, PER, FORCE><<<grid, threads, 0, s>>>(a);
+}
+
+template <bool FORCE>
+static void dispatch_pass(int ipt, bool per, const MixedArgs &a, dim3 grid, int threads, cudaStream_t s) {
+    switch (ipt) {
+        case 1: per ? launch_pass<1, true, FORCE>(a, grid, threads, s) : launch_pass<1, false, FORCE>(a, grid, threads, s); break;
+        case 2: per ? launch_pass<2, true, FORCE>(a, grid, threads, s) : launch_pass<2, false, FORCE>(a, grid, threads, s); break;
+        case 8: per ? launch_pass<8, true, FORCE>(a, grid, threads, s) : launch_pass<8, false, FORCE>(a, grid, threads, s); break;
+        default: per ? launch_pass<4, true, FORCE>(a, grid, threads, s) : launch_pass<4, false, FORCE>(a, grid, threads, s); break;
+    }
+}
+
+struct MixedPlan {
+    int ipt, threads, splits, j_chunk;
+    dim3 grid;
+};
+
+static MixedPlan plan_for(const dem_ctx *ctx, int n) {
+    MixedPlan p;
+    p.ipt = ctx->tuning.i_per_thread;
+    p.threads = ctx->tuning.threads;
+    const int per_cta = p.threads * p.ipt;
+    const int iblocks = ceil_div(n, per_cta);
+    int splits = ctx->tuning.j_splits;
+    if (splits <= 0) {
+        const int target = 4 * ctx->sm_count;  // CTAs in flight
+        splits = (target + iblocks - 1) / iblocks;
+    }
+    const int max_splits = ceil_div(n, TJ);
+    if (splits > max_splits) splits = max_splits;
+    if (splits < 1) splits = 1;
+    p.j_chunk = ceil_div(ceil_div(n, splits), TJ) * TJ;
+    p.splits = ceil_div(n, p.j_chunk);
+    p.grid = dim3(iblocks, p.splits, 1);
+    return p;
+}
+
+int launch_direct_forces_mixed(dem_ctx *ctx, int n, const double *x, const double *y, const double *z,
+                               const double *r, double m_const, double L, int periodic, double *fx, double *fy,
+                               double *fz, cudaStream_t s) {
+    const MixedPlan p = plan_for(ctx, n);
+    int rc = dem_ensure_partials(ctx, p.splits);
+    if (rc) return rc;
+    unsigned long long *scales = reinterpret_cast<unsigned long long *>(ctx->dscratch);
+    rc = dem_check_cuda(ctx, cudaMemsetAsync(scales, 0, 2 * sizeof(unsigned long long), s), "memset");
+    if (rc) return rc;
+    const int rgrid = min(ceil_div(n, 256), 4 * ctx->sm_count);
+    maxabs_kernel<<<rgrid, 256, 0, s>>>(n, r, nullptr, nullptr, scales);
+    float *krf = reinterpret_cast<float *>(ctx->pack_b);  // force pass: k_f r lives in pack_b
+    prep_positions_kernel<<<rgrid, 256, 0, s>>>(n, x, y, z, r, 0.5 * L, scales, ctx->tuning.near_force, ctx->pack_a, krf);
+    MixedArgs a{};
+    a.n = n;
+    a.j_chunk = p.j_chunk;
+    a.pos4 = ctx->pack_a;
+    a.krf = krf;
+    a.x = x;
+    a.y = y;
+    a.z = z;
+    a.r = r;
+    a.L = L;
+    a.halfL = 0.5 * L;
+    a.partial = ctx->partial;
+    a.err = ctx->d_err;
+    a.scales = scales;
+    rc = dem_check_launch(ctx, "direct_forces_mixed prep");
+    if (rc) return rc;
+    dem_prof_begin(ctx, "mixed_force_pass", s);
+    dispatch_pass<true>(p.ipt, periodic != 0, a, p.grid, p.threads, s);
+    dem_prof_end(ctx, s);
+    rc = dem_check_launch(ctx, "direct_forces_mixed");
+    if (rc) return rc;
+    reduce_partials_kernel<true><<<rgrid, 256, 0, s>>>(n, p.splits, ctx->partial, r, scales, m_const, fx, fy, fz,
+                                                       ctx->d_err);
+    return dem_check_launch(ctx, "direct_forces_mixed reduce");
+}
+
+int launch_direct_convection_mixed(dem_ctx *ctx, int n, const double *x, const double *y, const double *z,
+                                   const double *r, const double *fx, const double *fy, const double *fz, double eta,
+                                   double L, int periodic, double *vx, double *vy, double *vz, cudaStream_t s) {
+    const MixedPlan p = plan_for(ctx, n);
+    int rc = dem_ensure_partials(ctx, p.splits);
+    if (rc) return rc;
+    unsigned long long *scales = reinterpret_cast<unsigned long long *>(ctx->dscratch);
+    rc = dem_check_cuda(ctx, cudaMemsetAsync(scales, 0, 2 * sizeof(unsigned long long), s), "memset");
+    if (rc) return rc;
+    const int rgrid = min(ceil_div(n, 256), 4 * ctx->sm_count);
+    maxabs_kernel<<<rgrid, 256, 0, s>>>(n, r, nullptr, nullptr, scales);
+    maxabs_kernel<<<rgrid, 256, 0, s>>>(n, fx, fy, fz, scales + 1);
+    prep_positions_kernel<<<rgrid, 256, 0, s>>>(n, x, y, z, r, 0.5 * L, scales, 0.0, ctx->pack_a, nullptr);
+    prep_forces_kernel<<<rgrid, 256, 0, s>>>(n, fx, fy, fz, r, scales, ctx->tuning.near_oseen, ctx->pack_b);
+    rc = dem_check_launch(ctx, "direct_convection_mixed prep");
+    if (rc) return rc;
+    MixedArgs a{};
+    a.n = n;
+    a.j_chunk = p.j_chunk;
+    a.pos4 = ctx->pack_a;
+    a.frc4 = ctx->pack_b;
+    a.x = x;
+    a.y = y;
+    a.z = z;
+    a.r = r;
+    a.fx = fx;
+    a.fy = fy;
+    a.fz = fz;
+    a.L = L;
+    a.halfL = 0.5 * L;
+    a.scales = scales;
+    a.partial = ctx->partial;
+    a.err = ctx->d_err;
+    dem_prof_begin(ctx, "mixed_convection_pass", s);
+    dispatch_pass<false>(p.ipt, periodic != 0, a, p.grid, p.threads, s);
+    dem_prof_end(ctx, s);
+    rc = dem_check_launch(ctx, "direct_convection_mixed");
+    if (rc) return rc;
+    reduce_partials_kernel<false><<<rgrid, 256, 0, s>>>(n, p.splits, ctx->partial, r, scales, eta, vx, vy, vz,
+                                                        ctx->d_err);
+    return dem_check_launch(ctx, "direct_convection_mixed reduce");
+}
+
+}  // namespace dem

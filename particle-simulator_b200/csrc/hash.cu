@@ -1,0 +1,260 @@
+// hash.cu -- spatial-hash collision detection with the reference's exact
+// cell, hash and distance semantics, producing the sorted unique pair set.
+//
+// dem/collision_detector/spatial_hash_collision_detector.py:
+//   _hash_cell :74-76, _assign_cells :79-112, _prefix_sum :115-123,
+//   _scatter_particles :126-132, _detect_collisions :135-229, detect :233-316.
+//
+// Pipeline (all on the device, no host synchronisation):
+//   1. max radius            -> cell = 2 max r, grid = max(1, ceil(L / cell))
+//   2. bucket of every droplet, bucket counts (atomics)
+//   3. exclusive scan of the counts (bucket starts), scatter into buckets
+//   4. per droplet i: the distinct hash buckets of its 27 neighbour cells; count
+//      the j > i in them with MIC distance <= r_i + r_j
+//   5. exclusive scan of the per-i counts -> pair offsets (lexicographic order)
+//   6. per droplet i: write its pairs, sort its j's ascending
+// The candidate set of a droplet is exactly the reference's (the same buckets,
+// including buckets shared by aliased cells), and the distance test is the
+// same IEEE expression (this file is compiled with -fmad=false), so the pair
+// set is bit-identical to the reference's np.unique output.
+#include "common.cuh"
+#include "scan.cuh"
+
+namespace dem {
+
+struct HashParams {
+    double cell;
+    int32_t grid;
+    int32_t valid;
+};
+
+__device__ __forceinline__ unsigned long long ordered_bits(double v) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double from_ordered_bits(unsigned long long o) {
+    const unsigned long long b = (o >> 63) ? (o & 0x7fffffffffffffffull) : ~o;
+    return __longlong_as_double((long long)b);
+}
+
+__global__ void max_kernel(int n, const double *__restrict__ r, unsigned long long *__restrict__ slot) {
+    unsigned long long m = 0ull;  // below every ordered value
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const unsigned long long o = ordered_bits(r[i]);
+        m = o > m ? o : m;
+    }
+#pragma unroll
+    for (int off = 16; off; off >>= 1) {
+        const unsigned long long t = __shfl_xor_sync(0xffffffffu, m, off);
+        m = t > m ? t : m;
+    }
+    if ((threadIdx.x & 31) == 0) atomicMax(slot, m);
+}
+
+__global__ void hash_params_kernel(const unsigned long long *__restrict__ slot, double L, HashParams *__restrict__ hp) {
+    const double max_radius = from_ordered_bits(*slot);
+    const double cell = 2.0 * max_radius;  // :258
+    HashParams p;
+    p.cell = cell;
+    p.valid = cell > 0 ? 1 : 0;  // :259-260
+    double g = p.valid ? ceil(L / cell) : 1.0;
+    if (!(g >= 1.0)) g = 1.0;
+    if (g > 1073741824.0) g = 1073741824.0;
+    p.grid = (int32_t)g;  // :262
+    *hp = p;
+}
+
+__device__ __forceinline__ int32_t hash_cell(int32_t ix, int32_t iy, int32_t iz, int32_t mask) {
+    const uint32_t h = ((uint32_t)ix * 73856093u) ^ ((uint32_t)iy * 19349663u) ^ ((uint32_t)iz * 83492791u);
+    return (int32_t)(h & (uint32_t)mask);
+}
+
+__device__ __forceinline__ int32_t floor_mod(int32_t a, int32_t m) {
+    const int32_t q = a % m;
+    return q < 0 ? q + m : q;
+}
+
+__device__ __forceinline__ int32_t cell_coord(double p, double cell, int32_t grid, bool periodic) {
+    int32_t v = (int32_t)floor(p / cell);
+    if (periodic) return floor_mod(v, grid);
+    return v < 0 ? 0 : (v >= grid ? grid - 1 : v);
+}
+
+__global__ void assign_kernel(int n, const double *__restrict__ x, const double *__restrict__ y,
+                              const double *__restrict__ z, const HashParams *__restrict__ hp, int periodic,
+                              int32_t mask, int32_t *__restrict__ cell_hash, int32_t *__restrict__ bucket_count) {
+    const HashParams p = *hp;
+    if (!p.valid) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int32_t ix = cell_coord(x[i], p.cell, p.grid, periodic);
+        const int32_t iy = cell_coord(y[i], p.cell, p.grid, periodic);
+        const int32_t iz = cell_coord(z[i], p.cell, p.grid, periodic);
+        const int32_t h = hash_cell(ix, iy, iz, mask);
+        cell_hash[i] = h;
+        atomicAdd(&bucket_count[h], 1);
+    }
+}
+
+__global__ void scatter_kernel(int n, const int32_t *__restrict__ cell_hash, const HashParams *__restrict__ hp,
+                               int32_t *__restrict__ cursor, int32_t *__restrict__ sorted_idx) {
+    if (!hp->valid) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int32_t slot = atomicAdd(&cursor[cell_hash[i]], 1);
+        sorted_idx[slot] = i;
+    }
+}
+
+// Visits every candidate j > i of droplet i (the distinct buckets of its 27
+// neighbour cells) and calls f(j, multiplicity) for those in contact.
+template <typename F>
+__device__ __forceinline__ void for_each_contact(int i, const double *__restrict__ x, const double *__restrict__ y,
+                                                 const double *__restrict__ z, const double *__restrict__ r,
+                                                 const HashParams &p, int periodic, double L, double halfL,
+                                                 int32_t mask, int n, const int32_t *__restrict__ bstart,
+                                                 const int32_t *__restrict__ sorted_idx, F &&f) {
+    const double xi = x[i], yi = y[i], zi = z[i], ri = r[i];
+    const int32_t cx = cell_coord(xi, p.cell, p.grid, periodic);
+    const int32_t cy = cell_coord(yi, p.cell, p.grid, periodic);
+    const int32_t cz = cell_coord(zi, p.cell, p.grid, periodic);
+    int32_t hs[27];
+    int nh = 0;
+    int mult[27];
+    for (int di = -1; di <= 1; ++di)
+        for (int dj = -1; dj <= 1; ++dj)
+            for (int dk = -1; dk <= 1; ++dk) {
+                int32_t nx = cx + di, ny = cy + dj, nz = cz + dk;
+                if (periodic) {
+                    nx = floor_mod(nx, p.grid);
+                    ny = floor_mod(ny, p.grid);
+                    nz = floor_mod(nz, p.grid);
+                } else if (nx < 0 || ny < 0 || nz < 0 || nx >= p.grid || ny >= p.grid || nz >= p.grid) {
+                    continue;
+                }
+                const int32_t h = hash_cell(nx, ny, nz, mask);
+                int q = 0;
+                while (q < nh && hs[q] != h) ++q;
+                if (q == nh) {
+                    hs[nh] = h;
+                    mult[nh] = 1;
+                    ++nh;
+                } else {
+                    ++mult[q];
+                }
+            }
+    for (int q = 0; q < nh; ++q) {
+        const int32_t start = bstart[hs[q]];
+        int32_t end = bstart[hs[q] + 1];
+        if (end > n) end = n;  // :199-201
+        for (int32_t s = start; s < end; ++s) {
+            const int32_t j = sorted_idx[s];
+            if (!(i < j)) continue;
+            double dx = x[j] - xi, dy = y[j] - yi, dz = z[j] - zi;
+            if (periodic) {
+                dx = mic64(dx, L, halfL);
+                dy = mic64(dy, L, halfL);
+                dz = mic64(dz, L, halfL);
+            }
+            const double dist = sqrt(dx * dx + dy * dy + dz * dz);
+            if (dist <= ri + r[j]) f(j, mult[q]);
+        }
+    }
+}
+
+__global__ void count_pairs_kernel(int n, const double *__restrict__ x, const double *__restrict__ y,
+                                   const double *__restrict__ z, const double *__restrict__ r,
+                                   const HashParams *__restrict__ hp, int periodic, double L, int32_t mask,
+                                   const int32_t *__restrict__ bstart, const int32_t *__restrict__ sorted_idx,
+                                   int32_t *__restrict__ pair_count, unsigned long long *__restrict__ raw) {
+    const HashParams p = *hp;
+    unsigned long long local_raw = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int32_t c = 0;
+        if (p.valid) {
+            for_each_contact(i, x, y, z, r, p, periodic, L, 0.5 * L, mask, n, bstart, sorted_idx, [&](int32_t, int m) {
+                ++c;
+                local_raw += (unsigned long long)m;
+            });
+        }
+        pair_count[i] = c;
+    }
+    if (local_raw) atomicAdd(raw, local_raw);
+}
+
+__global__ void write_pairs_kernel(int n, const double *__restrict__ x, const double *__restrict__ y,
+                                   const double *__restrict__ z, const double *__restrict__ r,
+                                   const HashParams *__restrict__ hp, int periodic, double L, int32_t mask,
+                                   const int32_t *__restrict__ bstart, const int32_t *__restrict__ sorted_idx,
+                                   const int64_t *__restrict__ offset, int32_t *__restrict__ pairs, int64_t cap,
+                                   int64_t *__restrict__ counts, uint32_t *err) {
+    const HashParams p = *hp;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        counts[0] = p.valid ? offset[n] : 0;
+        if (p.valid && offset[n] > cap) raise_device_error(err, DEM_DEVERR_PAIR_OVERFLOW);
+    }
+    if (!p.valid) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int64_t o0 = offset[i], o1 = offset[i + 1];
+        if (o1 == o0) continue;
+        int64_t w = o0;
+        for_each_contact(i, x, y, z, r, p, periodic, L, 0.5 * L, mask, n, bstart, sorted_idx, [&](int32_t j, int) {
+            if (w < cap) {
+                pairs[2 * w] = i;
+                pairs[2 * w + 1] = j;
+            }
+            ++w;
+        });
+        // ascending j within the row of droplet i (insertion sort of a short run)
+        const int64_t e = o1 < cap ? o1 : cap;
+        for (int64_t a = o0 + 1; a < e; ++a) {
+            const int32_t v = pairs[2 * a + 1];
+            int64_t b = a - 1;
+            while (b >= o0 && pairs[2 * b + 1] > v) {
+                pairs[2 * (b + 1) + 1] = pairs[2 * b + 1];
+                --b;
+            }
+            pairs[2 * (b + 1) + 1] = v;
+        }
+    }
+}
+
+int launch_hash_detect(dem_ctx *ctx, int n, const double *x, const double *y, const double *z, const double *r,
+                       double L, int periodic, int table_size, int32_t *pairs, int64_t cap, int64_t *counts,
+                       cudaStream_t s) {
+    int rc = dem_ensure_table(ctx, table_size);
+    if (rc) return rc;
+    unsigned long long *slot = reinterpret_cast<unsigned long long *>(ctx->dscratch) + 2;
+    HashParams *hp = reinterpret_cast<HashParams *>(ctx->dscratch + 4);
+    const int32_t mask = table_size - 1;
+    const int grid = max(1, min(ceil_div(n, 256), 8 * ctx->sm_count));
+    rc = dem_check_cuda(ctx, cudaMemsetAsync(slot, 0, sizeof(unsigned long long), s), "memset");
+    if (!rc) rc = dem_check_cuda(ctx, cudaMemsetAsync(counts, 0, 2 * sizeof(int64_t), s), "memset");
+    if (!rc) rc = dem_check_cuda(ctx, cudaMemsetAsync(ctx->bucket_count, 0, sizeof(int32_t) * table_size, s), "memset");
+    if (rc) return rc;
+    if (n == 0) return DEM_OK;
+    dem_prof_begin(ctx, "hash_detect", s);
+    max_kernel<<<grid, 256, 0, s>>>(n, r, slot);
+    hash_params_kernel<<<1, 1, 0, s>>>(slot, L, hp);
+    assign_kernel<<<grid, 256, 0, s>>>(n, x, y, z, hp, periodic, mask, ctx->cell_hash, ctx->bucket_count);
+    rc = dem_check_launch(ctx, "hash assign");
+    if (rc) return rc;
+    rc = exclusive_scan<int32_t, int32_t>(ctx, ctx->bucket_count, ctx->bucket_start, table_size, s);
+    if (rc) return rc;
+    rc = dem_check_cuda(ctx, cudaMemcpyAsync(ctx->bucket_cursor, ctx->bucket_start, sizeof(int32_t) * table_size,
+                                             cudaMemcpyDeviceToDevice, s),
+                        "cursor copy");
+    if (rc) return rc;
+    scatter_kernel<<<grid, 256, 0, s>>>(n, ctx->cell_hash, hp, ctx->bucket_cursor, ctx->sorted_idx);
+    const int dgrid = ceil_div(n, 128);
+    count_pairs_kernel<<<dgrid, 128, 0, s>>>(n, x, y, z, r, hp, periodic, L, mask, ctx->bucket_start, ctx->sorted_idx,
+                                             ctx->pair_count, reinterpret_cast<unsigned long long *>(counts + 1));
+    rc = dem_check_launch(ctx, "hash count");
+    if (rc) return rc;
+    rc = exclusive_scan<int32_t, int64_t>(ctx, ctx->pair_count, ctx->pair_offset, n, s);
+    if (rc) return rc;
+    write_pairs_kernel<<<dgrid, 128, 0, s>>>(n, x, y, z, r, hp, periodic, L, mask, ctx->bucket_start, ctx->sorted_idx,
+                                             ctx->pair_offset, pairs, cap, counts, ctx->d_err);
+    dem_prof_end(ctx, s);
+    return dem_check_launch(ctx, "hash write");
+}
+
+}  // namespace dem

@@ -1,0 +1,286 @@
+"""ctypes binding of ``libdem_b200.so`` (declared in ``include/dem_b200.h``).
+
+PyTorch is used only for device memory, pinned host staging buffers and the
+current CUDA stream.  Every computation goes through the CUDA kernels of the
+library; there is no CPU fallback: if the library or a CUDA device is missing
+the classes raise instead of computing elsewhere.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parents[1] / "libdem_b200.so"
+
+DEM_OK = 0
+DEM_E_INVALID = 1
+DEM_E_CAPACITY = 2
+DEM_E_CUDA = 3
+DEM_E_DEVICE = 4
+DEM_E_NOT_ALLOCATED = 5
+
+PREC_FP64 = 0
+PREC_MIXED = 1
+PRECISIONS = {"fp64": PREC_FP64, "mixed": PREC_MIXED}
+
+DEVERR_WAIT_TIMEOUT = 1
+DEVERR_PAIR_OVERFLOW = 2
+DEVERR_NODE_OVERFLOW = 4
+DEVERR_NONFINITE = 8
+
+# name -> (restype, argtypes); the C ABI in include/dem_b200.h
+_i, _d, _vp, _i64 = C.c_int, C.c_double, C.c_void_p, C.c_int64
+SIGNATURES = {
+    "dem_version": (C.c_char_p, []),
+    "dem_ctx_create": (_i, [_i, _i, C.POINTER(_vp)]),
+    "dem_ctx_destroy": (None, [_vp]),
+    "dem_ctx_reserve": (_i, [_vp, _i]),
+    "dem_ctx_capacity": (_i, [_vp]),
+    "dem_last_error": (C.c_char_p, [_vp]),
+    "dem_device_errors": (_i, [_vp, C.POINTER(C.c_uint32), _vp]),
+    "dem_profile_enable": (_i, [_vp, _i]),
+    "dem_profile_read": (_i, [_vp, C.c_char_p, C.POINTER(_d), C.POINTER(_i)]),
+    "dem_profile_reset": (_i, [_vp]),
+    "dem_direct_set_tuning": (_i, [_vp, _i, _i, _i, _d, _d]),
+    "dem_direct_get_tuning": (_i, [_vp, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i), C.POINTER(_d), C.POINTER(_d)]),
+    "dem_aos_to_soa": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp]),
+    "dem_soa_to_aos": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp]),
+    "dem_direct_forces": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _d, _d, _i, _i, _vp, _vp, _vp, _vp]),
+    "dem_direct_convection": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _d, _d, _i, _i, _vp, _vp, _vp, _vp]),
+    "dem_euler_update": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _d, _d, _d, _i, _vp, _vp, _vp, _vp]),
+    "dem_euler_update_total": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _d, _d, _i, _vp, _vp, _vp, _vp]),
+    "dem_hash_detect": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _d, _i, _i, _vp, _i64, _vp, _vp]),
+    "dem_merge": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+class DemError(RuntimeError):
+    """A CUDA or device-side failure reported by libdem_b200."""
+
+
+def lib():
+    """Load the library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        with _lock:
+            if _lib is None:
+                if not LIB_PATH.exists():
+                    raise ImportError(
+                        f"{LIB_PATH} is missing: build it with `python particle-simulator_b200/build_native.py`"
+                    )
+                L = C.CDLL(str(LIB_PATH))
+                for name, (res, args) in SIGNATURES.items():
+                    fn = getattr(L, name)
+                    fn.restype = res
+                    fn.argtypes = args
+                _lib = L
+    return _lib
+
+
+def exported_symbols():
+    return sorted(SIGNATURES)
+
+
+def version() -> str:
+    return lib().dem_version().decode()
+
+
+def _torch():
+    import torch
+
+    if not torch.cuda.is_available():
+        raise RuntimeError("libdem_b200 needs a CUDA device (B200, sm_100a); none is available")
+    return torch
+
+
+def ptr(t) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+class Context:
+    """One ``dem_ctx`` (device workspace) bound to a CUDA device."""
+
+    def __init__(self, capacity: int, device=None):
+        torch = _torch()
+        self.torch = torch
+        if device is None:
+            device = torch.cuda.current_device()
+        self.device = torch.device("cuda", torch.device(device).index if not isinstance(device, int) else device)
+        self.handle = _vp()
+        with torch.cuda.device(self.device):
+            self._check(lib().dem_ctx_create(self.device.index, max(int(capacity), 1), C.byref(self.handle)), "create")
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value and _lib is not None:
+            try:
+                _lib.dem_ctx_destroy(h)
+            except Exception:  # pragma: no cover - interpreter shutdown
+                pass
+            self.handle = None
+
+    # -- errors -------------------------------------------------------------
+    def _check(self, rc: int, what: str):
+        if rc == DEM_OK:
+            return
+        msg = (lib().dem_last_error(self.handle).decode() if self.handle else "") or what
+        if rc in (DEM_E_INVALID, DEM_E_CAPACITY):
+            raise ValueError(msg)
+        if rc == DEM_E_NOT_ALLOCATED:
+            raise RuntimeError(msg)
+        raise DemError(f"{what}: {msg} (code {rc})")
+
+    def stream(self):
+        return self.torch.cuda.current_stream(self.device).cuda_stream
+
+    @property
+    def capacity(self) -> int:
+        return lib().dem_ctx_capacity(self.handle)
+
+    def reserve(self, capacity: int):
+        self._check(lib().dem_ctx_reserve(self.handle, int(capacity)), "reserve")
+
+    def device_errors(self) -> int:
+        out = C.c_uint32(0)
+        self._check(lib().dem_device_errors(self.handle, C.byref(out), self.stream()), "device_errors")
+        return int(out.value)
+
+    def raise_device_errors(self):
+        f = self.device_errors()
+        if f & DEVERR_WAIT_TIMEOUT:
+            raise DemError("a bounded device wait timed out")
+        if f & DEVERR_NONFINITE:
+            raise DemError("a kernel produced a non-finite value")
+        return f
+
+    # -- kernel timing ------------------------------------------------------
+    def profile(self, enable: bool = True):
+        self._check(lib().dem_profile_enable(self.handle, int(bool(enable))), "profile_enable")
+
+    def profile_read(self, name: str):
+        ms, k = _d(), _i()
+        self._check(lib().dem_profile_read(self.handle, name.encode(), C.byref(ms), C.byref(k)), "profile_read")
+        return float(ms.value), int(k.value)
+
+    def profile_reset(self):
+        self._check(lib().dem_profile_reset(self.handle), "profile_reset")
+
+    # -- tuning -------------------------------------------------------------
+    def set_tuning(self, i_per_thread=0, threads=0, j_splits=0, near_force=0.0, near_oseen=0.0):
+        self._check(
+            lib().dem_direct_set_tuning(self.handle, int(i_per_thread), int(threads), int(j_splits),
+                                        float(near_force), float(near_oseen)),
+            "set_tuning",
+        )
+
+    def get_tuning(self):
+        a, b, c = _i(), _i(), _i()
+        d, e = _d(), _d()
+        self._check(lib().dem_direct_get_tuning(self.handle, C.byref(a), C.byref(b), C.byref(c), C.byref(d), C.byref(e)),
+                    "get_tuning")
+        return dict(i_per_thread=a.value, threads=b.value, j_splits=c.value, near_force=d.value, near_oseen=e.value)
+
+    # -- thin wrappers over the C ABI (torch CUDA tensors in, no allocation) --
+    def aos_to_soa(self, n, aos, soa):
+        self._check(lib().dem_aos_to_soa(self.handle, n, ptr(aos), ptr(soa[0]), ptr(soa[1]), ptr(soa[2]), self.stream()),
+                    "aos_to_soa")
+
+    def soa_to_aos(self, n, soa, aos):
+        self._check(lib().dem_soa_to_aos(self.handle, n, ptr(soa[0]), ptr(soa[1]), ptr(soa[2]), ptr(aos), self.stream()),
+                    "soa_to_aos")
+
+    def direct_forces(self, n, pos, r, m_const, L, periodic, precision, out):
+        self._check(
+            lib().dem_direct_forces(self.handle, n, ptr(pos[0]), ptr(pos[1]), ptr(pos[2]), ptr(r), float(m_const),
+                                    float(L), int(periodic), int(precision), ptr(out[0]), ptr(out[1]), ptr(out[2]),
+                                    self.stream()),
+            "direct_forces",
+        )
+
+    def direct_convection(self, n, pos, r, F, eta_const, L, periodic, precision, out):
+        self._check(
+            lib().dem_direct_convection(self.handle, n, ptr(pos[0]), ptr(pos[1]), ptr(pos[2]), ptr(r), ptr(F[0]),
+                                        ptr(F[1]), ptr(F[2]), float(eta_const), float(L), int(periodic),
+                                        int(precision), ptr(out[0]), ptr(out[1]), ptr(out[2]), self.stream()),
+            "direct_convection",
+        )
+
+    def euler_update(self, n, pos, r, F, V, stokes, dt, L, periodic, out):
+        self._check(
+            lib().dem_euler_update(self.handle, n, ptr(pos[0]), ptr(pos[1]), ptr(pos[2]), ptr(r), ptr(F[0]), ptr(F[1]),
+                                   ptr(F[2]), ptr(V[0]), ptr(V[1]), ptr(V[2]), float(stokes), float(dt), float(L),
+                                   int(periodic), ptr(out[0]), ptr(out[1]), ptr(out[2]), self.stream()),
+            "euler_update",
+        )
+
+    def euler_update_total(self, n, pos, V, dt, L, periodic, out):
+        self._check(
+            lib().dem_euler_update_total(self.handle, n, ptr(pos[0]), ptr(pos[1]), ptr(pos[2]), ptr(V[0]), ptr(V[1]),
+                                         ptr(V[2]), float(dt), float(L), int(periodic), ptr(out[0]), ptr(out[1]),
+                                         ptr(out[2]), self.stream()),
+            "euler_update_total",
+        )
+
+    def hash_detect(self, n, pos, r, L, periodic, table_size, pairs, capacity, counts):
+        self._check(
+            lib().dem_hash_detect(self.handle, n, ptr(pos[0]), ptr(pos[1]), ptr(pos[2]), ptr(r), float(L),
+                                  int(periodic), int(table_size), ptr(pairs), int(capacity), ptr(counts),
+                                  self.stream()),
+            "hash_detect",
+        )
+
+    def merge(self, n, pos, r, pairs, num_pairs, out_pos, out_r, n_out, merged=None):
+        self._check(
+            lib().dem_merge(self.handle, n, ptr(pos[0]), ptr(pos[1]), ptr(pos[2]), ptr(r), ptr(pairs), ptr(num_pairs),
+                            ptr(out_pos[0]), ptr(out_pos[1]), ptr(out_pos[2]), ptr(out_r), ptr(n_out), ptr(merged),
+                            self.stream()),
+            "merge",
+        )
+
+
+class Buffers:
+    """Growable device and pinned-host buffers owned by one calculator."""
+
+    def __init__(self, device):
+        import torch
+
+        self.torch = torch
+        self.device = device
+        self._dev = {}
+        self._host = {}
+
+    def dev(self, name, shape, dtype=None):
+        torch = self.torch
+        dtype = dtype or torch.float64
+        numel = int(np.prod(shape))
+        t = self._dev.get(name)
+        if t is None or t.numel() < numel or t.dtype != dtype:
+            t = torch.empty(max(numel, 1), dtype=dtype, device=self.device)
+            self._dev[name] = t
+        return t[:numel].view(*shape)
+
+    def host(self, name, shape, dtype=None):
+        torch = self.torch
+        dtype = dtype or torch.float64
+        numel = int(np.prod(shape))
+        t = self._host.get(name)
+        if t is None or t.numel() < numel or t.dtype != dtype:
+            t = torch.empty(max(numel, 1), dtype=dtype, pin_memory=True)
+            self._host[name] = t
+        return t[:numel].view(*shape)
+
+
+def is_cuda_tensor(a) -> bool:
+    try:
+        import torch
+
+        return isinstance(a, torch.Tensor) and a.is_cuda
+    except Exception:  # pragma: no cover
+        return False

@@ -1,0 +1,124 @@
+"""Spatial-hash detection and coalescence on the GPU: bit-exact pair sets and
+merged states against the oracle and the reference's golden vectors."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import GOLDEN
+from gpu_util import lognormal_state
+
+pytestmark = pytest.mark.gpu
+
+
+def _det(n, L=1.0, mode="periodic"):
+    from dem.collision_detector import SpatialHashCollisionDetector
+
+    return SpatialHashCollisionDetector(num_particles=n, L=L, boundary_mode=mode)
+
+
+@pytest.mark.parametrize("name", sorted(p.name for p in GOLDEN.glob("hash_*.npz")))
+def test_pairs_bit_exact_against_golden(golden, name):
+    g = golden(name)
+    n = len(g["radii"])
+    det = _det(int(g["capacity"]), float(g["L"]), "periodic" if g["periodic"] else "open")
+    assert det._hash_table_size == int(g["table_size"])
+    hit, pairs = det.detect(g["positions"], g["radii"])
+    assert hit == bool(g["is_collision"])
+    assert pairs.dtype == np.int32 and pairs.shape[1] == 2
+    np.testing.assert_array_equal(pairs, g["pairs"])
+    assert n == len(g["radii"])
+
+
+@pytest.mark.parametrize("n,seed,gap", [(4096, 0, -2e-6), (20000, 1, -1e-6), (3000, 2, 1e-6)])
+def test_pairs_bit_exact_lognormal(n, seed, gap):
+    from dem.particle_generator import LognormalDropletGenerator
+
+    g = LognormalDropletGenerator(n, seed=seed, minimum_distance=gap)
+    s = g.generate()
+    det = _det(n, g.L)
+    hit, pairs = det.detect(s.positions, s.radii)
+    hit_ref, pairs_ref = O.hash_detect(s.positions, s.radii, g.L, True, table_size=det._hash_table_size)
+    assert hit == hit_ref
+    np.testing.assert_array_equal(pairs, pairs_ref)
+    if gap < 0:
+        assert len(pairs) > 0
+
+
+def test_reference_detector_cases():
+    # tests/collision_detector/test_spatial_hash_collision_detector.py upstream
+    det = _det(8, 1.0, "open")
+    hit, pairs = det.detect(np.array([[0.1, 0.1, 0.1], [0.9, 0.9, 0.9]]), np.full(2, 0.05), L=1.0, boundary_mode="open")
+    assert hit is False and pairs.shape == (0, 2)
+    hit, pairs = det.detect(np.array([[0.5, 0.5, 0.5], [0.52, 0.5, 0.5]]), np.full(2, 0.05), L=1.0, boundary_mode="open")
+    assert hit is True and [tuple(p) for p in pairs] == [(0, 1)]
+    det = _det(4, 1.0, "periodic")
+    pos = np.array([[0.01, 0.5, 0.5], [0.99, 0.5, 0.5]])
+    assert det.detect(pos, np.full(2, 0.05), L=1.0, boundary_mode="open")[0] is False
+    hit, pairs = det.detect(pos, np.full(2, 0.05), L=1.0, boundary_mode="periodic")
+    assert hit is True and len(pairs) >= 1
+    hit, pairs = _det(4, 1.0, "open").detect(np.zeros((2, 3)), np.zeros(2))
+    assert hit is False and pairs.shape == (0, 2)
+    hit, pairs = _det(8).detect(np.array([[0.5, 0.5, 0.5], [0.51, 0.5, 0.5], [0.52, 0.5, 0.5]]), np.full(3, 0.02))
+    assert hit is True and len(pairs) == len({tuple(sorted(p)) for p in pairs}) == 3
+
+
+def test_pair_buffer_grows_beyond_capacity():
+    rng = np.random.default_rng(9)
+    pos = rng.uniform(0, 1e-4, (300, 3))
+    r = np.full(300, 3e-5)  # nearly every pair overlaps
+    det = _det(300, 1e-4)
+    hit, pairs = det.detect(pos, r)
+    _, pairs_ref = O.hash_detect(pos, r, 1e-4, True, table_size=det._hash_table_size)
+    assert len(pairs_ref) > det._ctx.capacity
+    np.testing.assert_array_equal(pairs, pairs_ref)
+
+
+@pytest.mark.parametrize("name", sorted(p.name for p in GOLDEN.glob("merge_*.npz")))
+def test_merge_bit_exact_against_golden(golden, name):
+    from dem.particle_state import DropletState
+    from dem.solution import DropletSolution
+
+    g = golden(name)
+    sol = DropletSolution(initial_droplet_state=DropletState(g["positions"], g["radii"], 0.25), length=4)
+    sol.collided_droplets = g["pairs"]
+    nxt = sol.generate_next_solution()
+    np.testing.assert_array_equal(nxt.initial_droplet_state.positions, g["new_positions"])
+    np.testing.assert_array_equal(nxt.radii, g["new_radii"])
+    assert nxt._prev is sol and sol._next is nxt
+    assert nxt.get_current_time() == 0.25
+
+
+def test_merge_volume_arithmetic_matches_libm_on_many_pairs():
+    """Correctly rounded r^3 and v^(1/3) on the device agree with libm pow."""
+    from dem.solution.droplet_solution import merge_droplets
+
+    rng = np.random.default_rng(11)
+    n = 40000
+    r = np.exp(rng.uniform(np.log(1e-7), np.log(1e-3), n))
+    pos = rng.uniform(0, 1e-2, (n, 3))
+    pairs = np.stack([np.arange(0, n, 2), np.arange(1, n, 2)], 1).astype(np.int32)
+    p_gpu, r_gpu = merge_droplets(pos, r, pairs)
+    p_ref, r_ref, _ = O.merge(pos, r, pairs)
+    np.testing.assert_array_equal(r_gpu, r_ref)
+    np.testing.assert_array_equal(p_gpu, p_ref)
+
+
+def test_merge_greedy_order_random():
+    from dem.solution.droplet_solution import merge_droplets, order_pairs
+
+    pos, r, L = lognormal_state(3000, seed=3)
+    rng = np.random.default_rng(3)
+    a = rng.integers(0, 3000, 1500)
+    b = rng.integers(0, 3000, 1500)
+    keep = a != b
+    pairs = np.unique(np.sort(np.stack([a[keep], b[keep]], 1), axis=1), axis=0).astype(np.int32)
+    p_gpu, r_gpu = merge_droplets(pos, r, order_pairs(pairs))
+    p_ref, r_ref, _ = O.merge(pos, r, pairs)
+    np.testing.assert_array_equal(r_gpu, r_ref)
+    np.testing.assert_array_equal(p_gpu, p_ref)
+    assert len(r_gpu) < 3000
+    # volume is conserved to rounding
+    assert abs(np.sum(r_gpu**3) - np.sum(r**3)) <= 1e-12 * np.sum(r**3)

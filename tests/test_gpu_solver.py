@@ -1,0 +1,88 @@
+"""The device-resident Euler solver (detection, merge, direct passes, Euler
+update on the GPU) against the reference's golden solver run and the oracle."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle as O
+from gpu_util import ETA_OIL, lognormal_state
+
+pytestmark = pytest.mark.gpu
+
+
+class _Post:
+    stop_simulation = False
+
+    def update_solution(self, s):
+        self.solution = s
+
+    def update_live_plot(self):
+        pass
+
+    def live_plot(self):
+        pass
+
+    def finalize_live_plot(self):
+        pass
+
+
+def _run(pos, r, L, dt, total_time, precision="fp64", eta_oil=ETA_OIL, eps_oil=2.85, eta_water=0.001, E=3e5):
+    from dem.collision_detector import SpatialHashCollisionDetector
+    from dem.force_calculator import DirectDropletForceCalculator
+    from dem.particle_state import DropletState
+    from dem.solution import DropletSolution
+    from dem.solver import EulerDropletSolver
+
+    n = len(r)
+    fc = DirectDropletForceCalculator(num_particles=n, eps_oil=eps_oil, eta_oil=eta_oil, eta_water=eta_water, E=E,
+                                      L=L, boundary_mode="periodic", precision=precision)
+    det = SpatialHashCollisionDetector(num_particles=n, L=L, boundary_mode="periodic")
+    sol = DropletSolution(initial_droplet_state=DropletState(pos.copy(), r.copy(), time=0.0), length=4)
+    solver = EulerDropletSolver(fc, sol, _Post(), collision_detector=det, verbose=False)
+    solver.solve(dt, total_time)
+    chain = []
+    s = solver.solution.get_first_solution()
+    while s is not None:
+        chain.append(s)
+        s = s._next
+    return solver, chain
+
+
+def test_golden_solver_chain_bit_exact(golden):
+    g = golden("solver_direct_periodic_n48.npz")
+    _, chain = _run(g["positions"], g["radii"], float(g["L"]), float(g["dt"]), float(g["total_time"]),
+                    eta_oil=float(g["eta_oil"]), eps_oil=float(g["eps_oil"]), eta_water=float(g["eta_water"]),
+                    E=float(g["E"]))
+    assert len(chain) == int(g["n_solutions"])
+    for k, s in enumerate(chain):
+        np.testing.assert_array_equal(s.radii, g[f"sol{k}_radii"])
+        np.testing.assert_array_equal(s.get_times().ravel(), g[f"sol{k}_times"])
+        np.testing.assert_array_equal(s.get_trajectories(), g[f"sol{k}_trajectories"])
+        np.testing.assert_array_equal(np.asarray(s.collided_droplets, dtype=np.int32).reshape(-1, 2),
+                                      g[f"sol{k}_collided"])
+
+
+def test_lognormal_2000_twenty_steps_bit_exact():
+    pos, r, L = lognormal_state(2000, seed=0)
+    dt = 1e-4
+    _, chain = _run(pos, r, L, dt, 19 * dt)
+    ref = O.run_direct_solver(pos, r, L, True, dt, 19 * dt, eta_oil=ETA_OIL)
+    assert len(chain) == len(ref)
+    for s, q in zip(chain, ref):
+        np.testing.assert_array_equal(s.radii, q["radii"])
+        np.testing.assert_array_equal(s.get_trajectories(), q["trajectories"])
+
+
+def test_mixed_trajectory_tracks_fp64():
+    pos, r, L = lognormal_state(2000, seed=0)
+    dt = 1e-4
+    _, c64 = _run(pos, r, L, dt, 49 * dt)
+    _, cmx = _run(pos, r, L, dt, 49 * dt, precision="mixed")
+    assert [len(s.radii) for s in c64] == [len(s.radii) for s in cmx]
+    d0 = c64[-1].get_trajectories()[-1] - c64[0].get_trajectories()[0]
+    dm = cmx[-1].get_trajectories()[-1] - cmx[0].get_trajectories()[0]
+    d0 -= L * np.rint(d0 / L)
+    dm -= L * np.rint(dm / L)
+    assert np.linalg.norm(dm - d0) <= 1e-5 * np.linalg.norm(d0)
