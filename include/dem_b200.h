@@ -158,6 +158,52 @@ DEM_API int dem_merge(dem_ctx *ctx, int n, const double *x, const double *y, con
               const int32_t *pairs, const int64_t *num_pairs, double *xo, double *yo, double *zo, double *ro,
               int32_t *n_out, int32_t *merged, void *stream);
 
+/* ---- flat Barnes-Hut octree (reference drop-in, FP64) ------------------ */
+/* Same tree, node numbering, aggregates and walks as FlatOctree
+ * (dem/octree/flat_tree.py:36-1630): bit-identical forces and velocities. */
+typedef struct dem_tree dem_tree;
+
+/* Node pool of max_nodes nodes (the reference sizes it max(4 N / mpl, 1024),
+ * flat_tree.py:63-66) and room for `capacity` particles. */
+DEM_API int dem_tree_create(dem_ctx *ctx, int capacity, int max_nodes, dem_tree **out);
+DEM_API void dem_tree_destroy(dem_tree *tree);
+
+/* FlatOctree.build, flat_tree.py:180-246: level-by-level subdivision of
+ * leaves holding more than mpl droplets (skipped once the pool is full),
+ * leaf slots, next pointers, R^3 aggregates.  Synchronises `stream` once
+ * per level.  DEM_E_CAPACITY when n > capacity (the reference's ValueError,
+ * :184-189). */
+DEM_API int dem_tree_build(dem_tree *tree, int n, const double *x, const double *y, const double *z,
+                           const double *r, double L, int periodic, int mpl, void *stream);
+
+/* _compute_forces_kernel, flat_tree.py:783-894 (MAC s^2 < theta_sq D^2).
+ * The forces are also kept for the velocity walk. */
+DEM_API int dem_tree_forces(dem_tree *tree, double m_const, double theta_sq, double *fx, double *fy, double *fz,
+                            void *stream);
+
+/* Force sums and raw moments bottom-up, flat_tree.py:556-777.  fx == NULL
+ * uses the forces kept by dem_tree_forces (_propagate_forces_from_fields). */
+DEM_API int dem_tree_propagate_forces(dem_tree *tree, const double *fx, const double *fy, const double *fz,
+                                      void *stream);
+
+/* Stokeslet walk (stokes_factor <= 0, flat_tree.py:1000-1280) or total
+ * velocity walk (stokes_factor > 0, :1326-1588), correction off.  fx..fz are
+ * the leaf forces (forces_np); NULL uses the kept forces. */
+DEM_API int dem_tree_velocity(dem_tree *tree, const double *fx, const double *fy, const double *fz, double eta_const,
+                              double theta_sq, double stokes_factor, double *vx, double *vy, double *vz,
+                              void *stream);
+
+/* Host int64[8]: node_count, parent_count, leaf_slot_count, max_nodes,
+ * levels, num_particles, pool_exhausted, capacity. */
+DEM_API int dem_tree_stats(const dem_tree *tree, int64_t *out);
+
+/* Copies node data into DEVICE buffers of node_count entries (NULL skips):
+ * count, first_child, next, leaf_start (int32); r3 (4 per node: R3 sum and
+ * R3-weighted coordinate sums); fs (12 per node: force sum, 9 moments). */
+DEM_API int dem_tree_nodes(dem_tree *tree, int32_t *count, int32_t *first_child, int32_t *next, int32_t *leaf_start,
+                           double *r3, double *fs, void *stream);
+DEM_API int dem_tree_leaf_indices(dem_tree *tree, int32_t *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -29,6 +29,9 @@ namespace dem {
 constexpr int TJ = 128;    // j per shared-memory tile
 constexpr int FLUSH = 64;  // FP32 run length before the compensated fold
 constexpr float RINT_MAGIC = 12582912.0f;  // 1.5 * 2^23: (x + M) - M == rint(x) for |x| < 2^22
+// Pairs with a separation component within MIC_MARGIN * L of L/2 are sent to
+// FP64: FP32 coordinates carry <= ~2^-24 L of rounding, far below this margin.
+constexpr double MIC_MARGIN = 1.0 / 262144.0;  // 2^-18
 
 struct MixedArgs {
     int n;
@@ -64,6 +67,36 @@ __device__ __forceinline__ float mic32(float d, float Ls, float invLs) {
     if (!PER) return d;
     const float u = fmaf(d, invLs, RINT_MAGIC) - RINT_MAGIC;
     return fmaf(-Ls, u, d);
+}
+
+// Separation of a pair in FP32 (scaled units).  Returns true when the pair must
+// be evaluated exactly in FP64 instead:
+//   * near contact: |r_ij| <= k (r_i + r_j) (k folded into ki, kj), which also
+//     catches i == j;
+//   * periodic image ambiguous in FP32: some |d_axis| within MIC_MARGIN * L of
+//     L/2, where FP32 rounding could pick the other image than the reference's
+//     FP64 test |d| > L/2 (the pair term is discontinuous there).
+template <bool PER, bool FORCE>
+__device__ __forceinline__ bool pair_geometry(const float4 &pj, float xi, float yi, float zi, float ki, float kj,
+                                              float Ls, float invLs, float hm, float &dx, float &dy, float &dz,
+                                              float &r2) {
+    if (FORCE) {  // d = x_j - x_i (:229-231)
+        dx = pj.x - xi;
+        dy = pj.y - yi;
+        dz = pj.z - zi;
+    } else {  // d = x_i - x_j (:382-384)
+        dx = xi - pj.x;
+        dy = yi - pj.y;
+        dz = zi - pj.z;
+    }
+    dx = mic32<PER>(dx, Ls, invLs);
+    dy = mic32<PER>(dy, Ls, invLs);
+    dz = mic32<PER>(dz, Ls, invLs);
+    r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    const float sr = ki + kj;
+    bool exact = r2 <= sr * sr;
+    if (PER) exact = exact || fabsf(dx) > hm || fabsf(dy) > hm || fabsf(dz) > hm;
+    return exact;
 }
 
 // FP64 pair terms in scaled units (lengths / ell), reference formulas.
@@ -148,6 +181,7 @@ __global__ void __launch_bounds__(512) mixed_pass_kernel(const MixedArgs a) {
     const double fscale_inv = FORCE ? 1.0 : pow2_inv_of(a.scales[1]);
     const float Ls = (float)(a.L * inv_ell);
     const float invLs = (float)(1.0 / (a.L * inv_ell));
+    const float hm = (float)(a.L * inv_ell * (0.5 - MIC_MARGIN));
 
     float xi[IPT], yi[IPT], zi[IPT], ki[IPT];
     float ax[IPT], ay[IPT], az[IPT], hx[IPT], hy[IPT], hz[IPT], lx[IPT], ly[IPT], lz[IPT];
@@ -207,66 +241,60 @@ __global__ void __launch_bounds__(512) mixed_pass_kernel(const MixedArgs a) {
             const float4 *A = sA[t & 1];
             const float4 *B = sB[t & 1];
             const float *K = sK[t & 1];
-            for (int jj = 0; jj < cnt; ++jj) {
-                const float4 pj = A[jj];
-                float4 fj;
-                float kj;
-                if (FORCE) {
-                    kj = K[jj];
-                } else {
-                    fj = B[jj];
-                    kj = fj.w;
-                }
-                uint32_t nearmask = 0;
-#pragma unroll
-                for (int k = 0; k < IPT; ++k) {
-                    float dx, dy, dz;
-                    if (FORCE) {  // d = x_j - x_i (:229-231)
-                        dx = pj.x - xi[k];
-                        dy = pj.y - yi[k];
-                        dz = pj.z - zi[k];
-                    } else {  // d = x_i - x_j (:382-384)
-                        dx = xi[k] - pj.x;
-                        dy = yi[k] - pj.y;
-                        dz = zi[k] - pj.z;
-                    }
-                    dx = mic32<PER>(dx, Ls, invLs);
-                    dy = mic32<PER>(dy, Ls, invLs);
-                    dz = mic32<PER>(dz, Ls, invLs);
-                    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                    const float sr = ki[k] + kj;
-                    const bool nr = r2 <= sr * sr;
-                    nearmask |= (nr ? 1u : 0u) << k;
-                    float rinv = rsqrtf(r2);
+            for (int jj0 = 0; jj0 < cnt; jj0 += FLUSH) {
+                const int jend = min(jj0 + FLUSH, cnt);
+#pragma unroll 2
+                for (int jj = jj0; jj < jend; ++jj) {
+                    const float4 pj = A[jj];
+                    float4 fj;
+                    float kj;
                     if (FORCE) {
-                        const float rinv2 = rinv * rinv;
-                        const float rinv3 = rinv2 * rinv;
-                        const float rinv4 = rinv2 * rinv2;
-                        const float fac = nr ? 0.f : pj.w * (rinv4 * rinv3);
-                        const float ang = fmaf(5.f * dz, dz, -r2);   // 4dz^2 - dx^2 - dy^2
-                        const float angz = fmaf(-2.f, r2, ang);     // 2dz^2 - 3dx^2 - 3dy^2
-                        const float f = fac * ang;
-                        ax[k] = fmaf(f, dx, ax[k]);
-                        ay[k] = fmaf(f, dy, ay[k]);
-                        az[k] = fmaf(fac * angz, dz, az[k]);
+                        kj = K[jj];
                     } else {
-                        rinv = nr ? 0.f : rinv;
-                        const float rinv2 = rinv * rinv;
-                        const float dot = fmaf(dx, fj.x, fmaf(dy, fj.y, dz * fj.z));
-                        const float sc = dot * rinv2;
-                        ax[k] = fmaf(rinv, fmaf(dx, sc, fj.x), ax[k]);
-                        ay[k] = fmaf(rinv, fmaf(dy, sc, fj.y), ay[k]);
-                        az[k] = fmaf(rinv, fmaf(dz, sc, fj.z), az[k]);
+                        fj = B[jj];
+                        kj = fj.w;
                     }
-                }
-                // near-contact pairs (and i == j): FP64, reference formula
-                if (__any_sync(0xffffffffu, nearmask != 0u)) {
-                    if (nearmask) {
-                        const int j = js + jj;
+                    bool any_exact = false;
 #pragma unroll
-                        for (int k = 0; k < IPT; ++k) {
-                            if ((nearmask >> k) & 1u) {
-                                if (iidx[k] < n) {
+                    for (int k = 0; k < IPT; ++k) {
+                        float dx, dy, dz, r2;
+                        const bool exact = pair_geometry<PER, FORCE>(pj, xi[k], yi[k], zi[k], ki[k], kj, Ls, invLs,
+                                                                      hm, dx, dy, dz, r2);
+                        any_exact |= exact;
+                        float rinv = rsqrtf(r2);
+                        if (FORCE) {
+                            const float rinv2 = rinv * rinv;
+                            const float rinv3 = rinv2 * rinv;
+                            const float rinv4 = rinv2 * rinv2;
+                            const float fac = exact ? 0.f : pj.w * (rinv4 * rinv3);
+                            const float ang = fmaf(5.f * dz, dz, -r2);  // 4dz^2 - dx^2 - dy^2
+                            const float angz = fmaf(-2.f, r2, ang);    // 2dz^2 - 3dx^2 - 3dy^2
+                            const float f = fac * ang;
+                            ax[k] = fmaf(f, dx, ax[k]);
+                            ay[k] = fmaf(f, dy, ay[k]);
+                            az[k] = fmaf(fac * angz, dz, az[k]);
+                        } else {
+                            rinv = exact ? 0.f : rinv;
+                            const float rinv2 = rinv * rinv;
+                            const float dot = fmaf(dx, fj.x, fmaf(dy, fj.y, dz * fj.z));
+                            const float sc = dot * rinv2;
+                            ax[k] = fmaf(rinv, fmaf(dx, sc, fj.x), ax[k]);
+                            ay[k] = fmaf(rinv, fmaf(dy, sc, fj.y), ay[k]);
+                            az[k] = fmaf(rinv, fmaf(dz, sc, fj.z), az[k]);
+                        }
+                    }
+                    // Rare: near-contact pairs, i == j and pairs whose periodic
+                    // image is ambiguous in FP32 are evaluated in FP64 with the
+                    // reference formula (their FP32 term was zeroed above).
+                    if (__any_sync(0xffffffffu, any_exact)) {
+                        if (any_exact) {
+                            const int j = js + jj;
+#pragma unroll
+                            for (int k = 0; k < IPT; ++k) {
+                                float dx, dy, dz, r2;
+                                const bool exact = pair_geometry<PER, FORCE>(pj, xi[k], yi[k], zi[k], ki[k], kj, Ls,
+                                                                              invLs, hm, dx, dy, dz, r2);
+                                if (exact && iidx[k] < n) {
                                     const double3 v = FORCE ? near_force_fp64(iidx[k], j, a, PER ? 1 : 0, inv_ell)
                                                             : near_oseen_fp64(iidx[k], j, a, PER ? 1 : 0, inv_ell,
                                                                               fscale_inv);
@@ -278,14 +306,12 @@ __global__ void __launch_bounds__(512) mixed_pass_kernel(const MixedArgs a) {
                         }
                     }
                 }
-                if ((jj & (FLUSH - 1)) == FLUSH - 1 || jj == cnt - 1) {
 #pragma unroll
-                    for (int k = 0; k < IPT; ++k) {
-                        two_sum_fold(hx[k], lx[k], ax[k]);
-                        two_sum_fold(hy[k], ly[k], ay[k]);
-                        two_sum_fold(hz[k], lz[k], az[k]);
-                        ax[k] = ay[k] = az[k] = 0.f;
-                    }
+                for (int k = 0; k < IPT; ++k) {
+                    two_sum_fold(hx[k], lx[k], ax[k]);
+                    two_sum_fold(hy[k], ly[k], ay[k]);
+                    two_sum_fold(hz[k], lz[k], az[k]);
+                    ax[k] = ay[k] = az[k] = 0.f;
                 }
             }
         }
@@ -405,20 +431,57 @@ struct MixedPlan {
     dim3 grid;
 };
 
-static MixedPlan plan_for(const dem_ctx *ctx, int n) {
+template <bool FORCE>
+static int resident_ctas(int ipt, bool per, int threads) {
+    int occ = 0;
+    const void *f = nullptr;
+#define DEM_K(I) (per ? (const void *)mixed_pass_kernel<I, true, FORCE> : (const void *)mixed_pass_kernel<I, false, FORCE>)
+    switch (ipt) {
+        case 1: f = DEM_K(1); break;
+        case 2: f = DEM_K(2); break;
+        case 8: f = DEM_K(8); break;
+        default: f = DEM_K(4); break;
+    }
+#undef DEM_K
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, f, threads, 0) != cudaSuccess) occ = 1;
+    return occ > 0 ? occ : 1;
+}
+
+// Splits the N x N sum into iblocks x splits CTAs.  With j_splits = 0 the
+// split count is chosen so that the grid fills whole waves of the resident
+// CTA slots (all CTAs do the same work, so a partial last wave idles SMs).
+template <bool FORCE>
+static MixedPlan plan_for(const dem_ctx *ctx, int n, bool per) {
     MixedPlan p;
     p.ipt = ctx->tuning.i_per_thread;
     p.threads = ctx->tuning.threads;
     const int per_cta = p.threads * p.ipt;
     const int iblocks = ceil_div(n, per_cta);
+    const int max_splits = ceil_div(n, TJ);
+    auto actual = [&](int s) {
+        s = s < 1 ? 1 : (s > max_splits ? max_splits : s);
+        const int chunk = ceil_div(ceil_div(n, s), TJ) * TJ;
+        return ceil_div(n, chunk);
+    };
     int splits = ctx->tuning.j_splits;
     if (splits <= 0) {
-        const int target = 4 * ctx->sm_count;  // CTAs in flight
-        splits = (target + iblocks - 1) / iblocks;
+        const int slots = resident_ctas<FORCE>(p.ipt, per, p.threads) * ctx->sm_count;
+        const int s0 = actual((slots + iblocks - 1) / iblocks);
+        double best = -1.0;
+        splits = s0;
+        for (int s = s0; s <= 8 * s0 && s <= max_splits; ++s) {
+            const int sa = actual(s);
+            if (sa != s) continue;
+            const double waves = (double)iblocks * sa / slots;
+            const double eff = waves / std::ceil(waves);
+            if (eff > best + 1e-9) {
+                best = eff;
+                splits = sa;
+            }
+            if (eff > 0.97) break;
+        }
     }
-    const int max_splits = ceil_div(n, TJ);
-    if (splits > max_splits) splits = max_splits;
-    if (splits < 1) splits = 1;
+    splits = actual(splits);
     p.j_chunk = ceil_div(ceil_div(n, splits), TJ) * TJ;
     p.splits = ceil_div(n, p.j_chunk);
     p.grid = dim3(iblocks, p.splits, 1);
@@ -428,7 +491,7 @@ static MixedPlan plan_for(const dem_ctx *ctx, int n) {
 int launch_direct_forces_mixed(dem_ctx *ctx, int n, const double *x, const double *y, const double *z,
                                const double *r, double m_const, double L, int periodic, double *fx, double *fy,
                                double *fz, cudaStream_t s) {
-    const MixedPlan p = plan_for(ctx, n);
+    const MixedPlan p = plan_for<true>(ctx, n, periodic != 0);
     int rc = dem_ensure_partials(ctx, p.splits);
     if (rc) return rc;
     unsigned long long *scales = reinterpret_cast<unsigned long long *>(ctx->dscratch);
@@ -467,7 +530,7 @@ int launch_direct_forces_mixed(dem_ctx *ctx, int n, const double *x, const doubl
 int launch_direct_convection_mixed(dem_ctx *ctx, int n, const double *x, const double *y, const double *z,
                                    const double *r, const double *fx, const double *fy, const double *fz, double eta,
                                    double L, int periodic, double *vx, double *vy, double *vz, cudaStream_t s) {
-    const MixedPlan p = plan_for(ctx, n);
+    const MixedPlan p = plan_for<false>(ctx, n, periodic != 0);
     int rc = dem_ensure_partials(ctx, p.splits);
     if (rc) return rc;
     unsigned long long *scales = reinterpret_cast<unsigned long long *>(ctx->dscratch);

@@ -55,6 +55,15 @@ SIGNATURES = {
     "dem_euler_update_total": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _d, _d, _i, _vp, _vp, _vp, _vp]),
     "dem_hash_detect": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _d, _i, _i, _vp, _i64, _vp, _vp]),
     "dem_merge": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "dem_tree_create": (_i, [_vp, _i, _i, C.POINTER(_vp)]),
+    "dem_tree_destroy": (None, [_vp]),
+    "dem_tree_build": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _d, _i, _i, _vp]),
+    "dem_tree_forces": (_i, [_vp, _d, _d, _vp, _vp, _vp, _vp]),
+    "dem_tree_propagate_forces": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "dem_tree_velocity": (_i, [_vp, _vp, _vp, _vp, _d, _d, _d, _vp, _vp, _vp, _vp]),
+    "dem_tree_stats": (_i, [_vp, C.POINTER(_i64)]),
+    "dem_tree_nodes": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "dem_tree_leaf_indices": (_i, [_vp, _vp, _vp]),
 }
 
 _lib = None
@@ -243,6 +252,59 @@ class Context:
                             self.stream()),
             "merge",
         )
+
+
+class Tree:
+    """One ``dem_tree`` (FP64 flat octree) owned by a Context."""
+
+    def __init__(self, ctx: Context, capacity: int, max_nodes: int):
+        self.ctx = ctx
+        self.capacity = int(capacity)
+        self.max_nodes = int(max_nodes)
+        self.handle = _vp()
+        ctx._check(lib().dem_tree_create(ctx.handle, self.capacity, self.max_nodes, C.byref(self.handle)),
+                   "tree_create")
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value and _lib is not None:
+            try:
+                _lib.dem_tree_destroy(h)
+            except Exception:  # pragma: no cover
+                pass
+            self.handle = None
+
+    def build(self, n, pos, r, L, periodic, mpl):
+        self.ctx._check(lib().dem_tree_build(self.handle, n, ptr(pos[0]), ptr(pos[1]), ptr(pos[2]), ptr(r), float(L),
+                                             int(bool(periodic)), int(mpl), self.ctx.stream()), "tree_build")
+
+    def forces(self, m_const, theta_sq, out):
+        self.ctx._check(lib().dem_tree_forces(self.handle, float(m_const), float(theta_sq), ptr(out[0]), ptr(out[1]),
+                                              ptr(out[2]), self.ctx.stream()), "tree_forces")
+
+    def propagate_forces(self, F=None):
+        a = (None, None, None) if F is None else (ptr(F[0]), ptr(F[1]), ptr(F[2]))
+        self.ctx._check(lib().dem_tree_propagate_forces(self.handle, *a, self.ctx.stream()), "tree_propagate")
+
+    def velocity(self, F, eta_const, theta_sq, stokes_factor, out):
+        a = (None, None, None) if F is None else (ptr(F[0]), ptr(F[1]), ptr(F[2]))
+        self.ctx._check(lib().dem_tree_velocity(self.handle, *a, float(eta_const), float(theta_sq),
+                                                float(stokes_factor), ptr(out[0]), ptr(out[1]), ptr(out[2]),
+                                                self.ctx.stream()), "tree_velocity")
+
+    def stats(self):
+        out = (_i64 * 8)()
+        self.ctx._check(lib().dem_tree_stats(self.handle, out), "tree_stats")
+        keys = ("node_count", "parent_count", "leaf_slot_count", "max_nodes", "n_levels", "num_particles",
+                "pool_exhausted", "capacity")
+        return {k: int(v) for k, v in zip(keys, out)}
+
+    def nodes(self, count=None, first_child=None, next_=None, leaf_start=None, r3=None, fs=None):
+        self.ctx._check(lib().dem_tree_nodes(self.handle, ptr(count), ptr(first_child), ptr(next_), ptr(leaf_start),
+                                             ptr(r3), ptr(fs), self.ctx.stream()), "tree_nodes")
+
+    def leaf_indices(self, out):
+        self.ctx._check(lib().dem_tree_leaf_indices(self.handle, ptr(out), self.ctx.stream()), "tree_leaf_indices")
 
 
 class Buffers:
