@@ -22,7 +22,8 @@
 #include "scan.cuh"
 
 struct dem_tree {
-    dem_ctx *ctx = nullptr;
+    dem_ctx *ctx = nullptr;  // must outlive the tree while kernels run; destroy does not touch it
+    int device = 0;
     int cap = 0, max_nodes = 0;
     int n = 0, node_count = 0, parent_count = 0, leaf_slot_count = 0, pool_exhausted = 0;
     double L = 0;
@@ -622,6 +623,7 @@ int dem_tree_create(dem_ctx *ctx, int capacity, int max_nodes, dem_tree **out) {
     *out = nullptr;
     dem_tree *t = new dem_tree();
     t->ctx = ctx;
+    t->device = ctx->device;
     t->cap = capacity;
     t->max_nodes = max_nodes;
     const size_t M = (size_t)max_nodes, N = (size_t)capacity;
@@ -662,7 +664,7 @@ int dem_tree_create(dem_ctx *ctx, int capacity, int max_nodes, dem_tree **out) {
 
 void dem_tree_destroy(dem_tree *t) {
     if (!t) return;
-    cudaSetDevice(t->ctx->device);
+    cudaSetDevice(t->device);
     tree_free(t);
     delete t;
 }

@@ -10,6 +10,8 @@ bit-identical to the reference's expressions in IEEE binary64.
 
 from __future__ import annotations
 
+import weakref
+
 import numpy as np
 
 from .. import _native as N
@@ -50,15 +52,15 @@ class OctreeNode:
     """Node arrays of the tree (dem/octree/octree_node.py:12-154), read-only views."""
 
     def __init__(self, tree: "FlatOctree", max_nodes: int):
-        self._tree = tree
+        ref = weakref.ref(tree)  # no reference cycle: the native handles are released in order
         self.max_nodes = max_nodes
         for name in _FIELDS_I32:
-            setattr(self, name, _Field(lambda name=name: tree._node_array(name)))
+            setattr(self, name, _Field(lambda name=name: ref()._node_array(name)))
         for k, name in enumerate(("R3_sum", "R3_cx", "R3_cy", "R3_cz")):
-            setattr(self, name, _Field(lambda k=k: tree._node_array("r3")[:, k]))
+            setattr(self, name, _Field(lambda k=k: ref()._node_array("r3")[:, k]))
         for k, name in enumerate(("force_sum_x", "force_sum_y", "force_sum_z", "fmom_xx", "fmom_xy", "fmom_xz",
                                   "fmom_yx", "fmom_yy", "fmom_yz", "fmom_zx", "fmom_zy", "fmom_zz")):
-            setattr(self, name, _Field(lambda k=k: tree._node_array("fs")[:, k]))
+            setattr(self, name, _Field(lambda k=k: ref()._node_array("fs")[:, k]))
 
 
 class FlatOctree:
@@ -79,25 +81,27 @@ class FlatOctree:
         self._L = 0.0
         self._periodic = 0
         self._theta_sq = theta * theta
-        self.theta_sq = _Scalar(lambda: self._theta_sq, self._set_theta_sq)
-        self.mpl_field = _Scalar(lambda: self.mpl, self._set_mpl)
-        self.node_count = _Scalar(lambda: self._tree.stats()["node_count"])
-        self.parent_count = _Scalar(lambda: self._tree.stats()["parent_count"])
-        self.leaf_slot_count = _Scalar(lambda: self._tree.stats()["leaf_slot_count"])
-        self.num_particles = _Scalar(lambda: self._n)
-        self.L = _Scalar(lambda: self._L)
-        self.periodic = _Scalar(lambda: self._periodic)
+        me = weakref.ref(self)  # field views must not keep the tree alive (no reference cycles)
+
+        def _set_theta_sq(v):
+            me()._theta_sq = float(v)
+
+        def _set_mpl(v):
+            me().mpl = int(v)
+
+        self.theta_sq = _Scalar(lambda: me()._theta_sq, _set_theta_sq)
+        self.mpl_field = _Scalar(lambda: me().mpl, _set_mpl)
+        self.node_count = _Scalar(lambda: me()._tree.stats()["node_count"])
+        self.parent_count = _Scalar(lambda: me()._tree.stats()["parent_count"])
+        self.leaf_slot_count = _Scalar(lambda: me()._tree.stats()["leaf_slot_count"])
+        self.num_particles = _Scalar(lambda: me()._n)
+        self.L = _Scalar(lambda: me()._L)
+        self.periodic = _Scalar(lambda: me()._periodic)
         self.nodes = OctreeNode(self, max_nodes)
-        self.leaf_indices = _Field(self._leaf_indices)
+        self.leaf_indices = _Field(lambda: me()._leaf_indices())
         self._F = None  # device SoA forces of the last force walk
 
     # -- parameters (flat_tree.py:169-174) ------------------------------------
-    def _set_theta_sq(self, v):
-        self._theta_sq = float(v)
-
-    def _set_mpl(self, v):
-        self.mpl = int(v)
-
     def update_params(self, theta: float, mpl: int) -> None:
         self.theta = theta
         self.mpl = mpl
