@@ -145,6 +145,25 @@ DEM_API int dem_hash_detect(dem_ctx *ctx, int n, const double *x, const double *
                     double L, int periodic, int table_size, int32_t *pairs, int64_t pair_capacity, int64_t *counts,
                     void *stream);
 
+/* Allocation-free spatial-hash detection.  This entry point has no
+ * counterpart in the reference: it is for callers that cannot call
+ * cudaMalloc when they detect collisions (a fixed device-memory budget handed
+ * over up front, a control loop that must not take cudaMalloc's device-wide
+ * synchronisation between steps, or an allocator owned by another
+ * component).  Same arguments, semantics and pair output as dem_hash_detect,
+ * without a context: the workspace is a fixed device array inside the
+ * library (about 2.9 MB, held on every GPU that loads the library until the
+ * process exits).  Limits: n <= 65536 droplets and table_size <= 131072
+ * buckets; larger sizes return DEM_E_CAPACITY; bad pointers DEM_E_INVALID;
+ * CUDA failures DEM_E_CUDA (no message: there is no context).  The first call
+ * on a device looks up the array's device address (cudaGetSymbolAddress) with
+ * that device current; make that first call before any stream capture.  All
+ * calls share the one array: calls that overlap on the GPU (different streams
+ * or host threads at the same time) race and corrupt each other's results. */
+DEM_API int dem_hash_detect_noalloc(int n, const double *x, const double *y, const double *z, const double *r,
+                                    double L, int periodic, int table_size, int32_t *pairs, int64_t pair_capacity,
+                                    int64_t *counts, void *stream);
+
 /* ---- coalescence ------------------------------------------------------ */
 /* Greedy merge of the colliding pairs in (i, j) order; survivors keep their
  * order and the merged droplets are appended in pair order.

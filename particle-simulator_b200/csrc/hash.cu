@@ -258,3 +258,123 @@ int launch_hash_detect(dem_ctx *ctx, int n, const double *x, const double *y, co
 }
 
 }  // namespace dem
+
+// ===========================================================================
+// Allocation-free variant of the spatial-hash detector.
+//
+// Some callers cannot call cudaMalloc at the time they detect collisions: a
+// host application that hands the library a fixed device-memory budget up
+// front and forbids later allocations, a control loop that must not take the
+// device-wide synchronisation and latency jitter of cudaMalloc/cudaFree
+// between steps, or code that runs while another component owns the CUDA
+// allocator.  For them dem_hash_detect_noalloc needs no context and allocates
+// nothing: its workspace (bucket table, per-droplet hashes, bucket members,
+// per-droplet pair counts and offsets, scan totals) is the file-scope device
+// array below, sized for at most NOALLOC_MAX_N droplets and a hash table of at
+// most NOALLOC_MAX_TABLE buckets.  Every GPU that loads the library keeps this
+// array (about 2.9 MB) until the process exits.
+// ===========================================================================
+#include <mutex>
+
+namespace dem {
+
+constexpr int NOALLOC_MAX_N = 65536;
+constexpr int NOALLOC_MAX_TABLE = 131072;  // next power of two >= 2 * NOALLOC_MAX_N
+constexpr int NOALLOC_MAX_DEVICES = 64;
+
+constexpr size_t na_align(size_t b) { return (b + 255) & ~size_t(255); }
+constexpr size_t NA_CELL = 0;                                                      // int32[MAX_N]
+constexpr size_t NA_SORTED = NA_CELL + na_align(sizeof(int32_t) * NOALLOC_MAX_N);    // int32[MAX_N]
+constexpr size_t NA_PCOUNT = NA_SORTED + na_align(sizeof(int32_t) * NOALLOC_MAX_N);  // int32[MAX_N + 1]
+constexpr size_t NA_POFF = NA_PCOUNT + na_align(sizeof(int32_t) * (NOALLOC_MAX_N + 1));       // int64[MAX_N + 1]
+constexpr size_t NA_BCOUNT = NA_POFF + na_align(sizeof(int64_t) * (NOALLOC_MAX_N + 1));       // int32[MAX_TABLE]
+constexpr size_t NA_BSTART = NA_BCOUNT + na_align(sizeof(int32_t) * NOALLOC_MAX_TABLE);       // int32[MAX_TABLE + 1]
+constexpr size_t NA_BCURSOR = NA_BSTART + na_align(sizeof(int32_t) * (NOALLOC_MAX_TABLE + 1));  // int32[MAX_TABLE]
+constexpr size_t NA_SUMS = NA_BCURSOR + na_align(sizeof(int32_t) * NOALLOC_MAX_TABLE);  // int64[SCAN_MAX_BLOCKS + 1]
+constexpr size_t NA_MISC = NA_SUMS + na_align(sizeof(int64_t) * (SCAN_MAX_BLOCKS + 1));  // max slot, params, err
+constexpr size_t NA_BYTES = NA_MISC + 256;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
+
+struct NoallocDevice {
+    unsigned char *scratch = nullptr;  // device address of g_noalloc_scratch on this device
+    int sm_count = 0;
+};
+static NoallocDevice g_noalloc_dev[NOALLOC_MAX_DEVICES];
+static std::mutex g_noalloc_mutex;
+
+// Once per device, with that device current: the device address of the array.
+// (In host code g_noalloc_scratch names a host-side stand-in, not device memory.)
+static int noalloc_setup(NoallocDevice &out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return DEM_E_CUDA;
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return DEM_E_INVALID;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    NoallocDevice &d = g_noalloc_dev[dev];
+    if (!d.scratch) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return DEM_E_CUDA;
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return DEM_E_CUDA;
+        d.sm_count = sms > 0 ? sms : 1;
+        d.scratch = static_cast<unsigned char *>(p);
+    }
+    out = d;
+    return DEM_OK;
+}
+
+}  // namespace dem
+
+extern "C" int dem_hash_detect_noalloc(int n, const double *x, const double *y, const double *z, const double *r,
+                                       double L, int periodic, int table_size, int32_t *pairs,
+                                       int64_t pair_capacity, int64_t *counts, void *stream) {
+    using namespace dem;
+    if (n < 0 || n > NOALLOC_MAX_N) return DEM_E_CAPACITY;
+    if (table_size < 1 || table_size > NOALLOC_MAX_TABLE || (table_size & (table_size - 1))) return DEM_E_CAPACITY;
+    if (!counts || pair_capacity < 0 || (pair_capacity > 0 && !pairs)) return DEM_E_INVALID;
+    if (n > 0 && (!x || !y || !z || !r)) return DEM_E_INVALID;
+    NoallocDevice d;
+    int rc = noalloc_setup(d);
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned char *base = d.scratch;
+    int32_t *cell_hash = reinterpret_cast<int32_t *>(base + NA_CELL);
+    int32_t *sorted_idx = reinterpret_cast<int32_t *>(base + NA_SORTED);
+    int32_t *pair_count = reinterpret_cast<int32_t *>(base + NA_PCOUNT);
+    int64_t *pair_offset = reinterpret_cast<int64_t *>(base + NA_POFF);
+    int32_t *bucket_count = reinterpret_cast<int32_t *>(base + NA_BCOUNT);
+    int32_t *bucket_start = reinterpret_cast<int32_t *>(base + NA_BSTART);
+    int32_t *bucket_cursor = reinterpret_cast<int32_t *>(base + NA_BCURSOR);
+    void *sums = base + NA_SUMS;
+    unsigned long long *slot = reinterpret_cast<unsigned long long *>(base + NA_MISC);
+    HashParams *hp = reinterpret_cast<HashParams *>(base + NA_MISC + 16);
+    uint32_t *err = reinterpret_cast<uint32_t *>(base + NA_MISC + 64);
+    const int32_t mask = table_size - 1;
+    const int grid = max(1, min(ceil_div(n, 256), 8 * d.sm_count));
+    // the array keeps the previous call's contents: reset what must start at zero
+    if (cudaMemsetAsync(base + NA_MISC, 0, 256, s) != cudaSuccess) return DEM_E_CUDA;
+    if (cudaMemsetAsync(counts, 0, 2 * sizeof(int64_t), s) != cudaSuccess) return DEM_E_CUDA;
+    if (cudaMemsetAsync(bucket_count, 0, sizeof(int32_t) * table_size, s) != cudaSuccess) return DEM_E_CUDA;
+    if (n == 0) return DEM_OK;
+    max_kernel<<<grid, 256, 0, s>>>(n, r, slot);
+    hash_params_kernel<<<1, 1, 0, s>>>(slot, L, hp);
+    assign_kernel<<<grid, 256, 0, s>>>(n, x, y, z, hp, periodic, mask, cell_hash, bucket_count);
+    if (cudaGetLastError() != cudaSuccess) return DEM_E_CUDA;
+    if (exclusive_scan_into<int32_t, int32_t>(bucket_count, bucket_start, table_size, static_cast<int32_t *>(sums),
+                                              s) != cudaSuccess)
+        return DEM_E_CUDA;
+    if (cudaMemcpyAsync(bucket_cursor, bucket_start, sizeof(int32_t) * table_size, cudaMemcpyDeviceToDevice, s) !=
+        cudaSuccess)
+        return DEM_E_CUDA;
+    scatter_kernel<<<grid, 256, 0, s>>>(n, cell_hash, hp, bucket_cursor, sorted_idx);
+    const int dgrid = ceil_div(n, 128);
+    count_pairs_kernel<<<dgrid, 128, 0, s>>>(n, x, y, z, r, hp, periodic, L, mask, bucket_start, sorted_idx,
+                                             pair_count, reinterpret_cast<unsigned long long *>(counts + 1));
+    if (cudaGetLastError() != cudaSuccess) return DEM_E_CUDA;
+    if (exclusive_scan_into<int32_t, int64_t>(pair_count, pair_offset, n, static_cast<int64_t *>(sums), s) !=
+        cudaSuccess)
+        return DEM_E_CUDA;
+    write_pairs_kernel<<<dgrid, 128, 0, s>>>(n, x, y, z, r, hp, periodic, L, mask, bucket_start, sorted_idx,
+                                             pair_offset, pairs, pair_capacity, counts, err);
+    return cudaGetLastError() == cudaSuccess ? DEM_OK : DEM_E_CUDA;
+}

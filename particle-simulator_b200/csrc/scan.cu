@@ -113,6 +113,22 @@ int exclusive_scan(dem_ctx *ctx, const TIn *in, TOut *out, int64_t n, cudaStream
     return dem_check_launch(ctx, "exclusive_scan");
 }
 
+template <typename TIn, typename TOut>
+cudaError_t exclusive_scan_into(const TIn *in, TOut *out, int64_t n, TOut *sums, cudaStream_t s) {
+    const int64_t nb64 = n > 0 ? (n + SCAN_TILE - 1) / SCAN_TILE : 1;
+    if (nb64 > SCAN_MAX_BLOCKS) return cudaErrorInvalidValue;
+    const int nb = (int)nb64;
+    scan_block_totals<TIn, TOut><<<nb, SCAN_THREADS, 0, s>>>(in, n, sums);
+    scan_totals<TOut><<<1, 1024, 0, s>>>(sums, nb);
+    scan_apply<TIn, TOut><<<nb, SCAN_THREADS, 0, s>>>(in, n, sums, out);
+    return cudaGetLastError();
+}
+
+template cudaError_t exclusive_scan_into<int32_t, int32_t>(const int32_t *, int32_t *, int64_t, int32_t *,
+                                                            cudaStream_t);
+template cudaError_t exclusive_scan_into<int32_t, int64_t>(const int32_t *, int64_t *, int64_t, int64_t *,
+                                                            cudaStream_t);
+
 template int exclusive_scan<int32_t, int32_t>(dem_ctx *, const int32_t *, int32_t *, int64_t, cudaStream_t);
 template int exclusive_scan<int32_t, int64_t>(dem_ctx *, const int32_t *, int64_t *, int64_t, cudaStream_t);
 template int exclusive_scan<uint8_t, int32_t>(dem_ctx *, const uint8_t *, int32_t *, int64_t, cudaStream_t);

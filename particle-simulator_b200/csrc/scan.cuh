@@ -16,4 +16,9 @@ constexpr int SCAN_MAX_BLOCKS = 1024 * 8;             // => up to 33.5M elements
 template <typename TIn, typename TOut>
 int exclusive_scan(dem_ctx *ctx, const TIn *in, TOut *out, int64_t n, cudaStream_t s);
 
+// Same scan with a caller-provided workspace of SCAN_MAX_BLOCKS + 1 TOut
+// values (no context, no allocation).  Returns a cudaError_t value.
+template <typename TIn, typename TOut>
+cudaError_t exclusive_scan_into(const TIn *in, TOut *out, int64_t n, TOut *sums, cudaStream_t s);
+
 }  // namespace dem

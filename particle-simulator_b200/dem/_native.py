@@ -54,6 +54,7 @@ SIGNATURES = {
     "dem_euler_update": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _d, _d, _d, _i, _vp, _vp, _vp, _vp]),
     "dem_euler_update_total": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _d, _d, _i, _vp, _vp, _vp, _vp]),
     "dem_hash_detect": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _d, _i, _i, _vp, _i64, _vp, _vp]),
+    "dem_hash_detect_noalloc": (_i, [_i, _vp, _vp, _vp, _vp, _d, _i, _i, _vp, _i64, _vp, _vp]),
     "dem_merge": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "dem_tree_create": (_i, [_vp, _i, _i, C.POINTER(_vp)]),
     "dem_tree_destroy": (None, [_vp]),
