@@ -78,16 +78,23 @@ DEM_API int dem_profile_enable(dem_ctx *ctx, int enable);
 DEM_API int dem_profile_read(dem_ctx *ctx, const char *name, double *total_ms, int *launches);
 DEM_API int dem_profile_reset(dem_ctx *ctx);
 
+/* schedules of the mixed-precision direct passes */
+#define DEM_SCHED_AUTO 0      /* symmetric when its partial sums fit, else split */
+#define DEM_SCHED_SPLIT 1     /* every ordered pair; the j range split in chunks */
+#define DEM_SCHED_SYMMETRIC 2 /* every unordered pair once (F_ji = -F_ij, Oseen tensor even) */
+
 /* Tuning of the mixed-precision direct kernels (0 keeps the current value).
- *   i_per_thread  i-particles register-blocked per thread (1, 2, 4 or 8)
- *   threads       threads per CTA (64..512, multiple of 32)
- *   j_splits      number of j-chunks the N^2 sum is split into (>=1; 0 = auto)
+ *   i_per_thread  i-particles register-blocked per thread (1, 2, 4 or 8;
+ *                 the symmetric schedule uses 1, 2 or 4)
+ *   threads       threads per CTA of the split schedule (64..512, multiple of 32)
+ *   j_splits      number of j-chunks of the split schedule (>=1; 0 = auto)
  *   near_force    FP64 radius factor k: pairs with |r_ij| <= k (r_i + r_j) are
- *   near_oseen    computed in FP64 (force / convection pass) */
+ *   near_oseen    computed in FP64 (force / convection pass)
+ *   schedule      DEM_SCHED_* (this one is always applied) */
 DEM_API int dem_direct_set_tuning(dem_ctx *ctx, int i_per_thread, int threads, int j_splits, double near_force,
-                          double near_oseen);
+                                  double near_oseen, int schedule);
 DEM_API int dem_direct_get_tuning(const dem_ctx *ctx, int *i_per_thread, int *threads, int *j_splits,
-                          double *near_force, double *near_oseen);
+                                  double *near_force, double *near_oseen, int *schedule);
 
 /* ---- layout ---------------------------------------------------------- */
 /* (n, 3) row-major <-> three component arrays.  The reference's public

@@ -20,6 +20,7 @@ struct dem_mixed_tuning {
     int j_splits = 0;  // 0: choose from the SM count
     double near_force = 5.0;
     double near_oseen = 3.0;
+    int schedule = 0;  // DEM_SCHED_AUTO / DEM_SCHED_SPLIT / DEM_SCHED_SYMMETRIC
 };
 
 struct dem_prof_rec {
@@ -45,6 +46,8 @@ struct dem_ctx {
     float4 *pack_a = nullptr;   // mixed: (x, y, z, r^3) or (x, y, z, -) scaled, per particle
     float4 *pack_b = nullptr;   // mixed: (Fx, Fy, Fz, k r) scaled, per particle
     double *partial = nullptr;  // mixed: [splits][3][capacity] chunk partial sums
+    double *sym_partial = nullptr;  // mixed, symmetric schedule: per block-pair partial sums
+    size_t sym_partial_bytes = 0;
     int partial_splits = 0;
     double *dscratch = nullptr;     // 8 doubles: reductions (max radius, ...)
     int32_t *cell_hash = nullptr;   // hash bucket per particle
@@ -68,6 +71,7 @@ int dem_check_cuda(dem_ctx *ctx, cudaError_t e, const char *where);
 int dem_check_launch(dem_ctx *ctx, const char *where);
 int dem_ensure_table(dem_ctx *ctx, int64_t table_size);
 int dem_ensure_partials(dem_ctx *ctx, int splits);
+int dem_ensure_sym_partials(dem_ctx *ctx, size_t bytes);
 // Records a CUDA event before/after a kernel launch when profiling is on.
 void dem_prof_begin(dem_ctx *ctx, const char *name, cudaStream_t s);
 void dem_prof_end(dem_ctx *ctx, cudaStream_t s);

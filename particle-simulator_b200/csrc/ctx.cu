@@ -43,6 +43,15 @@ int dem_ensure_partials(dem_ctx *ctx, int splits) {
     return DEM_OK;
 }
 
+int dem_ensure_sym_partials(dem_ctx *ctx, size_t bytes) {
+    if (bytes <= ctx->sym_partial_bytes) return DEM_OK;
+    ctx->sym_partial_bytes = 0;
+    int rc = grow(ctx, &ctx->sym_partial, bytes / sizeof(double) + 1, "symmetric partial sums");
+    if (rc) return rc;
+    ctx->sym_partial_bytes = bytes;
+    return DEM_OK;
+}
+
 static cudaEvent_t prof_event(dem_ctx *ctx) {
     if (!ctx->prof_pool.empty()) {
         cudaEvent_t e = ctx->prof_pool.back();
@@ -163,7 +172,7 @@ void dem_ctx_destroy(dem_ctx *ctx) {
     void *ptrs[] = {ctx->d_err,         ctx->pack_a,      ctx->pack_b,     ctx->partial,    ctx->dscratch,
                     ctx->cell_hash,     ctx->bucket_count, ctx->bucket_start, ctx->bucket_cursor, ctx->sorted_idx,
                     ctx->pair_count,    ctx->pair_offset, ctx->flags,      ctx->keep_off,   ctx->merged_buf,
-                    ctx->merged_cnt,    ctx->scan_tmp};
+                    ctx->merged_cnt,    ctx->scan_tmp,    ctx->sym_partial};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     prof_clear(ctx);
@@ -186,7 +195,7 @@ int dem_device_errors(dem_ctx *ctx, uint32_t *flags_host, void *stream) {
 }
 
 int dem_direct_set_tuning(dem_ctx *ctx, int i_per_thread, int threads, int j_splits, double near_force,
-                          double near_oseen) {
+                          double near_oseen, int schedule) {
     if (!ctx) return DEM_E_INVALID;
     if (i_per_thread) {
         if (i_per_thread != 1 && i_per_thread != 2 && i_per_thread != 4 && i_per_thread != 8)
@@ -202,17 +211,21 @@ int dem_direct_set_tuning(dem_ctx *ctx, int i_per_thread, int threads, int j_spl
     ctx->tuning.j_splits = j_splits;
     if (near_force > 0) ctx->tuning.near_force = near_force;
     if (near_oseen > 0) ctx->tuning.near_oseen = near_oseen;
+    if (schedule < DEM_SCHED_AUTO || schedule > DEM_SCHED_SYMMETRIC)
+        return dem_set_error(ctx, DEM_E_INVALID, "unknown schedule");
+    ctx->tuning.schedule = schedule;
     return DEM_OK;
 }
 
 int dem_direct_get_tuning(const dem_ctx *ctx, int *i_per_thread, int *threads, int *j_splits, double *near_force,
-                          double *near_oseen) {
+                          double *near_oseen, int *schedule) {
     if (!ctx) return DEM_E_INVALID;
     if (i_per_thread) *i_per_thread = ctx->tuning.i_per_thread;
     if (threads) *threads = ctx->tuning.threads;
     if (j_splits) *j_splits = ctx->tuning.j_splits;
     if (near_force) *near_force = ctx->tuning.near_force;
     if (near_oseen) *near_oseen = ctx->tuning.near_oseen;
+    if (schedule) *schedule = ctx->tuning.schedule;
     return DEM_OK;
 }
 

@@ -27,6 +27,11 @@ PREC_FP64 = 0
 PREC_MIXED = 1
 PRECISIONS = {"fp64": PREC_FP64, "mixed": PREC_MIXED}
 
+SCHED_AUTO = 0
+SCHED_SPLIT = 1
+SCHED_SYMMETRIC = 2
+SCHEDULES = {"auto": SCHED_AUTO, "split": SCHED_SPLIT, "symmetric": SCHED_SYMMETRIC}
+
 DEVERR_WAIT_TIMEOUT = 1
 DEVERR_PAIR_OVERFLOW = 2
 DEVERR_NODE_OVERFLOW = 4
@@ -45,8 +50,9 @@ SIGNATURES = {
     "dem_profile_enable": (_i, [_vp, _i]),
     "dem_profile_read": (_i, [_vp, C.c_char_p, C.POINTER(_d), C.POINTER(_i)]),
     "dem_profile_reset": (_i, [_vp]),
-    "dem_direct_set_tuning": (_i, [_vp, _i, _i, _i, _d, _d]),
-    "dem_direct_get_tuning": (_i, [_vp, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i), C.POINTER(_d), C.POINTER(_d)]),
+    "dem_direct_set_tuning": (_i, [_vp, _i, _i, _i, _d, _d, _i]),
+    "dem_direct_get_tuning": (_i, [_vp, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i), C.POINTER(_d), C.POINTER(_d),
+                                   C.POINTER(_i)]),
     "dem_aos_to_soa": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp]),
     "dem_soa_to_aos": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp]),
     "dem_direct_forces": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _d, _d, _i, _i, _vp, _vp, _vp, _vp]),
@@ -183,19 +189,26 @@ class Context:
         self._check(lib().dem_profile_reset(self.handle), "profile_reset")
 
     # -- tuning -------------------------------------------------------------
-    def set_tuning(self, i_per_thread=0, threads=0, j_splits=0, near_force=0.0, near_oseen=0.0):
+    def set_tuning(self, i_per_thread=0, threads=0, j_splits=None, near_force=0.0, near_oseen=0.0, schedule=None):
+        cur = self.get_tuning()
+        if j_splits is None:
+            j_splits = cur["j_splits"]
+        if schedule is None:
+            schedule = cur["schedule"]
+        schedule = SCHEDULES.get(schedule, schedule)
         self._check(
             lib().dem_direct_set_tuning(self.handle, int(i_per_thread), int(threads), int(j_splits),
-                                        float(near_force), float(near_oseen)),
+                                        float(near_force), float(near_oseen), int(schedule)),
             "set_tuning",
         )
 
     def get_tuning(self):
-        a, b, c = _i(), _i(), _i()
+        a, b, c, g = _i(), _i(), _i(), _i()
         d, e = _d(), _d()
-        self._check(lib().dem_direct_get_tuning(self.handle, C.byref(a), C.byref(b), C.byref(c), C.byref(d), C.byref(e)),
-                    "get_tuning")
-        return dict(i_per_thread=a.value, threads=b.value, j_splits=c.value, near_force=d.value, near_oseen=e.value)
+        self._check(lib().dem_direct_get_tuning(self.handle, C.byref(a), C.byref(b), C.byref(c), C.byref(d), C.byref(e),
+                                                C.byref(g)), "get_tuning")
+        return dict(i_per_thread=a.value, threads=b.value, j_splits=c.value, near_force=d.value, near_oseen=e.value,
+                    schedule=g.value)
 
     # -- thin wrappers over the C ABI (torch CUDA tensors in, no allocation) --
     def aos_to_soa(self, n, aos, soa):

@@ -78,12 +78,15 @@ def test_mixed_against_fp64_oracle(n, seed):
     assert ref_metric(V, V_ref)[1] <= MIXED_V_PER_DROPLET_TOL
 
 
-@pytest.mark.parametrize("ipt,threads,splits", [(1, 128, 0), (2, 256, 3), (4, 64, 1), (8, 128, 0), (4, 512, 7)])
-def test_mixed_tunings_agree_and_are_deterministic(ipt, threads, splits):
+@pytest.mark.parametrize("ipt,threads,splits,schedule", [
+    (1, 128, 0, "split"), (2, 256, 3, "split"), (4, 64, 1, "split"), (8, 128, 0, "split"), (4, 512, 7, "split"),
+    (1, 0, 0, "symmetric"), (2, 0, 0, "symmetric"), (4, 0, 0, "symmetric"),
+])
+def test_mixed_tunings_agree_and_are_deterministic(ipt, threads, splits, schedule):
     pos, r, L = lognormal_state(3000, seed=2)
     m, eta, _ = consts()
     fc = _calc(3000, L, precision="mixed")
-    fc.set_tuning(i_per_thread=ipt, threads=threads, j_splits=splits)
+    fc.set_tuning(i_per_thread=ipt, threads=threads, j_splits=splits, schedule=schedule)
     F1, V1 = fc.calculate_forces_and_convection(pos, r)
     F2, V2 = fc.calculate_forces_and_convection(pos, r)
     np.testing.assert_array_equal(F1, F2)
