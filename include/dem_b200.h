@@ -68,6 +68,10 @@ DEM_API const char *dem_last_error(const dem_ctx *ctx);
 DEM_API int dem_device_errors(dem_ctx *ctx, uint32_t *flags_host, void *stream);
 /* Library version string (host). */
 DEM_API const char *dem_version(void);
+/* Number of kernels this library has launched in the process so far (all
+ * contexts and devices; host-side counter, no synchronisation).  The
+ * difference across a region is the count of the library's launches in it. */
+DEM_API unsigned long long dem_launch_count(void);
 
 /* Opt-in kernel timing: while enabled, CUDA events are recorded on the launch
  * stream around the main kernels ("mixed_force_pass", "mixed_convection_pass",
@@ -95,6 +99,12 @@ DEM_API int dem_direct_set_tuning(dem_ctx *ctx, int i_per_thread, int threads, i
                                   double near_oseen, int schedule);
 DEM_API int dem_direct_get_tuning(const dem_ctx *ctx, int *i_per_thread, int *threads, int *j_splits,
                                   double *near_force, double *near_oseen, int *schedule);
+/* The plan the mixed-precision passes run for n droplets under the current
+ * tuning (no launch): the resolved schedule (DEM_SCHED_SPLIT or
+ * DEM_SCHED_SYMMETRIC), i-per-thread blocking, threads per CTA, CTAs per pass
+ * and, for the split schedule, the number of j-chunks. */
+DEM_API int dem_direct_plan(const dem_ctx *ctx, int n, int periodic, int *schedule, int *i_per_thread,
+                            int *threads, long long *ctas, int *j_splits);
 
 /* ---- layout ---------------------------------------------------------- */
 /* (n, 3) row-major <-> three component arrays.  The reference's public

@@ -66,6 +66,11 @@ struct dem_ctx {
     size_t scan_tmp_bytes = 0;
 };
 
+// Every kernel launch of the library passes its stream through counted(), so
+// dem_launch_count() reports how many kernels of this library were launched
+// (process-wide, all contexts); callers use it to show that the device path ran.
+cudaStream_t counted(cudaStream_t s);
+
 int dem_set_error(dem_ctx *ctx, int code, const std::string &msg);
 int dem_check_cuda(dem_ctx *ctx, cudaError_t e, const char *where);
 int dem_check_launch(dem_ctx *ctx, const char *where);

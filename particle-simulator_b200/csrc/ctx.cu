@@ -1,10 +1,25 @@
 // ctx.cu -- context, workspace and error handling of libdem_b200.
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 
 #include "common.cuh"
 
 #define DEM_VERSION "dem_b200 0.1 (sm_100a)"
+
+static std::atomic<unsigned long long> g_launches{0};
+
+cudaStream_t counted(cudaStream_t s) {
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    return s;
+}
+
+unsigned long long dem_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+namespace dem {
+int direct_plan(const dem_ctx *ctx, int n, int periodic, int *schedule, int *i_per_thread, int *threads,
+                long long *ctas, int *j_splits);
+}
 
 int dem_set_error(dem_ctx *ctx, int code, const std::string &msg) {
     if (ctx) ctx->last_error = msg;
@@ -227,6 +242,12 @@ int dem_direct_get_tuning(const dem_ctx *ctx, int *i_per_thread, int *threads, i
     if (near_oseen) *near_oseen = ctx->tuning.near_oseen;
     if (schedule) *schedule = ctx->tuning.schedule;
     return DEM_OK;
+}
+
+int dem_direct_plan(const dem_ctx *ctx, int n, int periodic, int *schedule, int *i_per_thread, int *threads,
+                    long long *ctas, int *j_splits) {
+    if (!ctx || n < 0 || !schedule || !i_per_thread || !threads || !ctas || !j_splits) return DEM_E_INVALID;
+    return dem::direct_plan(ctx, n, periodic, schedule, i_per_thread, threads, ctas, j_splits);
 }
 
 }  // extern "C"

@@ -140,9 +140,9 @@ int launch_direct_forces_fp64(dem_ctx *ctx, int n, const double *x, const double
     const int grid = ceil_div(n, F64_THREADS);
     dem_prof_begin(ctx, "fp64_force_pass", s);
     if (periodic)
-        direct_force_fp64_kernel<true><<<grid, F64_THREADS, 0, s>>>(n, x, y, z, r, m_const, L, L * 0.5, fx, fy, fz);
+        direct_force_fp64_kernel<true><<<grid, F64_THREADS, 0, counted(s)>>>(n, x, y, z, r, m_const, L, L * 0.5, fx, fy, fz);
     else
-        direct_force_fp64_kernel<false><<<grid, F64_THREADS, 0, s>>>(n, x, y, z, r, m_const, L, L * 0.5, fx, fy, fz);
+        direct_force_fp64_kernel<false><<<grid, F64_THREADS, 0, counted(s)>>>(n, x, y, z, r, m_const, L, L * 0.5, fx, fy, fz);
     dem_prof_end(ctx, s);
     return dem_check_launch(ctx, "direct_force_fp64");
 }
@@ -154,10 +154,10 @@ int launch_direct_convection_fp64(dem_ctx *ctx, int n, const double *x, const do
     dem_prof_begin(ctx, "fp64_convection_pass", s);
     if (periodic)
         direct_convection_fp64_kernel<true>
-            <<<grid, F64_THREADS, 0, s>>>(n, x, y, z, fx, fy, fz, eta, L, L * 0.5, vx, vy, vz);
+            <<<grid, F64_THREADS, 0, counted(s)>>>(n, x, y, z, fx, fy, fz, eta, L, L * 0.5, vx, vy, vz);
     else
         direct_convection_fp64_kernel<false>
-            <<<grid, F64_THREADS, 0, s>>>(n, x, y, z, fx, fy, fz, eta, L, L * 0.5, vx, vy, vz);
+            <<<grid, F64_THREADS, 0, counted(s)>>>(n, x, y, z, fx, fy, fz, eta, L, L * 0.5, vx, vy, vz);
     dem_prof_end(ctx, s);
     return dem_check_launch(ctx, "direct_convection_fp64");
 }

@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(512) mixed_pass_kernel(const MixedArgs a) {
 
 template <int IPT, bool PER, bool FORCE>
 static void launch_pass(const MixedArgs &a, dim3 grid, int threads, cudaStream_t s) {
-    mixed_pass_kernel<IPT, PER, FORCE><<<grid, threads, 0, s>>>(a);
+    mixed_pass_kernel<IPT, PER, FORCE><<<grid, threads, 0, counted(s)>>>(a);
 }
 
 template <bool FORCE>
@@ -295,6 +295,29 @@ static int symmetric_ipt(const dem_ctx *ctx, int n) {
     return ipt;
 }
 
+// The plan the mixed passes would run for n droplets (no launch).
+int direct_plan(const dem_ctx *ctx, int n, int periodic, int *schedule, int *i_per_thread, int *threads,
+                long long *ctas, int *j_splits) {
+    const int sym = symmetric_ipt(ctx, n);
+    if (sym) {
+        const long long B = (long long)128 * sym;
+        const long long nb = (n + B - 1) / B;
+        *schedule = DEM_SCHED_SYMMETRIC;
+        *i_per_thread = sym;
+        *threads = 128;
+        *ctas = nb * (nb + 1) / 2;
+        *j_splits = 0;
+    } else {
+        const MixedPlan p = plan_for<true>(ctx, n, periodic != 0);
+        *schedule = DEM_SCHED_SPLIT;
+        *i_per_thread = p.ipt;
+        *threads = p.threads;
+        *ctas = (long long)p.grid.x * p.grid.y;
+        *j_splits = p.splits;
+    }
+    return DEM_OK;
+}
+
 int launch_direct_forces_mixed(dem_ctx *ctx, int n, const double *x, const double *y, const double *z,
                                const double *r, double m_const, double L, int periodic, double *fx, double *fy,
                                double *fz, cudaStream_t s) {
@@ -306,9 +329,9 @@ int launch_direct_forces_mixed(dem_ctx *ctx, int n, const double *x, const doubl
     rc = dem_check_cuda(ctx, cudaMemsetAsync(scales, 0, 2 * sizeof(unsigned long long), s), "memset");
     if (rc) return rc;
     const int rgrid = min(ceil_div(n, 256), 4 * ctx->sm_count);
-    maxabs_kernel<<<rgrid, 256, 0, s>>>(n, r, nullptr, nullptr, scales);
+    maxabs_kernel<<<rgrid, 256, 0, counted(s)>>>(n, r, nullptr, nullptr, scales);
     float *krf = reinterpret_cast<float *>(ctx->pack_b);  // force pass: k_f r lives in pack_b
-    prep_positions_kernel<<<rgrid, 256, 0, s>>>(n, x, y, z, r, 0.5 * L, scales, ctx->tuning.near_force, ctx->pack_a, krf);
+    prep_positions_kernel<<<rgrid, 256, 0, counted(s)>>>(n, x, y, z, r, 0.5 * L, scales, ctx->tuning.near_force, ctx->pack_a, krf);
     MixedArgs a{};
     a.n = n;
     a.j_chunk = p.j_chunk;
@@ -331,7 +354,7 @@ int launch_direct_forces_mixed(dem_ctx *ctx, int n, const double *x, const doubl
     dem_prof_end(ctx, s);
     rc = dem_check_launch(ctx, "direct_forces_mixed");
     if (rc) return rc;
-    reduce_partials_kernel<true><<<rgrid, 256, 0, s>>>(n, p.splits, ctx->partial, r, scales, m_const, fx, fy, fz,
+    reduce_partials_kernel<true><<<rgrid, 256, 0, counted(s)>>>(n, p.splits, ctx->partial, r, scales, m_const, fx, fy, fz,
                                                        ctx->d_err);
     return dem_check_launch(ctx, "direct_forces_mixed reduce");
 }
@@ -347,10 +370,10 @@ int launch_direct_convection_mixed(dem_ctx *ctx, int n, const double *x, const d
     rc = dem_check_cuda(ctx, cudaMemsetAsync(scales, 0, 2 * sizeof(unsigned long long), s), "memset");
     if (rc) return rc;
     const int rgrid = min(ceil_div(n, 256), 4 * ctx->sm_count);
-    maxabs_kernel<<<rgrid, 256, 0, s>>>(n, r, nullptr, nullptr, scales);
-    maxabs_kernel<<<rgrid, 256, 0, s>>>(n, fx, fy, fz, scales + 1);
-    prep_positions_kernel<<<rgrid, 256, 0, s>>>(n, x, y, z, r, 0.5 * L, scales, 0.0, ctx->pack_a, nullptr);
-    prep_forces_kernel<<<rgrid, 256, 0, s>>>(n, fx, fy, fz, r, scales, ctx->tuning.near_oseen, ctx->pack_b);
+    maxabs_kernel<<<rgrid, 256, 0, counted(s)>>>(n, r, nullptr, nullptr, scales);
+    maxabs_kernel<<<rgrid, 256, 0, counted(s)>>>(n, fx, fy, fz, scales + 1);
+    prep_positions_kernel<<<rgrid, 256, 0, counted(s)>>>(n, x, y, z, r, 0.5 * L, scales, 0.0, ctx->pack_a, nullptr);
+    prep_forces_kernel<<<rgrid, 256, 0, counted(s)>>>(n, fx, fy, fz, r, scales, ctx->tuning.near_oseen, ctx->pack_b);
     rc = dem_check_launch(ctx, "direct_convection_mixed prep");
     if (rc) return rc;
     MixedArgs a{};
@@ -376,7 +399,7 @@ int launch_direct_convection_mixed(dem_ctx *ctx, int n, const double *x, const d
     dem_prof_end(ctx, s);
     rc = dem_check_launch(ctx, "direct_convection_mixed");
     if (rc) return rc;
-    reduce_partials_kernel<false><<<rgrid, 256, 0, s>>>(n, p.splits, ctx->partial, r, scales, eta, vx, vy, vz,
+    reduce_partials_kernel<false><<<rgrid, 256, 0, counted(s)>>>(n, p.splits, ctx->partial, r, scales, eta, vx, vy, vz,
                                                         ctx->d_err);
     return dem_check_launch(ctx, "direct_convection_mixed reduce");
 }

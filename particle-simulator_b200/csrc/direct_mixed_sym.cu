@@ -365,9 +365,9 @@ __global__ void reduce_sym_kernel(int n, int nb, int B, const double *__restrict
 template <int IPT, bool FORCE>
 static void launch_sym(bool per, const SymArgs &a, cudaStream_t s) {
     if (per)
-        mixed_sym_kernel<IPT, true, FORCE><<<a.nitems, SYM_T, 0, s>>>(a);
+        mixed_sym_kernel<IPT, true, FORCE><<<a.nitems, SYM_T, 0, counted(s)>>>(a);
     else
-        mixed_sym_kernel<IPT, false, FORCE><<<a.nitems, SYM_T, 0, s>>>(a);
+        mixed_sym_kernel<IPT, false, FORCE><<<a.nitems, SYM_T, 0, counted(s)>>>(a);
 }
 
 // Bytes of partial sums the symmetric schedule needs for n droplets.
@@ -407,7 +407,7 @@ int run_sym_pass(dem_ctx *ctx, int n, int ipt, bool per, const MixedArgs &m, dou
     int rc = dem_check_launch(ctx, FORCE ? "mixed force (symmetric)" : "mixed convection (symmetric)");
     if (rc) return rc;
     const int rgrid = min(ceil_div(n, 256), 4 * ctx->sm_count);
-    reduce_sym_kernel<FORCE><<<rgrid, 256, 0, s>>>(n, nb, B, a.pi, a.pj, r, m.scales, coeff, ox, oy, oz, ctx->d_err);
+    reduce_sym_kernel<FORCE><<<rgrid, 256, 0, counted(s)>>>(n, nb, B, a.pi, a.pj, r, m.scales, coeff, ox, oy, oz, ctx->d_err);
     return dem_check_launch(ctx, "mixed reduce (symmetric)");
 }
 

@@ -53,7 +53,7 @@ int launch_euler_direct(dem_ctx *ctx, int n, const double *x, const double *y, c
                         const double *vz, double stokes, double dt, double L, int periodic, double *xo, double *yo,
                         double *zo, cudaStream_t s) {
     const int grid = min(ceil_div(n, 256), 8 * ctx->sm_count);
-    euler_direct_kernel<<<grid, 256, 0, s>>>(n, x, y, z, r, fx, fy, fz, vx, vy, vz, stokes, dt, L, periodic, xo, yo,
+    euler_direct_kernel<<<grid, 256, 0, counted(s)>>>(n, x, y, z, r, fx, fy, fz, vx, vy, vz, stokes, dt, L, periodic, xo, yo,
                                              zo);
     return dem_check_launch(ctx, "euler_direct");
 }
@@ -62,7 +62,7 @@ int launch_euler_total(dem_ctx *ctx, int n, const double *x, const double *y, co
                        const double *vy, const double *vz, double dt, double L, int periodic, double *xo, double *yo,
                        double *zo, cudaStream_t s) {
     const int grid = min(ceil_div(n, 256), 8 * ctx->sm_count);
-    euler_total_kernel<<<grid, 256, 0, s>>>(n, x, y, z, vx, vy, vz, dt, L, periodic, xo, yo, zo);
+    euler_total_kernel<<<grid, 256, 0, counted(s)>>>(n, x, y, z, vx, vy, vz, dt, L, periodic, xo, yo, zo);
     return dem_check_launch(ctx, "euler_total");
 }
 
@@ -100,7 +100,7 @@ int dem_aos_to_soa(dem_ctx *ctx, int n, const double *aos, double *x, double *y,
     if (!ctx || n < 0) return DEM_E_INVALID;
     if (n == 0) return DEM_OK;
     const int grid = min(ceil_div(n, 256), 8 * ctx->sm_count);
-    dem::aos_to_soa_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(n, aos, x, y, z);
+    dem::aos_to_soa_kernel<<<grid, 256, 0, counted((cudaStream_t)stream)>>>(n, aos, x, y, z);
     return dem_check_launch(ctx, "aos_to_soa");
 }
 
@@ -108,7 +108,7 @@ int dem_soa_to_aos(dem_ctx *ctx, int n, const double *x, const double *y, const 
     if (!ctx || n < 0) return DEM_E_INVALID;
     if (n == 0) return DEM_OK;
     const int grid = min(ceil_div(n, 256), 8 * ctx->sm_count);
-    dem::soa_to_aos_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(n, x, y, z, aos);
+    dem::soa_to_aos_kernel<<<grid, 256, 0, counted((cudaStream_t)stream)>>>(n, x, y, z, aos);
     return dem_check_launch(ctx, "soa_to_aos");
 }
 

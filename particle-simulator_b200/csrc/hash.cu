@@ -232,9 +232,9 @@ int launch_hash_detect(dem_ctx *ctx, int n, const double *x, const double *y, co
     if (rc) return rc;
     if (n == 0) return DEM_OK;
     dem_prof_begin(ctx, "hash_detect", s);
-    max_kernel<<<grid, 256, 0, s>>>(n, r, slot);
-    hash_params_kernel<<<1, 1, 0, s>>>(slot, L, hp);
-    assign_kernel<<<grid, 256, 0, s>>>(n, x, y, z, hp, periodic, mask, ctx->cell_hash, ctx->bucket_count);
+    max_kernel<<<grid, 256, 0, counted(s)>>>(n, r, slot);
+    hash_params_kernel<<<1, 1, 0, counted(s)>>>(slot, L, hp);
+    assign_kernel<<<grid, 256, 0, counted(s)>>>(n, x, y, z, hp, periodic, mask, ctx->cell_hash, ctx->bucket_count);
     rc = dem_check_launch(ctx, "hash assign");
     if (rc) return rc;
     rc = exclusive_scan<int32_t, int32_t>(ctx, ctx->bucket_count, ctx->bucket_start, table_size, s);
@@ -243,15 +243,15 @@ int launch_hash_detect(dem_ctx *ctx, int n, const double *x, const double *y, co
                                              cudaMemcpyDeviceToDevice, s),
                         "cursor copy");
     if (rc) return rc;
-    scatter_kernel<<<grid, 256, 0, s>>>(n, ctx->cell_hash, hp, ctx->bucket_cursor, ctx->sorted_idx);
+    scatter_kernel<<<grid, 256, 0, counted(s)>>>(n, ctx->cell_hash, hp, ctx->bucket_cursor, ctx->sorted_idx);
     const int dgrid = ceil_div(n, 128);
-    count_pairs_kernel<<<dgrid, 128, 0, s>>>(n, x, y, z, r, hp, periodic, L, mask, ctx->bucket_start, ctx->sorted_idx,
+    count_pairs_kernel<<<dgrid, 128, 0, counted(s)>>>(n, x, y, z, r, hp, periodic, L, mask, ctx->bucket_start, ctx->sorted_idx,
                                              ctx->pair_count, reinterpret_cast<unsigned long long *>(counts + 1));
     rc = dem_check_launch(ctx, "hash count");
     if (rc) return rc;
     rc = exclusive_scan<int32_t, int64_t>(ctx, ctx->pair_count, ctx->pair_offset, n, s);
     if (rc) return rc;
-    write_pairs_kernel<<<dgrid, 128, 0, s>>>(n, x, y, z, r, hp, periodic, L, mask, ctx->bucket_start, ctx->sorted_idx,
+    write_pairs_kernel<<<dgrid, 128, 0, counted(s)>>>(n, x, y, z, r, hp, periodic, L, mask, ctx->bucket_start, ctx->sorted_idx,
                                              ctx->pair_offset, pairs, cap, counts, ctx->d_err);
     dem_prof_end(ctx, s);
     return dem_check_launch(ctx, "hash write");
@@ -356,9 +356,9 @@ extern "C" int dem_hash_detect_noalloc(int n, const double *x, const double *y, 
     if (cudaMemsetAsync(counts, 0, 2 * sizeof(int64_t), s) != cudaSuccess) return DEM_E_CUDA;
     if (cudaMemsetAsync(bucket_count, 0, sizeof(int32_t) * table_size, s) != cudaSuccess) return DEM_E_CUDA;
     if (n == 0) return DEM_OK;
-    max_kernel<<<grid, 256, 0, s>>>(n, r, slot);
-    hash_params_kernel<<<1, 1, 0, s>>>(slot, L, hp);
-    assign_kernel<<<grid, 256, 0, s>>>(n, x, y, z, hp, periodic, mask, cell_hash, bucket_count);
+    max_kernel<<<grid, 256, 0, counted(s)>>>(n, r, slot);
+    hash_params_kernel<<<1, 1, 0, counted(s)>>>(slot, L, hp);
+    assign_kernel<<<grid, 256, 0, counted(s)>>>(n, x, y, z, hp, periodic, mask, cell_hash, bucket_count);
     if (cudaGetLastError() != cudaSuccess) return DEM_E_CUDA;
     if (exclusive_scan_into<int32_t, int32_t>(bucket_count, bucket_start, table_size, static_cast<int32_t *>(sums),
                                               s) != cudaSuccess)
@@ -366,15 +366,15 @@ extern "C" int dem_hash_detect_noalloc(int n, const double *x, const double *y, 
     if (cudaMemcpyAsync(bucket_cursor, bucket_start, sizeof(int32_t) * table_size, cudaMemcpyDeviceToDevice, s) !=
         cudaSuccess)
         return DEM_E_CUDA;
-    scatter_kernel<<<grid, 256, 0, s>>>(n, cell_hash, hp, bucket_cursor, sorted_idx);
+    scatter_kernel<<<grid, 256, 0, counted(s)>>>(n, cell_hash, hp, bucket_cursor, sorted_idx);
     const int dgrid = ceil_div(n, 128);
-    count_pairs_kernel<<<dgrid, 128, 0, s>>>(n, x, y, z, r, hp, periodic, L, mask, bucket_start, sorted_idx,
+    count_pairs_kernel<<<dgrid, 128, 0, counted(s)>>>(n, x, y, z, r, hp, periodic, L, mask, bucket_start, sorted_idx,
                                              pair_count, reinterpret_cast<unsigned long long *>(counts + 1));
     if (cudaGetLastError() != cudaSuccess) return DEM_E_CUDA;
     if (exclusive_scan_into<int32_t, int64_t>(pair_count, pair_offset, n, static_cast<int64_t *>(sums), s) !=
         cudaSuccess)
         return DEM_E_CUDA;
-    write_pairs_kernel<<<dgrid, 128, 0, s>>>(n, x, y, z, r, hp, periodic, L, mask, bucket_start, sorted_idx,
+    write_pairs_kernel<<<dgrid, 128, 0, counted(s)>>>(n, x, y, z, r, hp, periodic, L, mask, bucket_start, sorted_idx,
                                              pair_offset, pairs, pair_capacity, counts, err);
     return cudaGetLastError() == cudaSuccess ? DEM_OK : DEM_E_CUDA;
 }

@@ -119,14 +119,14 @@ int launch_merge(dem_ctx *ctx, int n, const double *x, const double *y, const do
     // the hash detector's per-droplet offset buffer (int64[capacity + 1]), which
     // is free once the pairs have been written.
     int32_t *sel = reinterpret_cast<int32_t *>(ctx->pair_offset);
-    merge_select_kernel<<<1, 32, 0, s>>>(n, pairs, num_pairs, ctx->flags, sel, ctx->merged_cnt, ctx->d_err);
+    merge_select_kernel<<<1, 32, 0, counted(s)>>>(n, pairs, num_pairs, ctx->flags, sel, ctx->merged_cnt, ctx->d_err);
     const int grid = max(1, min(ceil_div(n, 256), 8 * ctx->sm_count));
-    merge_compute_kernel<<<grid, 256, 0, s>>>(x, y, z, r, sel, ctx->merged_cnt, ctx->merged_buf);
+    merge_compute_kernel<<<grid, 256, 0, counted(s)>>>(x, y, z, r, sel, ctx->merged_cnt, ctx->merged_buf);
     rc = dem_check_launch(ctx, "merge select");
     if (rc) return rc;
     rc = exclusive_scan<int32_t, int32_t>(ctx, ctx->flags, ctx->keep_off, n, s);
     if (rc) return rc;
-    merge_compact_kernel<<<grid, 256, 0, s>>>(n, x, y, z, r, ctx->flags, ctx->keep_off, ctx->merged_buf, sel,
+    merge_compact_kernel<<<grid, 256, 0, counted(s)>>>(n, x, y, z, r, ctx->flags, ctx->keep_off, ctx->merged_buf, sel,
                                               ctx->merged_cnt, xo, yo, zo, ro, n_out, merged_pairs);
     return dem_check_launch(ctx, "merge compact");
 }

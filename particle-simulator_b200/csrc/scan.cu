@@ -107,9 +107,9 @@ int exclusive_scan(dem_ctx *ctx, const TIn *in, TOut *out, int64_t n, cudaStream
         ctx->scan_tmp_bytes = need;
     }
     TOut *sums = reinterpret_cast<TOut *>(ctx->scan_tmp);
-    scan_block_totals<TIn, TOut><<<nb, SCAN_THREADS, 0, s>>>(in, n, sums);
-    scan_totals<TOut><<<1, 1024, 0, s>>>(sums, nb);
-    scan_apply<TIn, TOut><<<nb, SCAN_THREADS, 0, s>>>(in, n, sums, out);
+    scan_block_totals<TIn, TOut><<<nb, SCAN_THREADS, 0, counted(s)>>>(in, n, sums);
+    scan_totals<TOut><<<1, 1024, 0, counted(s)>>>(sums, nb);
+    scan_apply<TIn, TOut><<<nb, SCAN_THREADS, 0, counted(s)>>>(in, n, sums, out);
     return dem_check_launch(ctx, "exclusive_scan");
 }
 
@@ -118,9 +118,9 @@ cudaError_t exclusive_scan_into(const TIn *in, TOut *out, int64_t n, TOut *sums,
     const int64_t nb64 = n > 0 ? (n + SCAN_TILE - 1) / SCAN_TILE : 1;
     if (nb64 > SCAN_MAX_BLOCKS) return cudaErrorInvalidValue;
     const int nb = (int)nb64;
-    scan_block_totals<TIn, TOut><<<nb, SCAN_THREADS, 0, s>>>(in, n, sums);
-    scan_totals<TOut><<<1, 1024, 0, s>>>(sums, nb);
-    scan_apply<TIn, TOut><<<nb, SCAN_THREADS, 0, s>>>(in, n, sums, out);
+    scan_block_totals<TIn, TOut><<<nb, SCAN_THREADS, 0, counted(s)>>>(in, n, sums);
+    scan_totals<TOut><<<1, 1024, 0, counted(s)>>>(sums, nb);
+    scan_apply<TIn, TOut><<<nb, SCAN_THREADS, 0, counted(s)>>>(in, n, sums, out);
     return cudaGetLastError();
 }
 

@@ -687,14 +687,14 @@ int dem_tree_build(dem_tree *t, int n, const double *x, const double *y, const d
     t->pool_exhausted = 0;
     t->level_off.clear();
     dem_prof_begin(ctx, "tree_build", s);
-    tree_init_kernel<<<grid_for(ctx, max(n, 1)), 256, 0, s>>>(view(t), n, L, x, y, z, r);
+    tree_init_kernel<<<grid_for(ctx, max(n, 1)), 256, 0, counted(s)>>>(view(t), n, L, x, y, z, r);
     int ls = 0, le = 1;
     for (int level = 0; level < 40; ++level) {
         const int pc_before = t->parent_count;
         const int width = le - ls;
-        zero_child_cnt_kernel<<<grid_for(ctx, 8LL * width), 256, 0, s>>>(t->child_cnt, ls, le);
-        assign_octants_kernel<<<grid_for(ctx, max(n, 1)), 256, 0, s>>>(view(t), n, ls, le);
-        subdivide_flags_kernel<<<grid_for(ctx, width), 256, 0, s>>>(view(t), ls, le, mpl);
+        zero_child_cnt_kernel<<<grid_for(ctx, 8LL * width), 256, 0, counted(s)>>>(t->child_cnt, ls, le);
+        assign_octants_kernel<<<grid_for(ctx, max(n, 1)), 256, 0, counted(s)>>>(view(t), n, ls, le);
+        subdivide_flags_kernel<<<grid_for(ctx, width), 256, 0, counted(s)>>>(view(t), ls, le, mpl);
         int rc = exclusive_scan<int32_t, int32_t>(ctx, t->flag, t->rank, width, s);
         if (rc) return rc;
         rc = dem_check_cuda(ctx, cudaMemcpyAsync(t->h_total, t->rank + width, sizeof(int32_t), cudaMemcpyDeviceToHost, s),
@@ -706,32 +706,32 @@ int dem_tree_build(dem_tree *t, int n, const double *x, const double *y, const d
         const int sub = total < room ? total : (room > 0 ? room : 0);
         if (sub < total) t->pool_exhausted = 1;
         if (sub > 0) {
-            subdivide_kernel<<<grid_for(ctx, width), 256, 0, s>>>(view(t), ls, le, sub, t->node_count, t->parent_count);
+            subdivide_kernel<<<grid_for(ctx, width), 256, 0, counted(s)>>>(view(t), ls, le, sub, t->node_count, t->parent_count);
             t->node_count += 8 * sub;
             t->parent_count += sub;
         }
-        level_scatter_kernel<<<grid_for(ctx, max(n, 1)), 256, 0, s>>>(view(t), n);
+        level_scatter_kernel<<<grid_for(ctx, max(n, 1)), 256, 0, counted(s)>>>(view(t), n);
         ls = le;
         le = t->node_count;
         if (t->parent_count > pc_before) t->level_off.push_back(pc_before);
         if (sub == 0) break;
     }
     const int nc = t->node_count;
-    leaf_flags_kernel<<<grid_for(ctx, nc), 256, 0, s>>>(view(t), nc);
+    leaf_flags_kernel<<<grid_for(ctx, nc), 256, 0, counted(s)>>>(view(t), nc);
     int rc = exclusive_scan<int32_t, int32_t>(ctx, t->flag, t->rank, nc, s);
     if (rc) return rc;
-    leaf_start_kernel<<<grid_for(ctx, nc), 256, 0, s>>>(view(t), nc);
-    leaf_scatter_kernel<<<grid_for(ctx, max(n, 1)), 256, 0, s>>>(view(t), n);
-    leaf_sort_kernel<<<grid_for(ctx, nc), 256, 0, s>>>(view(t), nc);
+    leaf_start_kernel<<<grid_for(ctx, nc), 256, 0, counted(s)>>>(view(t), nc);
+    leaf_scatter_kernel<<<grid_for(ctx, max(n, 1)), 256, 0, counted(s)>>>(view(t), n);
+    leaf_sort_kernel<<<grid_for(ctx, nc), 256, 0, counted(s)>>>(view(t), nc);
     const int nl = (int)t->level_off.size();
     auto lev_end = [&](int l) { return l + 1 < nl ? t->level_off[l + 1] : t->parent_count; };
     for (int l = 0; l < nl; ++l)
-        next_pass1_kernel<<<grid_for(ctx, lev_end(l) - t->level_off[l]), 256, 0, s>>>(view(t), t->level_off[l], lev_end(l));
+        next_pass1_kernel<<<grid_for(ctx, lev_end(l) - t->level_off[l]), 256, 0, counted(s)>>>(view(t), t->level_off[l], lev_end(l));
     for (int l = 0; l < nl; ++l)
-        next_pass2_kernel<<<grid_for(ctx, lev_end(l) - t->level_off[l]), 256, 0, s>>>(view(t), t->level_off[l], lev_end(l));
-    leaf_r3_kernel<<<grid_for(ctx, nc), 256, 0, s>>>(view(t), nc);
+        next_pass2_kernel<<<grid_for(ctx, lev_end(l) - t->level_off[l]), 256, 0, counted(s)>>>(view(t), t->level_off[l], lev_end(l));
+    leaf_r3_kernel<<<grid_for(ctx, nc), 256, 0, counted(s)>>>(view(t), nc);
     for (int l = nl - 1; l >= 0; --l)
-        sweep_r3_kernel<<<grid_for(ctx, lev_end(l) - t->level_off[l]), 256, 0, s>>>(view(t), t->level_off[l], lev_end(l));
+        sweep_r3_kernel<<<grid_for(ctx, lev_end(l) - t->level_off[l]), 256, 0, counted(s)>>>(view(t), t->level_off[l], lev_end(l));
     rc = dem_check_cuda(ctx, cudaMemcpyAsync(t->h_total + 1, t->rank + nc, sizeof(int32_t), cudaMemcpyDeviceToHost, s),
                         "tree build");
     if (!rc) rc = dem_check_cuda(ctx, cudaStreamSynchronize(s), "tree build");
@@ -748,9 +748,9 @@ int dem_tree_forces(dem_tree *t, double m_const, double theta_sq, double *fx, do
     dem_prof_begin(t->ctx, "tree_force_walk", s);
     const int grid = ceil_div(t->n, 128);
     if (t->periodic)
-        force_walk_kernel<true><<<grid, 128, 0, s>>>(view(t), m_const, theta_sq, fx, fy, fz);
+        force_walk_kernel<true><<<grid, 128, 0, counted(s)>>>(view(t), m_const, theta_sq, fx, fy, fz);
     else
-        force_walk_kernel<false><<<grid, 128, 0, s>>>(view(t), m_const, theta_sq, fx, fy, fz);
+        force_walk_kernel<false><<<grid, 128, 0, counted(s)>>>(view(t), m_const, theta_sq, fx, fy, fz);
     dem_prof_end(t->ctx, s);
     return dem_check_launch(t->ctx, "tree force walk");
 }
@@ -765,11 +765,11 @@ int dem_tree_propagate_forces(dem_tree *t, const double *fx, const double *fy, c
         fy = t->pf + N;
         fz = t->pf + 2 * (size_t)N;
     }
-    leaf_forces_kernel<<<grid_for(ctx, nc), 256, 0, s>>>(view(t), nc, fx, fy, fz);
+    leaf_forces_kernel<<<grid_for(ctx, nc), 256, 0, counted(s)>>>(view(t), nc, fx, fy, fz);
     const int nl = (int)t->level_off.size();
     for (int l = nl - 1; l >= 0; --l) {
         const int a = t->level_off[l], b = l + 1 < nl ? t->level_off[l + 1] : t->parent_count;
-        sweep_forces_kernel<<<grid_for(ctx, b - a), 256, 0, s>>>(view(t), a, b);
+        sweep_forces_kernel<<<grid_for(ctx, b - a), 256, 0, counted(s)>>>(view(t), a, b);
     }
     return dem_check_launch(ctx, "tree propagate forces");
 }
@@ -788,9 +788,9 @@ int dem_tree_velocity(dem_tree *t, const double *fx, const double *fy, const dou
     dem_prof_begin(t->ctx, "tree_velocity_walk", s);
     const int grid = ceil_div(t->n, 128);
     if (t->periodic)
-        velocity_walk_kernel<true><<<grid, 128, 0, s>>>(view(t), fx, fy, fz, eta_const, theta_sq, stokes_factor, vx, vy, vz);
+        velocity_walk_kernel<true><<<grid, 128, 0, counted(s)>>>(view(t), fx, fy, fz, eta_const, theta_sq, stokes_factor, vx, vy, vz);
     else
-        velocity_walk_kernel<false><<<grid, 128, 0, s>>>(view(t), fx, fy, fz, eta_const, theta_sq, stokes_factor, vx, vy, vz);
+        velocity_walk_kernel<false><<<grid, 128, 0, counted(s)>>>(view(t), fx, fy, fz, eta_const, theta_sq, stokes_factor, vx, vy, vz);
     dem_prof_end(t->ctx, s);
     return dem_check_launch(t->ctx, "tree velocity walk");
 }
@@ -812,7 +812,7 @@ int dem_tree_nodes(dem_tree *t, int32_t *count, int32_t *first_child, int32_t *n
                    double *fs, void *stream) {
     if (!t) return DEM_E_INVALID;
     const int nc = t->node_count;
-    copy_nodes_kernel<<<grid_for(t->ctx, nc), 256, 0, (cudaStream_t)stream>>>(view(t), nc, count, first_child, next,
+    copy_nodes_kernel<<<grid_for(t->ctx, nc), 256, 0, counted((cudaStream_t)stream)>>>(view(t), nc, count, first_child, next,
                                                                              leaf_start, r3, fs);
     return dem_check_launch(t->ctx, "tree nodes");
 }

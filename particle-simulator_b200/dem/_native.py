@@ -41,6 +41,7 @@ DEVERR_NONFINITE = 8
 _i, _d, _vp, _i64 = C.c_int, C.c_double, C.c_void_p, C.c_int64
 SIGNATURES = {
     "dem_version": (C.c_char_p, []),
+    "dem_launch_count": (C.c_ulonglong, []),
     "dem_ctx_create": (_i, [_i, _i, C.POINTER(_vp)]),
     "dem_ctx_destroy": (None, [_vp]),
     "dem_ctx_reserve": (_i, [_vp, _i]),
@@ -53,6 +54,8 @@ SIGNATURES = {
     "dem_direct_set_tuning": (_i, [_vp, _i, _i, _i, _d, _d, _i]),
     "dem_direct_get_tuning": (_i, [_vp, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i), C.POINTER(_d), C.POINTER(_d),
                                    C.POINTER(_i)]),
+    "dem_direct_plan": (_i, [_vp, _i, _i, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i), C.POINTER(C.c_longlong),
+                             C.POINTER(_i)]),
     "dem_aos_to_soa": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp]),
     "dem_soa_to_aos": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp]),
     "dem_direct_forces": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _d, _d, _i, _i, _vp, _vp, _vp, _vp]),
@@ -106,6 +109,11 @@ def exported_symbols():
 
 def version() -> str:
     return lib().dem_version().decode()
+
+
+def launch_count() -> int:
+    """Kernels launched by the library in this process so far (host counter)."""
+    return int(lib().dem_launch_count())
 
 
 def _torch():
@@ -209,6 +217,17 @@ class Context:
                                                 C.byref(g)), "get_tuning")
         return dict(i_per_thread=a.value, threads=b.value, j_splits=c.value, near_force=d.value, near_oseen=e.value,
                     schedule=g.value)
+
+    def plan(self, n, periodic=True):
+        """The plan the mixed passes run for n droplets: resolved schedule name,
+        i-per-thread, threads per CTA, CTAs per pass, j-chunks (split only)."""
+        sc, ipt, th, js = _i(), _i(), _i(), _i()
+        ctas = C.c_longlong()
+        self._check(lib().dem_direct_plan(self.handle, int(n), int(bool(periodic)), C.byref(sc), C.byref(ipt),
+                                          C.byref(th), C.byref(ctas), C.byref(js)), "plan")
+        names = {v: k for k, v in SCHEDULES.items()}
+        return dict(schedule=names[sc.value], i_per_thread=ipt.value, threads=th.value, ctas=ctas.value,
+                    j_splits=js.value)
 
     # -- thin wrappers over the C ABI (torch CUDA tensors in, no allocation) --
     def aos_to_soa(self, n, aos, soa):

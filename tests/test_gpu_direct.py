@@ -162,3 +162,21 @@ def test_euler_update_bit_exact():
     got = fc._io.download([out], st.n)[0]
     np.testing.assert_array_equal(got, np.mod(shifted, L))
     assert fc._ctx.device_errors() == 0
+
+
+def test_plan_and_launch_counter():
+    from dem._native import launch_count
+
+    pos, r, L = lognormal_state(1000, seed=3)
+    fc = _calc(1000, L, precision="mixed")
+    assert fc._ctx.plan(65536)["schedule"] == "symmetric"
+    assert fc._ctx.plan(100)["schedule"] == "split"  # auto: too small for block pairs
+    fc.set_tuning(schedule="split")
+    p = fc._ctx.plan(65536)
+    assert p["schedule"] == "split" and p["j_splits"] >= 1 and p["ctas"] >= 148
+    fc.set_tuning(schedule="auto")
+    fc.calculate_forces_and_convection(pos, r)  # first call allocates
+    c0 = launch_count()
+    fc.calculate_forces_and_convection(pos, r)
+    # forces: max, prep, pass, reduce; convection: 2 max, 2 prep, pass, reduce; plus the layout kernels
+    assert launch_count() - c0 >= 10
