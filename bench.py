@@ -289,11 +289,16 @@ def cpu_step_rate(pos, r, L, budget_s, threads=0):
     F = O.direct_forces(pos, r, m, L, True, rows=(0, rows), threads=threads)
     O.direct_convection(pos, F, eta, L, True, rows=(0, rows), threads=threads)
     per_row = (time.perf_counter() - t0) / rows
-    rows = int(min(n, max(rows, budget_s / max(per_row, 1e-9))))
-    t0 = time.perf_counter()
-    F = O.direct_forces(pos, r, m, L, True, rows=(0, rows), threads=threads)
-    O.direct_convection(pos, F, eta, L, True, rows=(0, rows), threads=threads)
-    t_rows = time.perf_counter() - t0
+    # timed sample: consecutive row chunks until the budget is spent (or every row is done)
+    chunk = int(min(n, max(rows, 0.25 * budget_s / max(per_row, 1e-9))))
+    rows, t_rows = 0, 0.0
+    while rows < n and t_rows < budget_s:
+        r1 = min(n, rows + chunk)
+        t0 = time.perf_counter()
+        F = O.direct_forces(pos, r, m, L, True, rows=(rows, r1), threads=threads)
+        O.direct_convection(pos, F, eta, L, True, rows=(rows, r1), threads=threads)
+        t_rows += time.perf_counter() - t0
+        rows = r1
     t0 = time.perf_counter()
     O.euler_direct(pos, r, np.zeros((n, 3)), np.zeros((n, 3)), stokes, DT, L, True)
     t_euler = time.perf_counter() - t0

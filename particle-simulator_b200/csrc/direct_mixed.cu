@@ -289,7 +289,7 @@ constexpr size_t SYM_BUDGET = size_t(4) << 30;
 static int symmetric_ipt(const dem_ctx *ctx, int n) {
     const int sched = ctx->tuning.schedule;
     if (sched == DEM_SCHED_SPLIT) return 0;
-    const int ipt = ctx->tuning.i_per_thread >= 4 ? 4 : (ctx->tuning.i_per_thread >= 2 ? 2 : 1);
+    const int ipt = ctx->tuning.i_per_thread >= 4 ? 4 : 2;  // two i's per packed FP32x2 operation
     if (sched == DEM_SCHED_SYMMETRIC) return ipt;
     if (n < 256 || sym_partial_bytes(n, ipt) > SYM_BUDGET) return 0;
     return ipt;
@@ -331,7 +331,9 @@ int launch_direct_forces_mixed(dem_ctx *ctx, int n, const double *x, const doubl
     const int rgrid = min(ceil_div(n, 256), 4 * ctx->sm_count);
     maxabs_kernel<<<rgrid, 256, 0, counted(s)>>>(n, r, nullptr, nullptr, scales);
     float *krf = reinterpret_cast<float *>(ctx->pack_b);  // force pass: k_f r lives in pack_b
-    prep_positions_kernel<<<rgrid, 256, 0, counted(s)>>>(n, x, y, z, r, 0.5 * L, scales, ctx->tuning.near_force, ctx->pack_a, krf);
+    if (!sym)  // the symmetric schedule packs its own layout
+        prep_positions_kernel<<<rgrid, 256, 0, counted(s)>>>(n, x, y, z, r, 0.5 * L, scales, ctx->tuning.near_force,
+                                                             ctx->pack_a, krf);
     MixedArgs a{};
     a.n = n;
     a.j_chunk = p.j_chunk;
@@ -372,8 +374,12 @@ int launch_direct_convection_mixed(dem_ctx *ctx, int n, const double *x, const d
     const int rgrid = min(ceil_div(n, 256), 4 * ctx->sm_count);
     maxabs_kernel<<<rgrid, 256, 0, counted(s)>>>(n, r, nullptr, nullptr, scales);
     maxabs_kernel<<<rgrid, 256, 0, counted(s)>>>(n, fx, fy, fz, scales + 1);
-    prep_positions_kernel<<<rgrid, 256, 0, counted(s)>>>(n, x, y, z, r, 0.5 * L, scales, 0.0, ctx->pack_a, nullptr);
-    prep_forces_kernel<<<rgrid, 256, 0, counted(s)>>>(n, fx, fy, fz, r, scales, ctx->tuning.near_oseen, ctx->pack_b);
+    if (!sym) {  // the symmetric schedule packs its own layout
+        prep_positions_kernel<<<rgrid, 256, 0, counted(s)>>>(n, x, y, z, r, 0.5 * L, scales, 0.0, ctx->pack_a,
+                                                             nullptr);
+        prep_forces_kernel<<<rgrid, 256, 0, counted(s)>>>(n, fx, fy, fz, r, scales, ctx->tuning.near_oseen,
+                                                          ctx->pack_b);
+    }
     rc = dem_check_launch(ctx, "direct_convection_mixed prep");
     if (rc) return rc;
     MixedArgs a{};

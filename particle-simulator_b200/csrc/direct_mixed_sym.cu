@@ -11,13 +11,23 @@
 //     32-j sub-tile lane l meets j = (l + step) mod 32, so the lanes always
 //     hold different j's; each lane adds its j-side terms to the running sum
 //     of the j it holds and passes that sum to lane l - 1 (one shuffle per
-//     component), so after 32 steps every sum is back with the lane owning j;
+//     component and half), so after 32 steps every sum is back with the lane
+//     owning j;
 //   * I == J: ordered pairs, i side only (every i != j pair seen from both ends);
 //   * near-contact pairs, i == j and pairs whose periodic image is ambiguous in
 //     FP32 are recomputed in FP64 with the reference formula; their j-side
 //     terms go to the slot of that j in shared memory (one slot per warp and j);
 //   * the per-(I, J) partial sums are written to HBM and added per droplet in a
 //     fixed order by reduce_sym_kernel, so results are deterministic.
+//
+// Arithmetic is packed FP32x2 (sm_100 add/mul/fma.f32x2, round to nearest):
+// one instruction evaluates the same j against two i's of the thread, which
+// halves the issue slots of the pair terms.  The j tiles are therefore stored
+// with every value duplicated, (x, x, y, y), so that they feed the packed
+// operands directly; only the comparisons, the rsqrt and the exact-pair
+// selects are per element.  Arrays are zero-padded to whole blocks: a padding
+// droplet has r^3 = 0 (force) or F = 0 (convection), so its terms vanish and
+// no per-pair validity test is needed.
 // j-tiles come in by 1-D TMA bulk copies (no multicast) into a double buffer on
 // mbarriers with bounded waits, exactly as in the split schedule.
 #include "mixed_common.cuh"
@@ -26,14 +36,25 @@ namespace dem {
 
 constexpr int SYM_T = 128;  // threads per CTA (4 warps); TJ == SYM_T
 
+__device__ __forceinline__ float2 p_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 p_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 p_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
+
+// Packed layout of the symmetric passes (npad = nb * B entries, zero padded):
+//   force:       p0 = (x, x, y, y)      p1 = (z, z, r^3, r^3)   k2 = (k r, k r)
+//   convection:  p0 = -(x, x, y, y)     p1 = (-z, -z, k r, k r)
+//                q0 = (Fx, Fx, Fy, Fy)  q1 = (Fz, Fz)
+// Coordinates are box-centred and scaled by 1/ell, forces by 2^-q (the scale
+// slots); the convection coordinates are stored negated so that d = x_i - x_j
+// is one packed add.
 struct SymArgs {
-    int n, nb, nitems;
-    const float4 *pos4;  // (x, y, z, r^3) scaled
-    const float *krf;    // force pass: k_f r scaled
-    const float4 *frc4;  // convection pass: (F scaled, k_o r scaled)
-    MixedArgs m;         // FP64 originals for the exact path
-    double *pi;          // [nitems][3][B]  i-side partials
-    double *pj;          // [nitems][3][B]  j-side partials (I < J)
+    int n, npad, nb, nitems;
+    const float4 *p0, *p1, *q0;
+    const float2 *k2, *q1;
+    MixedArgs m;  // FP64 originals for the exact path
+    double *pi;   // [nitems][3][B]  i-side partials
+    double *pj;   // [nitems][3][B]  j-side partials (I < J)
 };
 
 __host__ __device__ __forceinline__ long long rows_before(long long i, long long nb) {
@@ -51,12 +72,29 @@ __device__ __forceinline__ void decode_item(int q, int nb, int &I, int &J) {
     J = I + (int)(q - rows_before(I, nb));
 }
 
+template <bool PER>
+__device__ __forceinline__ float2 p_mic(float2 d, float2 invL, float2 magic, float2 nmagic, float2 nL) {
+    if (!PER) return d;
+    const float2 u = p_add(p_fma(d, invL, magic), nmagic);  // rint(d / L)
+    return p_fma(nL, u, d);
+}
+
+template <bool PER>
+__device__ __forceinline__ bool needs_exact(float r2, float sr2, float dx, float dy, float dz, float hm) {
+    bool e = r2 <= sr2;
+    if (PER) e = e || fabsf(dx) > hm || fabsf(dy) > hm || fabsf(dz) > hm;
+    return e;
+}
+
 template <int IPT, bool PER, bool FORCE>
 __global__ void __launch_bounds__(SYM_T, 4) mixed_sym_kernel(const SymArgs a) {
+    static_assert(IPT % 2 == 0, "two i's per packed operation");
     constexpr int B = SYM_T * IPT;
-    __shared__ __align__(128) float4 sA[2][TJ];
-    __shared__ __align__(128) float4 sB[2][TJ];
-    __shared__ __align__(128) float sK[2][TJ];
+    constexpr int KP = IPT / 2;
+    __shared__ __align__(128) float4 s0[2][TJ];
+    __shared__ __align__(128) float4 s1[2][TJ];
+    __shared__ __align__(128) float4 s2[2][FORCE ? 1 : TJ];
+    __shared__ __align__(128) float2 s3[2][TJ];
     __shared__ float jred[SYM_T / 32][3][TJ];
     __shared__ double jnear[SYM_T / 32][3][TJ];
     __shared__ __align__(8) uint64_t bar[2];
@@ -68,41 +106,44 @@ __global__ void __launch_bounds__(SYM_T, 4) mixed_sym_kernel(const SymArgs a) {
     decode_item(blockIdx.x, a.nb, I, J);
     const bool diag = (I == J);
     const int j0 = J * B;
-    const int j1 = min(n, j0 + B);
-    const int ntiles = j1 > j0 ? (j1 - j0 + TJ - 1) / TJ : 0;
+    constexpr int ntiles = B / TJ;
     const double inv_ell = pow2_inv_of(a.m.scales[0]);
     const double fscale_inv = FORCE ? 1.0 : pow2_inv_of(a.m.scales[1]);
     const float Ls = (float)(a.m.L * inv_ell);
-    const float invLs = (float)(1.0 / (a.m.L * inv_ell));
+    const float2 invL2 = dup2((float)(1.0 / (a.m.L * inv_ell)));
+    const float2 nL2 = dup2(-Ls);
+    const float2 magic2 = dup2(RINT_MAGIC), nmagic2 = dup2(-RINT_MAGIC);
     const float hm = (float)(a.m.L * inv_ell * (0.5 - MIC_MARGIN));
 
-    float xi[IPT], yi[IPT], zi[IPT], ki[IPT], wi[IPT];  // wi: r^3 (force) / unused
-    float fxi[IPT], fyi[IPT], fzi[IPT];                // convection: F_i scaled
-    float ax[IPT], ay[IPT], az[IPT], hx[IPT], hy[IPT], hz[IPT], lx[IPT], ly[IPT], lz[IPT];
-    int iidx[IPT];
+    // i state, two i's per packed register: k = 2 kp (.x) and 2 kp + 1 (.y)
+    float2 xi[KP], yi[KP], zi[KP], ki[KP], wi[KP];  // force: xi.. = -x_i; wi = r_i^3
+    float2 fxi[KP], fyi[KP], fzi[KP];                // convection: F_i
+    float2 ax[KP], ay[KP], az[KP];
+    float hx[IPT], hy[IPT], hz[IPT], lx[IPT], ly[IPT], lz[IPT];
 #pragma unroll
-    for (int k = 0; k < IPT; ++k) {
-        const int i = I * B + k * SYM_T + tid;
-        iidx[k] = i;
-        xi[k] = yi[k] = zi[k] = ki[k] = wi[k] = fxi[k] = fyi[k] = fzi[k] = 0.f;
-        if (i < n) {
-            const float4 p = a.pos4[i];
-            xi[k] = p.x;
-            yi[k] = p.y;
-            zi[k] = p.z;
-            wi[k] = p.w;
-            if (FORCE) {
-                ki[k] = a.krf[i];
-            } else {
-                const float4 f = a.frc4[i];
-                fxi[k] = f.x;
-                fyi[k] = f.y;
-                fzi[k] = f.z;
-                ki[k] = f.w;
-            }
+    for (int kp = 0; kp < KP; ++kp) {
+        const int ia = I * B + (2 * kp) * SYM_T + tid, ib = ia + SYM_T;
+        const float4 a0 = a.p0[ia], b0 = a.p0[ib], a1 = a.p1[ia], b1 = a.p1[ib];
+        if (FORCE) {  // d = x_j - x_i: keep -x_i
+            xi[kp] = make_float2(-a0.x, -b0.x);
+            yi[kp] = make_float2(-a0.z, -b0.z);
+            zi[kp] = make_float2(-a1.x, -b1.x);
+            wi[kp] = make_float2(a1.z, b1.z);
+            ki[kp] = make_float2(a.k2[ia].x, a.k2[ib].x);
+        } else {  // d = x_i - x_j, coordinates stored negated: keep +x_i
+            xi[kp] = make_float2(-a0.x, -b0.x);
+            yi[kp] = make_float2(-a0.z, -b0.z);
+            zi[kp] = make_float2(-a1.x, -b1.x);
+            ki[kp] = make_float2(a1.z, b1.z);
+            const float4 fa = a.q0[ia], fb = a.q0[ib];
+            fxi[kp] = make_float2(fa.x, fb.x);
+            fyi[kp] = make_float2(fa.z, fb.z);
+            fzi[kp] = make_float2(a.q1[ia].x, a.q1[ib].x);
         }
-        ax[k] = ay[k] = az[k] = hx[k] = hy[k] = hz[k] = lx[k] = ly[k] = lz[k] = 0.f;
+        ax[kp] = ay[kp] = az[kp] = make_float2(0.f, 0.f);
     }
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) hx[k] = hy[k] = hz[k] = lx[k] = ly[k] = lz[k] = 0.f;
 
     if (tid == 0) {
         mbar_init(&bar[0], 1);
@@ -114,22 +155,20 @@ __global__ void __launch_bounds__(SYM_T, 4) mixed_sym_kernel(const SymArgs a) {
 
     auto issue = [&](int t) {
         const int js = j0 + t * TJ;
-        const int cnt = min(TJ, j1 - js);
         const int b = t & 1;
-        const uint32_t bytes_a = (uint32_t)cnt * 16u;
+        constexpr uint32_t b4 = TJ * 16u, b2 = TJ * 8u;
+        mbar_arrive_expect_tx(&bar[b], FORCE ? 2 * b4 + b2 : 3 * b4 + b2);
+        tma_load_1d(s0[b], a.p0 + js, b4, &bar[b]);
+        tma_load_1d(s1[b], a.p1 + js, b4, &bar[b]);
         if (FORCE) {
-            const uint32_t bytes_k = (uint32_t)((cnt + 3) & ~3) * 4u;
-            mbar_arrive_expect_tx(&bar[b], bytes_a + bytes_k);
-            tma_load_1d(sA[b], a.pos4 + js, bytes_a, &bar[b]);
-            tma_load_1d(sK[b], a.krf + js, bytes_k, &bar[b]);
+            tma_load_1d(s3[b], a.k2 + js, b2, &bar[b]);
         } else {
-            mbar_arrive_expect_tx(&bar[b], 2u * bytes_a);
-            tma_load_1d(sA[b], a.pos4 + js, bytes_a, &bar[b]);
-            tma_load_1d(sB[b], a.frc4 + js, bytes_a, &bar[b]);
+            tma_load_1d(s2[b], a.q0 + js, b4, &bar[b]);
+            tma_load_1d(s3[b], a.q1 + js, b2, &bar[b]);
         }
     };
 
-    if (tid == 0 && ntiles > 0) issue(0);
+    if (tid == 0) issue(0);
     const size_t plane = (size_t)B;
     double *PJ = a.pj + (size_t)blockIdx.x * 3 * plane;
     bool aborted = false;
@@ -141,160 +180,163 @@ __global__ void __launch_bounds__(SYM_T, 4) mixed_sym_kernel(const SymArgs a) {
         const bool ok = mbar_wait_bounded(&bar[t & 1], (uint32_t)((t >> 1) & 1), a.m.err);
         if (!ok) s_abort = 1;
         const int js = j0 + t * TJ;
-        const int cnt = min(TJ, j1 - js);
         if (ok) {
-            const float4 *A = sA[t & 1];
-            const float4 *Bf = sB[t & 1];
-            const float *K = sK[t & 1];
-            // j-side sums of the j's this lane owns (j = 32 s + lane of the tile)
-            float jx[TJ / 32], jy[TJ / 32], jz[TJ / 32];
-#pragma unroll
-            for (int s = 0; s < TJ / 32; ++s) jx[s] = jy[s] = jz[s] = 0.f;
+            const float4 *S0 = s0[t & 1];
+            const float4 *S1 = s1[t & 1];
+            const float4 *S2 = s2[t & 1];
+            const float2 *S3 = s3[t & 1];
             if (!diag)
                 for (int q = lane; q < 3 * TJ; q += 32) (&jnear[warp][0][0])[q] = 0.0;
             __syncwarp();
 #pragma unroll
             for (int s = 0; s < TJ / 32; ++s) {
                 const int jjs = s * 32;
-                if (jjs >= cnt) break;
-                // Step st: lane l works on j = jjs + (l + st) mod 32, so the 32
-                // lanes hold 32 different j's.  (sx, sy, sz) is the running
-                // j-side sum of the j this lane holds; it moves to lane l - 1
-                // after every step and is back with lane l after 32 steps.
-                float sx = 0.f, sy = 0.f, sz = 0.f;
+                // Step st: lane l works on j = jjs + (l + st) mod 32.  (sx, sy, sz)
+                // is the running j-side sum of the j this lane holds (one half per
+                // i of the packed pair); it moves to lane l - 1 after every step.
+                float2 sx = make_float2(0.f, 0.f), sy = sx, sz = sx;
 #pragma unroll 1
                 for (int st = 0; st < 32; ++st) {
-                    const int jj_raw = jjs + ((lane + st) & 31);
-                    const bool valid = jj_raw < cnt;
-                    const int jj = valid ? jj_raw : jjs;  // a real droplet's data keeps every term finite
-                    const float4 pj = A[jj];
-                    float4 fj;
-                    float kj;
+                    const int jj = jjs + ((lane + st) & 31);
+                    const float4 A = S0[jj], Bv = S1[jj];
+                    const float2 pjx = make_float2(A.x, A.y), pjy = make_float2(A.z, A.w);
+                    const float2 pjz = make_float2(Bv.x, Bv.y);
+                    float2 wj, kj, fjx, fjy, fjz;
                     if (FORCE) {
-                        kj = K[jj];
+                        wj = make_float2(Bv.z, Bv.w);
+                        kj = S3[jj];
                     } else {
-                        fj = Bf[jj];
-                        kj = fj.w;
+                        kj = make_float2(Bv.z, Bv.w);
+                        const float4 Q = S2[jj];
+                        fjx = make_float2(Q.x, Q.y);
+                        fjy = make_float2(Q.z, Q.w);
+                        fjz = S3[jj];
                     }
-                    bool any_exact = false;
+                    bool ex[IPT];
 #pragma unroll
-                    for (int k = 0; k < IPT; ++k) {
-                        float dx, dy, dz, r2;
-                        const bool exact = pair_geometry<PER, FORCE>(pj, xi[k], yi[k], zi[k], ki[k], kj, Ls, invLs,
-                                                                      hm, dx, dy, dz, r2) ||
-                                           !valid;
-                        any_exact |= exact;
-                        float rinv = rsqrtf(r2);
+                    for (int kp = 0; kp < KP; ++kp) {
+                        float2 dx = p_add(pjx, xi[kp]), dy = p_add(pjy, yi[kp]), dz = p_add(pjz, zi[kp]);
+                        dx = p_mic<PER>(dx, invL2, magic2, nmagic2, nL2);
+                        dy = p_mic<PER>(dy, invL2, magic2, nmagic2, nL2);
+                        dz = p_mic<PER>(dz, invL2, magic2, nmagic2, nL2);
+                        const float2 r2 = p_fma(dx, dx, p_fma(dy, dy, p_mul(dz, dz)));
+                        const float2 sr = p_add(ki[kp], kj);
+                        const float2 sr2 = p_mul(sr, sr);
+                        const bool ea = needs_exact<PER>(r2.x, sr2.x, dx.x, dy.x, dz.x, hm);
+                        const bool eb = needs_exact<PER>(r2.y, sr2.y, dx.y, dy.y, dz.y, hm);
+                        ex[2 * kp] = ea;
+                        ex[2 * kp + 1] = eb;
+                        float2 rinv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
                         if (FORCE) {
-                            const float rinv2 = rinv * rinv;
-                            const float rinv3 = rinv2 * rinv;
-                            const float rinv4 = rinv2 * rinv2;
-                            const float base = exact ? 0.f : rinv4 * rinv3;  // r^-7
-                            const float ang = fmaf(5.f * dz, dz, -r2);
-                            const float angz = fmaf(-2.f, r2, ang);
-                            const float g = base * ang;
-                            const float tx = g * dx, ty = g * dy, tz = (base * angz) * dz;
-                            ax[k] = fmaf(pj.w, tx, ax[k]);  // force on i: r_j^3 P(d) / r^7
-                            ay[k] = fmaf(pj.w, ty, ay[k]);
-                            az[k] = fmaf(pj.w, tz, az[k]);
-                            if (!diag) {  // force on j: - r_i^3 P(d) / r^7
-                                sx = fmaf(-wi[k], tx, sx);
-                                sy = fmaf(-wi[k], ty, sy);
-                                sz = fmaf(-wi[k], tz, sz);
+                            // t = -P(d) / r^7 with P the reference's angular factor (:192-199):
+                            // P_xy = d_xy (4 dz^2 - dx^2 - dy^2) = -d_xy (r^2 - 5 dz^2),
+                            // P_z = dz (2 dz^2 - 3 dx^2 - 3 dy^2) = -dz (r^2 - 5 dz^2 + 2 r^2)
+                            const float2 rinv2 = p_mul(rinv, rinv);
+                            const float2 rinv4 = p_mul(rinv2, rinv2);
+                            float2 base = p_mul(rinv4, p_mul(rinv2, rinv));  // r^-7
+                            base.x = ea ? 0.f : base.x;
+                            base.y = eb ? 0.f : base.y;
+                            const float2 angp = p_fma(p_mul(dup2(-5.f), dz), dz, r2);
+                            const float2 angzp = p_fma(dup2(2.f), r2, angp);
+                            const float2 gp = p_mul(base, angp);
+                            const float2 tx = p_mul(gp, dx), ty = p_mul(gp, dy);
+                            const float2 tz = p_mul(p_mul(base, angzp), dz);
+                            // i side: sum r_j^3 t = -(force on i) / (m r_i^3); sign restored at the end
+                            ax[kp] = p_fma(wj, tx, ax[kp]);
+                            ay[kp] = p_fma(wj, ty, ay[kp]);
+                            az[kp] = p_fma(wj, tz, az[kp]);
+                            if (!diag) {  // force on j: r_i^3 P(-d) / r^7 = r_i^3 t
+                                sx = p_fma(wi[kp], tx, sx);
+                                sy = p_fma(wi[kp], ty, sy);
+                                sz = p_fma(wi[kp], tz, sz);
                             }
                         } else {
-                            rinv = exact ? 0.f : rinv;
-                            const float rinv2 = rinv * rinv;
-                            const float dot = fmaf(dx, fj.x, fmaf(dy, fj.y, dz * fj.z));
-                            const float sc = dot * rinv2;
-                            ax[k] = fmaf(rinv, fmaf(dx, sc, fj.x), ax[k]);
-                            ay[k] = fmaf(rinv, fmaf(dy, sc, fj.y), ay[k]);
-                            az[k] = fmaf(rinv, fmaf(dz, sc, fj.z), az[k]);
-                            if (!diag) {  // velocity at j: same tensor applied to F_i
-                                const float doti = fmaf(dx, fxi[k], fmaf(dy, fyi[k], dz * fzi[k]));
-                                const float sci = doti * rinv2;
-                                sx = fmaf(rinv, fmaf(dx, sci, fxi[k]), sx);
-                                sy = fmaf(rinv, fmaf(dy, sci, fyi[k]), sy);
-                                sz = fmaf(rinv, fmaf(dz, sci, fzi[k]), sz);
+                            rinv.x = ea ? 0.f : rinv.x;
+                            rinv.y = eb ? 0.f : rinv.y;
+                            const float2 rinv2 = p_mul(rinv, rinv);
+                            const float2 dot = p_fma(dx, fjx, p_fma(dy, fjy, p_mul(dz, fjz)));
+                            const float2 sc = p_mul(dot, rinv2);
+                            ax[kp] = p_fma(rinv, p_fma(dx, sc, fjx), ax[kp]);
+                            ay[kp] = p_fma(rinv, p_fma(dy, sc, fjy), ay[kp]);
+                            az[kp] = p_fma(rinv, p_fma(dz, sc, fjz), az[kp]);
+                            if (!diag) {  // velocity at j: the same (even) tensor applied to F_i
+                                const float2 doti = p_fma(dx, fxi[kp], p_fma(dy, fyi[kp], p_mul(dz, fzi[kp])));
+                                const float2 sci = p_mul(doti, rinv2);
+                                sx = p_fma(rinv, p_fma(dx, sci, fxi[kp]), sx);
+                                sy = p_fma(rinv, p_fma(dy, sci, fyi[kp]), sy);
+                                sz = p_fma(rinv, p_fma(dz, sci, fzi[kp]), sz);
                             }
                         }
                     }
+                    bool any = false;
+#pragma unroll
+                    for (int k = 0; k < IPT; ++k) any |= ex[k];
                     // Rare: exact FP64 terms.  The lanes hold different j's, so
                     // each lane adds its j-side terms to its own j's slot.
-                    if (__any_sync(0xffffffffu, any_exact)) {
-                        if (any_exact && valid) {
-                            const int j = js + jj;
-                            double ex = 0.0, ey = 0.0, ez = 0.0;
+                    if (__any_sync(0xffffffffu, any)) {
+                        const int j = js + jj;
+                        if (any && j < n) {
+                            double ex_ = 0.0, ey_ = 0.0, ez_ = 0.0;
 #pragma unroll
                             for (int k = 0; k < IPT; ++k) {
-                                float dx, dy, dz, r2;
-                                const bool exact = pair_geometry<PER, FORCE>(pj, xi[k], yi[k], zi[k], ki[k], kj, Ls,
-                                                                              invLs, hm, dx, dy, dz, r2);
-                                if (exact && iidx[k] < n) {
-                                    const double3 v = FORCE ? near_force_fp64(iidx[k], j, a.m, PER ? 1 : 0, inv_ell)
-                                                            : near_oseen_fp64(iidx[k], j, a.m, PER ? 1 : 0, inv_ell,
+                                const int i = I * B + k * SYM_T + tid;
+                                if (ex[k] && i < n) {
+                                    const double3 v = FORCE ? near_force_fp64(i, j, a.m, PER ? 1 : 0, inv_ell)
+                                                            : near_oseen_fp64(i, j, a.m, PER ? 1 : 0, inv_ell,
                                                                               fscale_inv);
-                                    fold_double(hx[k], lx[k], v.x);
-                                    fold_double(hy[k], ly[k], v.y);
-                                    fold_double(hz[k], lz[k], v.z);
+                                    const double sg = FORCE ? -1.0 : 1.0;  // the force i side is held negated
+                                    fold_double(hx[k], lx[k], sg * v.x);
+                                    fold_double(hy[k], ly[k], sg * v.y);
+                                    fold_double(hz[k], lz[k], sg * v.z);
                                     if (!diag) {
                                         const double3 w = FORCE
-                                                              ? near_force_fp64(j, iidx[k], a.m, PER ? 1 : 0, inv_ell)
-                                                              : near_oseen_fp64(j, iidx[k], a.m, PER ? 1 : 0, inv_ell,
+                                                              ? near_force_fp64(j, i, a.m, PER ? 1 : 0, inv_ell)
+                                                              : near_oseen_fp64(j, i, a.m, PER ? 1 : 0, inv_ell,
                                                                                 fscale_inv);
-                                        ex += w.x;
-                                        ey += w.y;
-                                        ez += w.z;
+                                        ex_ += w.x;
+                                        ey_ += w.y;
+                                        ez_ += w.z;
                                     }
                                 }
                             }
                             if (!diag) {
-                                jnear[warp][0][jj] += ex;
-                                jnear[warp][1][jj] += ey;
-                                jnear[warp][2][jj] += ez;
+                                jnear[warp][0][jj] += ex_;
+                                jnear[warp][1][jj] += ey_;
+                                jnear[warp][2][jj] += ez_;
                             }
                         }
                     }
                     if (!diag) {  // pass the running j-side sum to lane - 1
                         const int src = (lane + 1) & 31;
-                        sx = __shfl_sync(0xffffffffu, sx, src);
-                        sy = __shfl_sync(0xffffffffu, sy, src);
-                        sz = __shfl_sync(0xffffffffu, sz, src);
+                        sx.x = __shfl_sync(0xffffffffu, sx.x, src);
+                        sx.y = __shfl_sync(0xffffffffu, sx.y, src);
+                        sy.x = __shfl_sync(0xffffffffu, sy.x, src);
+                        sy.y = __shfl_sync(0xffffffffu, sy.y, src);
+                        sz.x = __shfl_sync(0xffffffffu, sz.x, src);
+                        sz.y = __shfl_sync(0xffffffffu, sz.y, src);
                     }
                 }
-                if (!diag) {
-                    jx[s] = sx;
-                    jy[s] = sy;
-                    jz[s] = sz;
+                if (!diag) {  // the sums are back with the lanes owning their j's
+                    jred[warp][0][jjs + lane] = sx.x + sx.y;
+                    jred[warp][1][jjs + lane] = sy.x + sy.y;
+                    jred[warp][2][jjs + lane] = sz.x + sz.y;
                 }
                 if (s & 1) {  // fold the FP32 i-side runs every 64 j
 #pragma unroll
-                    for (int k = 0; k < IPT; ++k) {
-                        two_sum_fold(hx[k], lx[k], ax[k]);
-                        two_sum_fold(hy[k], ly[k], ay[k]);
-                        two_sum_fold(hz[k], lz[k], az[k]);
-                        ax[k] = ay[k] = az[k] = 0.f;
+                    for (int kp = 0; kp < KP; ++kp) {
+                        two_sum_fold(hx[2 * kp], lx[2 * kp], ax[kp].x);
+                        two_sum_fold(hx[2 * kp + 1], lx[2 * kp + 1], ax[kp].y);
+                        two_sum_fold(hy[2 * kp], ly[2 * kp], ay[kp].x);
+                        two_sum_fold(hy[2 * kp + 1], ly[2 * kp + 1], ay[kp].y);
+                        two_sum_fold(hz[2 * kp], lz[2 * kp], az[kp].x);
+                        two_sum_fold(hz[2 * kp + 1], lz[2 * kp + 1], az[kp].y);
+                        ax[kp] = ay[kp] = az[kp] = make_float2(0.f, 0.f);
                     }
-                }
-            }
-#pragma unroll
-            for (int k = 0; k < IPT; ++k) {
-                two_sum_fold(hx[k], lx[k], ax[k]);
-                two_sum_fold(hy[k], ly[k], ay[k]);
-                two_sum_fold(hz[k], lz[k], az[k]);
-                ax[k] = ay[k] = az[k] = 0.f;
-            }
-            if (!diag) {
-#pragma unroll
-                for (int s = 0; s < TJ / 32; ++s) {
-                    jred[warp][0][s * 32 + lane] = jx[s];
-                    jred[warp][1][s * 32 + lane] = jy[s];
-                    jred[warp][2][s * 32 + lane] = jz[s];
                 }
             }
         }
         __syncthreads();
-        if (ok && !diag && tid < cnt) {  // combine the warps in a fixed order
+        if (ok && !diag) {  // combine the warps in a fixed order
             const int lj = t * TJ + tid;
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
@@ -313,12 +355,51 @@ __global__ void __launch_bounds__(SYM_T, 4) mixed_sym_kernel(const SymArgs a) {
     }
     if (aborted) return;
     double *PI = a.pi + (size_t)blockIdx.x * 3 * plane;
+    const double sg = FORCE ? -1.0 : 1.0;
 #pragma unroll
     for (int k = 0; k < IPT; ++k) {
         const int li = k * SYM_T + tid;
-        PI[li] = (double)hx[k] + (double)lx[k];
-        PI[plane + li] = (double)hy[k] + (double)ly[k];
-        PI[2 * plane + li] = (double)hz[k] + (double)lz[k];
+        PI[li] = sg * ((double)hx[k] + (double)lx[k]);
+        PI[plane + li] = sg * ((double)hy[k] + (double)ly[k]);
+        PI[2 * plane + li] = sg * ((double)hz[k] + (double)lz[k]);
+    }
+}
+
+// Packed, zero-padded layout of the symmetric passes (see SymArgs).
+template <bool FORCE>
+__global__ void prep_sym_kernel(int n, int npad, const double *__restrict__ x, const double *__restrict__ y,
+                                const double *__restrict__ z, const double *__restrict__ r,
+                                const double *__restrict__ fx, const double *__restrict__ fy,
+                                const double *__restrict__ fz, double center,
+                                const unsigned long long *__restrict__ scales, double k_near, float4 *__restrict__ p0,
+                                float4 *__restrict__ p1, float4 *__restrict__ q0, float2 *__restrict__ k2q1) {
+    const double s = pow2_inv_of(scales[0]);
+    const double q = FORCE ? 1.0 : pow2_inv_of(scales[1]);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npad; i += gridDim.x * blockDim.x) {
+        float X = 0.f, Y = 0.f, Z = 0.f, W = 0.f, K = 0.f, Fx = 0.f, Fy = 0.f, Fz = 0.f;
+        if (i < n) {
+            const double rs = r[i] * s;
+            X = (float)((x[i] - center) * s);
+            Y = (float)((y[i] - center) * s);
+            Z = (float)((z[i] - center) * s);
+            W = (float)(rs * rs * rs);
+            K = (float)(k_near * rs);
+            if (!FORCE) {
+                Fx = (float)(fx[i] * q);
+                Fy = (float)(fy[i] * q);
+                Fz = (float)(fz[i] * q);
+            }
+        }
+        if (FORCE) {
+            p0[i] = make_float4(X, X, Y, Y);
+            p1[i] = make_float4(Z, Z, W, W);
+            k2q1[i] = make_float2(K, K);
+        } else {
+            p0[i] = make_float4(-X, -X, -Y, -Y);
+            p1[i] = make_float4(-Z, -Z, K, K);
+            q0[i] = make_float4(Fx, Fx, Fy, Fy);
+            k2q1[i] = make_float2(Fz, Fz);
+        }
     }
 }
 
@@ -370,39 +451,57 @@ static void launch_sym(bool per, const SymArgs &a, cudaStream_t s) {
         mixed_sym_kernel<IPT, false, FORCE><<<a.nitems, SYM_T, 0, counted(s)>>>(a);
 }
 
-// Bytes of partial sums the symmetric schedule needs for n droplets.
+static size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+// Workspace of the symmetric schedule for n droplets: the packed layout
+// (64 bytes per padded droplet) followed by the per-block-pair partial sums.
 size_t sym_partial_bytes(int n, int ipt) {
     const long long B = (long long)SYM_T * ipt;
     const long long nb = (n + B - 1) / B;
     const long long items = nb * (nb + 1) / 2;
-    return (size_t)(2 * items * 3 * B) * sizeof(double);
+    return align256((size_t)(nb * B) * 64) + (size_t)(2 * items * 3 * B) * sizeof(double);
 }
 
-// Runs the symmetric pass; prep kernels have already filled pos4/krf/frc4 and
-// the scale slots.  `partial` holds sym_partial_bytes(n, ipt) bytes.
+// Runs the symmetric pass: packs the inputs, evaluates the block pairs and
+// reduces per droplet.  The scale slots (max r; max |F| for convection) are
+// already filled.  `work` holds sym_partial_bytes(n, ipt) bytes.
 template <bool FORCE>
-int run_sym_pass(dem_ctx *ctx, int n, int ipt, bool per, const MixedArgs &m, double *partial, const double *r,
+int run_sym_pass(dem_ctx *ctx, int n, int ipt, bool per, const MixedArgs &m, double *work, const double *r,
                  double coeff, double *ox, double *oy, double *oz, cudaStream_t s) {
+    ipt = ipt >= 4 ? 4 : 2;
     const int B = SYM_T * ipt;
     const int nb = (n + B - 1) / B;
     const long long items = (long long)nb * (nb + 1) / 2;
     if (items > 0x7fffffffLL) return dem_set_error(ctx, DEM_E_CAPACITY, "symmetric schedule: too many blocks");
+    const int npad = nb * B;
+    char *base = reinterpret_cast<char *>(work);
+    float4 *p0 = reinterpret_cast<float4 *>(base);
+    float4 *p1 = p0 + npad;
+    float4 *q0 = p1 + npad;
+    float2 *k2q1 = reinterpret_cast<float2 *>(q0 + npad);
+    const int pgrid = max(1, min(ceil_div(npad, 256), 4 * ctx->sm_count));
+    prep_sym_kernel<FORCE><<<pgrid, 256, 0, counted(s)>>>(n, npad, m.x, m.y, m.z, r, m.fx, m.fy, m.fz, 0.5 * m.L,
+                                                          m.scales, FORCE ? ctx->tuning.near_force
+                                                                          : ctx->tuning.near_oseen,
+                                                          p0, p1, q0, k2q1);
     SymArgs a;
     a.n = n;
+    a.npad = npad;
     a.nb = nb;
     a.nitems = (int)items;
-    a.pos4 = m.pos4;
-    a.krf = m.krf;
-    a.frc4 = m.frc4;
+    a.p0 = p0;
+    a.p1 = p1;
+    a.q0 = q0;
+    a.k2 = k2q1;
+    a.q1 = k2q1;
     a.m = m;
-    a.pi = partial;
-    a.pj = partial + (size_t)items * 3 * B;
+    a.pi = reinterpret_cast<double *>(base + align256((size_t)npad * 64));
+    a.pj = a.pi + (size_t)items * 3 * B;
     dem_prof_begin(ctx, FORCE ? "mixed_force_pass" : "mixed_convection_pass", s);
-    switch (ipt) {
-        case 1: launch_sym<1, FORCE>(per, a, s); break;
-        case 2: launch_sym<2, FORCE>(per, a, s); break;
-        default: launch_sym<4, FORCE>(per, a, s); break;
-    }
+    if (ipt == 4)
+        launch_sym<4, FORCE>(per, a, s);
+    else
+        launch_sym<2, FORCE>(per, a, s);
     dem_prof_end(ctx, s);
     int rc = dem_check_launch(ctx, FORCE ? "mixed force (symmetric)" : "mixed convection (symmetric)");
     if (rc) return rc;
