@@ -106,6 +106,56 @@ DEM_API int dem_direct_get_tuning(const dem_ctx *ctx, int *i_per_thread, int *th
 DEM_API int dem_direct_plan(const dem_ctx *ctx, int n, int periodic, int *schedule, int *i_per_thread,
                             int *threads, long long *ctas, int *j_splits);
 
+/* ---- ensembles of independent boxes ---------------------------------- */
+/* main_multi.py:52-77 runs one direct simulation per initial state, one after
+ * another, without a collision detector.  A batch steps many such boxes
+ * together: droplets [offsets[b], offsets[b+1]) of the caller's SoA arrays live
+ * in a periodic (or open) box of side L[b]; every pass is one set of launches
+ * over all boxes (the mixed-precision symmetric pair kernel walks the block
+ * pairs of every box in one grid).  Per box the results are bit-identical to
+ * the single-box mixed-precision calls with the same i-per-thread blocking.
+ * offsets (host, nbox + 1 entries, offsets[0] = 0, non-decreasing) and L
+ * (host, nbox) are copied.  The batch keeps its own workspace; it uses the
+ * context's device, error word and near-pair factors. */
+typedef struct dem_batch dem_batch;
+DEM_API int dem_batch_create(dem_ctx *ctx, int nbox, const int64_t *offsets, const double *L, int periodic,
+                             dem_batch **out);
+DEM_API void dem_batch_destroy(dem_batch *batch);
+/* Boxes, droplets and block pairs per pass for i-per-thread 2 and 4. */
+DEM_API int dem_batch_info(const dem_batch *batch, int *nbox, int *n, int *items_ipt2, int *items_ipt4);
+/* i_per_thread 2 or 4 (block size 256 / 512); ctas = 0: one CTA per block
+ * pair, else a persistent grid of that many CTAs. */
+DEM_API int dem_batch_set_tuning(dem_batch *batch, int i_per_thread, int ctas);
+DEM_API int dem_batch_get_tuning(const dem_batch *batch, int *i_per_thread, int *ctas);
+/* Forces / convection of every box (mixed precision; as dem_direct_forces and
+ * dem_direct_convection per box). */
+DEM_API int dem_batch_forces(dem_batch *batch, const double *x, const double *y, const double *z, const double *r,
+                             double m_const, double *fx, double *fy, double *fz, void *stream);
+DEM_API int dem_batch_convection(dem_batch *batch, const double *x, const double *y, const double *z,
+                                 const double *r, const double *fx, const double *fy, const double *fz,
+                                 double eta_const, double *vx, double *vy, double *vz, void *stream);
+/* One Euler step of every box, in place (euler_droplet_solver.py:121-131 per
+ * box): forces, convection, x += (F / (stokes_factor r) + v) dt, x %= L[b].
+ * f* and v* receive this step's forces and convection velocities. */
+DEM_API int dem_batch_step(dem_batch *batch, double *x, double *y, double *z, const double *r, double m_const,
+                           double eta_const, double stokes_factor, double dt, double *fx, double *fy, double *fz,
+                           double *vx, double *vy, double *vz, void *stream);
+/* Times every candidate tiling (i per thread 2 / 4 x one CTA per block pair or
+ * a persistent grid of 1, 2, 4 x the resident CTA slots) over `reps` force +
+ * convection passes on these inputs and keeps the fastest.  Synchronises
+ * `stream`; overwrites f* and v* with valid results; best_ms (host, may be
+ * NULL) receives the best time per force + convection pair of passes. */
+DEM_API int dem_batch_autotune(dem_batch *batch, const double *x, const double *y, const double *z, const double *r,
+                               double m_const, double eta_const, double *fx, double *fy, double *fz, double *vx,
+                               double *vy, double *vz, int reps, void *stream, double *best_ms);
+/* Records one dem_batch_step on these buffers as a CUDA graph (nothing runs);
+ * dem_batch_replay launches it `steps` times on `stream`.  The graph keeps the
+ * pointers and scalars given here; a new capture replaces the old one. */
+DEM_API int dem_batch_capture(dem_batch *batch, double *x, double *y, double *z, const double *r, double m_const,
+                              double eta_const, double stokes_factor, double dt, double *fx, double *fy, double *fz,
+                              double *vx, double *vy, double *vz);
+DEM_API int dem_batch_replay(dem_batch *batch, int steps, void *stream);
+
 /* ---- layout ---------------------------------------------------------- */
 /* (n, 3) row-major <-> three component arrays.  The reference's public
  * methods take and return (N, 3) numpy arrays

@@ -16,6 +16,9 @@ cudaStream_t counted(cudaStream_t s) {
 
 unsigned long long dem_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
+// Kernels launched by a CUDA graph replay (they bypass counted()).
+void dem_count_launches(unsigned long long k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+
 namespace dem {
 int direct_plan(const dem_ctx *ctx, int n, int periodic, int *schedule, int *i_per_thread, int *threads,
                 long long *ctas, int *j_splits);

@@ -159,9 +159,9 @@ __global__ void __launch_bounds__(512) mixed_pass_kernel(const MixedArgs a) {
                                 const bool exact = pair_geometry<PER, FORCE>(pj, xi[k], yi[k], zi[k], ki[k], kj, Ls,
                                                                               invLs, hm, dx, dy, dz, r2);
                                 if (exact && iidx[k] < n) {
-                                    const double3 v = FORCE ? near_force_fp64(iidx[k], j, a, PER ? 1 : 0, inv_ell)
+                                    const double3 v = FORCE ? near_force_fp64(iidx[k], j, a, PER ? 1 : 0, inv_ell, a.L)
                                                             : near_oseen_fp64(iidx[k], j, a, PER ? 1 : 0, inv_ell,
-                                                                              fscale_inv);
+                                                                              fscale_inv, a.L);
                                     fold_double(hx[k], lx[k], v.x);
                                     fold_double(hy[k], ly[k], v.y);
                                     fold_double(hz[k], lz[k], v.z);

@@ -48,6 +48,50 @@ __global__ void euler_total_kernel(int n, const double *__restrict__ x, const do
     }
 }
 
+// Several independent boxes: droplets [off[b], off[b+1]) live in a box of side L[b].
+__global__ void euler_direct_boxes_kernel(int n, int nbox, const int *__restrict__ off, const double *__restrict__ Lb,
+                                          const double *__restrict__ x, const double *__restrict__ y,
+                                          const double *__restrict__ z, const double *__restrict__ r,
+                                          const double *__restrict__ fx, const double *__restrict__ fy,
+                                          const double *__restrict__ fz, const double *__restrict__ vx,
+                                          const double *__restrict__ vy, const double *__restrict__ vz, double stokes,
+                                          double dt, int periodic, double *xo, double *yo, double *zo) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int lo = 0, hi = nbox - 1;  // box of droplet i: the last b with off[b] <= i
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (off[mid] <= i)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const double L = Lb[lo];
+        const double denom = stokes * r[i];
+        double px = x[i] + (fx[i] / denom + vx[i]) * dt;
+        double py = y[i] + (fy[i] / denom + vy[i]) * dt;
+        double pz = z[i] + (fz[i] / denom + vz[i]) * dt;
+        if (periodic) {
+            px = np_remainder(px, L);
+            py = np_remainder(py, L);
+            pz = np_remainder(pz, L);
+        }
+        xo[i] = px;
+        yo[i] = py;
+        zo[i] = pz;
+    }
+}
+
+int launch_euler_direct_boxes(dem_ctx *ctx, int n, int nbox, const int *off, const double *Lb, const double *x,
+                              const double *y, const double *z, const double *r, const double *fx, const double *fy,
+                              const double *fz, const double *vx, const double *vy, const double *vz, double stokes,
+                              double dt, int periodic, double *xo, double *yo, double *zo, cudaStream_t s) {
+    if (n == 0) return DEM_OK;
+    const int grid = min(ceil_div(n, 256), 8 * ctx->sm_count);
+    euler_direct_boxes_kernel<<<grid, 256, 0, counted(s)>>>(n, nbox, off, Lb, x, y, z, r, fx, fy, fz, vx, vy, vz, stokes,
+                                                            dt, periodic, xo, yo, zo);
+    return dem_check_launch(ctx, "euler_direct (boxes)");
+}
+
 int launch_euler_direct(dem_ctx *ctx, int n, const double *x, const double *y, const double *z, const double *r,
                         const double *fx, const double *fy, const double *fz, const double *vx, const double *vy,
                         const double *vz, double stokes, double dt, double L, int periodic, double *xo, double *yo,

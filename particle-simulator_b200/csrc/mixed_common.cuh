@@ -82,15 +82,17 @@ __device__ __forceinline__ bool pair_geometry(const float4 &pj, float xi, float 
     return exact;
 }
 
-// FP64 pair terms in scaled units (lengths / ell), reference formulas.
-static __device__ __noinline__ double3 near_force_fp64(int i, int j, const MixedArgs a, int periodic, double inv_ell) {
+// FP64 pair terms in scaled units (lengths / ell), reference formulas; L is
+// the side of the box the pair lives in.
+static __device__ __noinline__ double3 near_force_fp64(int i, int j, const MixedArgs a, int periodic, double inv_ell,
+                                                       double L) {
     double3 o = make_double3(0.0, 0.0, 0.0);
     if (i == j) return o;
     double dx = a.x[j] - a.x[i], dy = a.y[j] - a.y[i], dz = a.z[j] - a.z[i];
     if (periodic) {
-        dx = mic64(dx, a.L, a.halfL);
-        dy = mic64(dy, a.L, a.halfL);
-        dz = mic64(dz, a.L, a.halfL);
+        dx = mic64(dx, L, 0.5 * L);
+        dy = mic64(dy, L, 0.5 * L);
+        dz = mic64(dz, L, 0.5 * L);
     }
     const double r_mag = sqrt(dx * dx + dy * dy + dz * dz);
     if (!(r_mag > a.r[i] + a.r[j])) return o;  // contact cut, :246
@@ -109,14 +111,14 @@ static __device__ __noinline__ double3 near_force_fp64(int i, int j, const Mixed
 }
 
 static __device__ __noinline__ double3 near_oseen_fp64(int i, int j, const MixedArgs a, int periodic, double inv_ell,
-                                                double fscale_inv) {
+                                                       double fscale_inv, double L) {
     double3 o = make_double3(0.0, 0.0, 0.0);
     if (i == j) return o;
     double X = a.x[i] - a.x[j], Y = a.y[i] - a.y[j], Z = a.z[i] - a.z[j];
     if (periodic) {
-        X = mic64(X, a.L, a.halfL);
-        Y = mic64(Y, a.L, a.halfL);
-        Z = mic64(Z, a.L, a.halfL);
+        X = mic64(X, L, 0.5 * L);
+        Y = mic64(Y, L, 0.5 * L);
+        Z = mic64(Z, L, 0.5 * L);
     }
     const double s = inv_ell;
     X *= s;

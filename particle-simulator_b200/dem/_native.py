@@ -56,6 +56,18 @@ SIGNATURES = {
                                    C.POINTER(_i)]),
     "dem_direct_plan": (_i, [_vp, _i, _i, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i), C.POINTER(C.c_longlong),
                              C.POINTER(_i)]),
+    "dem_batch_create": (_i, [_vp, _i, C.POINTER(_i64), C.POINTER(_d), _i, C.POINTER(_vp)]),
+    "dem_batch_destroy": (None, [_vp]),
+    "dem_batch_info": (_i, [_vp, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i), C.POINTER(_i)]),
+    "dem_batch_set_tuning": (_i, [_vp, _i, _i]),
+    "dem_batch_get_tuning": (_i, [_vp, C.POINTER(_i), C.POINTER(_i)]),
+    "dem_batch_forces": (_i, [_vp, _vp, _vp, _vp, _vp, _d, _vp, _vp, _vp, _vp]),
+    "dem_batch_convection": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _d, _vp, _vp, _vp, _vp]),
+    "dem_batch_step": (_i, [_vp, _vp, _vp, _vp, _vp, _d, _d, _d, _d, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "dem_batch_autotune": (_i, [_vp, _vp, _vp, _vp, _vp, _d, _d, _vp, _vp, _vp, _vp, _vp, _vp, _i, _vp,
+                                C.POINTER(_d)]),
+    "dem_batch_capture": (_i, [_vp, _vp, _vp, _vp, _vp, _d, _d, _d, _d, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "dem_batch_replay": (_i, [_vp, _i, _vp]),
     "dem_aos_to_soa": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp]),
     "dem_soa_to_aos": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp]),
     "dem_direct_forces": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _d, _d, _i, _i, _vp, _vp, _vp, _vp]),
@@ -338,6 +350,77 @@ class Tree:
 
     def leaf_indices(self, out):
         self.ctx._check(lib().dem_tree_leaf_indices(self.handle, ptr(out), self.ctx.stream()), "tree_leaf_indices")
+
+
+class Batch:
+    """One ``dem_batch``: independent boxes, droplets [offsets[b], offsets[b+1])."""
+
+    def __init__(self, ctx: Context, offsets, L, periodic: bool):
+        self.ctx = ctx
+        off = np.ascontiguousarray(offsets, dtype=np.int64)
+        Ls = np.ascontiguousarray(L, dtype=np.float64)
+        self.nbox = len(Ls)
+        if len(off) != self.nbox + 1:
+            raise ValueError("offsets must have one entry more than L")
+        self.handle = _vp()
+        ctx._check(lib().dem_batch_create(ctx.handle, self.nbox, off.ctypes.data_as(C.POINTER(_i64)),
+                                          Ls.ctypes.data_as(C.POINTER(_d)), int(bool(periodic)),
+                                          C.byref(self.handle)), "batch_create")
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value and _lib is not None:
+            try:
+                _lib.dem_batch_destroy(h)
+            except Exception:  # pragma: no cover
+                pass
+            self.handle = None
+
+    def info(self):
+        a, b, c, d = _i(), _i(), _i(), _i()
+        self.ctx._check(lib().dem_batch_info(self.handle, C.byref(a), C.byref(b), C.byref(c), C.byref(d)), "info")
+        return dict(nbox=a.value, n=b.value, items_ipt2=c.value, items_ipt4=d.value)
+
+    def set_tuning(self, i_per_thread=4, ctas=0):
+        self.ctx._check(lib().dem_batch_set_tuning(self.handle, int(i_per_thread), int(ctas)), "batch_set_tuning")
+
+    def get_tuning(self):
+        a, b = _i(), _i()
+        self.ctx._check(lib().dem_batch_get_tuning(self.handle, C.byref(a), C.byref(b)), "batch_get_tuning")
+        return dict(i_per_thread=a.value, ctas=b.value)
+
+    def forces(self, pos, r, m_const, out):
+        self.ctx._check(lib().dem_batch_forces(self.handle, ptr(pos[0]), ptr(pos[1]), ptr(pos[2]), ptr(r),
+                                               float(m_const), ptr(out[0]), ptr(out[1]), ptr(out[2]),
+                                               self.ctx.stream()), "batch_forces")
+
+    def convection(self, pos, r, F, eta_const, out):
+        self.ctx._check(lib().dem_batch_convection(self.handle, ptr(pos[0]), ptr(pos[1]), ptr(pos[2]), ptr(r),
+                                                   ptr(F[0]), ptr(F[1]), ptr(F[2]), float(eta_const), ptr(out[0]),
+                                                   ptr(out[1]), ptr(out[2]), self.ctx.stream()), "batch_convection")
+
+    def step(self, pos, r, m_const, eta_const, stokes, dt, F, V):
+        self.ctx._check(lib().dem_batch_step(self.handle, ptr(pos[0]), ptr(pos[1]), ptr(pos[2]), ptr(r),
+                                             float(m_const), float(eta_const), float(stokes), float(dt), ptr(F[0]),
+                                             ptr(F[1]), ptr(F[2]), ptr(V[0]), ptr(V[1]), ptr(V[2]),
+                                             self.ctx.stream()), "batch_step")
+
+    def autotune(self, pos, r, m_const, eta_const, F, V, reps=3):
+        best = _d()
+        self.ctx._check(lib().dem_batch_autotune(self.handle, ptr(pos[0]), ptr(pos[1]), ptr(pos[2]), ptr(r),
+                                                 float(m_const), float(eta_const), ptr(F[0]), ptr(F[1]), ptr(F[2]),
+                                                 ptr(V[0]), ptr(V[1]), ptr(V[2]), int(reps), self.ctx.stream(),
+                                                 C.byref(best)), "batch_autotune")
+        return float(best.value)
+
+    def capture(self, pos, r, m_const, eta_const, stokes, dt, F, V):
+        self.ctx._check(lib().dem_batch_capture(self.handle, ptr(pos[0]), ptr(pos[1]), ptr(pos[2]), ptr(r),
+                                                float(m_const), float(eta_const), float(stokes), float(dt),
+                                                ptr(F[0]), ptr(F[1]), ptr(F[2]), ptr(V[0]), ptr(V[1]), ptr(V[2])),
+                        "batch_capture")
+
+    def replay(self, steps):
+        self.ctx._check(lib().dem_batch_replay(self.handle, int(steps), self.ctx.stream()), "batch_replay")
 
 
 class Buffers:
