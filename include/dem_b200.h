@@ -106,6 +106,24 @@ DEM_API int dem_direct_get_tuning(const dem_ctx *ctx, int *i_per_thread, int *th
 DEM_API int dem_direct_plan(const dem_ctx *ctx, int n, int periodic, int *schedule, int *i_per_thread,
                             int *threads, long long *ctas, int *j_splits);
 
+/* ---- adjoint of the direct step --------------------------------------- */
+/* Vector-Jacobian product of the direct-path droplet velocity
+ *   u_i = F_i / (stokes_factor r_i) + V_i    (euler_droplet_solver.py:121-125)
+ * with F the dipole forces (direct_droplet_force_calculator.py:183-253, contact
+ * cut |d| > r_i + r_j) and V the Oseen convection of F (:354-411), in FP64.
+ * Given the cotangent lambda on u (l*), returns
+ *   g*_i = sum_k lambda_k . du_k/dx_i,  gr_i = sum_k lambda_k . du_k/dr_i,
+ * and mu (m*), the cotangent reaching the forces:
+ *   mu_i = lambda_i / (stokes_factor r_i) + eta sum_{j != i} G(x_i - x_j) lambda_j.
+ * f* must hold the forces of this state (dem_direct_forces, FP64 or mixed).
+ * The collision cut and the periodic wrap are treated as non-differentiable;
+ * d/dE of u is 2 u / E (m_const is proportional to E^2) and needs no call. */
+DEM_API int dem_direct_vjp(dem_ctx *ctx, int n, const double *x, const double *y, const double *z, const double *r,
+                           const double *fx, const double *fy, const double *fz, const double *lx, const double *ly,
+                           const double *lz, double m_const, double eta_const, double stokes_factor, double L,
+                           int periodic, double *mx, double *my, double *mz, double *gx, double *gy, double *gz,
+                           double *gr, void *stream);
+
 /* ---- ensembles of independent boxes ---------------------------------- */
 /* main_multi.py:52-77 runs one direct simulation per initial state, one after
  * another, without a collision detector.  A batch steps many such boxes

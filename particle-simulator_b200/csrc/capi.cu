@@ -22,6 +22,10 @@ int launch_hash_detect(dem_ctx *, int, const double *, const double *, const dou
                        int, int32_t *, int64_t, int64_t *, cudaStream_t);
 int launch_merge(dem_ctx *, int, const double *, const double *, const double *, const double *, const int32_t *,
                  const int64_t *, double *, double *, double *, double *, int32_t *, int32_t *, cudaStream_t);
+int launch_direct_vjp(dem_ctx *, int, const double *, const double *, const double *, const double *, const double *,
+                      const double *, const double *, const double *, const double *, const double *, double, double,
+                      double, double, int, double *, double *, double *, double *, double *, double *, double *,
+                      cudaStream_t);
 }  // namespace dem
 
 static int check_n(dem_ctx *ctx, int n) {
@@ -116,6 +120,18 @@ int dem_merge(dem_ctx *ctx, int n, const double *x, const double *y, const doubl
     if (xo == x || yo == y || zo == z || ro == r) return dem_set_error(ctx, DEM_E_INVALID, "outputs alias inputs");
     return dem::launch_merge(ctx, n, x, y, z, r, pairs, num_pairs, xo, yo, zo, ro, n_out, merged,
                              (cudaStream_t)stream);
+}
+
+int dem_direct_vjp(dem_ctx *ctx, int n, const double *x, const double *y, const double *z, const double *r,
+                   const double *fx, const double *fy, const double *fz, const double *lx, const double *ly,
+                   const double *lz, double m_const, double eta_const, double stokes_factor, double L, int periodic,
+                   double *mx, double *my, double *mz, double *gx, double *gy, double *gz, double *gr, void *stream) {
+    int rc = check_n(ctx, n);
+    if (rc) return rc;
+    if ((rc = check_box(ctx, L, periodic))) return rc;
+    if (!(stokes_factor > 0)) return dem_set_error(ctx, DEM_E_INVALID, "stokes_factor must be > 0");
+    return dem::launch_direct_vjp(ctx, n, x, y, z, r, fx, fy, fz, lx, ly, lz, m_const, eta_const, stokes_factor, L,
+                                  periodic, mx, my, mz, gx, gy, gz, gr, (cudaStream_t)stream);
 }
 
 }  // extern "C"

@@ -56,6 +56,7 @@ SIGNATURES = {
                                    C.POINTER(_i)]),
     "dem_direct_plan": (_i, [_vp, _i, _i, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i), C.POINTER(C.c_longlong),
                              C.POINTER(_i)]),
+    "dem_direct_vjp": (_i, [_vp, _i] + [_vp] * 10 + [_d, _d, _d, _d, _i] + [_vp] * 7 + [_vp]),
     "dem_batch_create": (_i, [_vp, _i, C.POINTER(_i64), C.POINTER(_d), _i, C.POINTER(_vp)]),
     "dem_batch_destroy": (None, [_vp]),
     "dem_batch_info": (_i, [_vp, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i), C.POINTER(_i)]),
@@ -264,6 +265,15 @@ class Context:
                                         ptr(F[1]), ptr(F[2]), float(eta_const), float(L), int(periodic),
                                         int(precision), ptr(out[0]), ptr(out[1]), ptr(out[2]), self.stream()),
             "direct_convection",
+        )
+
+    def direct_vjp(self, n, pos, r, F, lam, m_const, eta_const, stokes, L, periodic, mu, g, gr):
+        self._check(
+            lib().dem_direct_vjp(self.handle, n, ptr(pos[0]), ptr(pos[1]), ptr(pos[2]), ptr(r), ptr(F[0]), ptr(F[1]),
+                                 ptr(F[2]), ptr(lam[0]), ptr(lam[1]), ptr(lam[2]), float(m_const), float(eta_const),
+                                 float(stokes), float(L), int(periodic), ptr(mu[0]), ptr(mu[1]), ptr(mu[2]),
+                                 ptr(g[0]), ptr(g[1]), ptr(g[2]), ptr(gr), self.stream()),
+            "direct_vjp",
         )
 
     def euler_update(self, n, pos, r, F, V, stokes, dt, L, periodic, out):
