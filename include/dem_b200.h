@@ -106,6 +106,42 @@ DEM_API int dem_direct_get_tuning(const dem_ctx *ctx, int *i_per_thread, int *th
 DEM_API int dem_direct_plan(const dem_ctx *ctx, int n, int periodic, int *schedule, int *i_per_thread,
                             int *threads, long long *ctas, int *j_splits);
 
+/* ---- Barnes-Hut octree from Morton keys (fast form) ------------------- */
+/* The Barnes-Hut method of dem/octree (flat_tree.py:180-1588) built from
+ * 30-bit Morton keys: positions -> keys in the root cube ([0, L)^3 when
+ * periodic, else the droplets' bounding cube) -> stable on-device radix sort
+ * -> octree level by level from key prefixes (a node holding more than
+ * leaf_size droplets is split into its non-empty octants, at most 10 levels)
+ * -> R^3 sums and R^3-weighted centres.  Walks use the reference's acceptance
+ * test s^2 < theta^2 D^2 (flat_tree.py:871), opened per warp of 32 spatially
+ * adjacent targets, with monopole forces (:873-884), Stokeslet + dipole
+ * velocities (:1215-1265) and exact leaf pairs with the contact cut
+ * r^2 >= (r_i + r_j)^2 (:835); separations in FP64, terms in FP32.  Results
+ * approximate the direct sums; the FP64 reference-parity tree is dem_tree_*.
+ * dem_bh_build synchronises `stream` once per tree level (level sizes). */
+typedef struct dem_bh dem_bh;
+DEM_API int dem_bh_create(dem_ctx *ctx, int capacity, dem_bh **out);
+DEM_API void dem_bh_destroy(dem_bh *bh);
+DEM_API int dem_bh_build(dem_bh *bh, int n, const double *x, const double *y, const double *z, const double *r,
+                         double L, int periodic, int leaf_size, void *stream);
+/* Dipole forces of the built tree's droplets, in the caller's order. */
+DEM_API int dem_bh_forces(dem_bh *bh, double m_const, double theta, double *fx, double *fy, double *fz, void *stream);
+/* Oseen convection from the tree (f* = NULL: the forces of the last
+ * dem_bh_forces); with stokes_factor > 0 the total velocity
+ * F / (stokes_factor r) + V (flat_tree.py:1326-1347), else V alone. */
+DEM_API int dem_bh_velocity(dem_bh *bh, const double *fx, const double *fy, const double *fz, double eta_const,
+                            double theta, double stokes_factor, double *vx, double *vy, double *vz, void *stream);
+/* Periodic boxes: a node whose cell is larger than L / 2^window_level is
+ * opened unless the whole cell lies inside the target's minimum-image window
+ * (|D_axis| + s < L/2); smaller straddling cells are taken at their centre's
+ * image, as the reference does for every node (flat_tree.py:871).
+ * 0 (the default) = the reference's rule. */
+DEM_API int dem_bh_set_window(dem_bh *bh, int window_level);
+/* out (host, 8): nodes, levels, droplets, node capacity, leaf pair terms and
+ * accepted-node terms of the last walk (summed over targets), leaf size,
+ * droplet capacity. */
+DEM_API int dem_bh_stats(dem_bh *bh, int64_t *out);
+
 /* ---- adjoint of the direct step --------------------------------------- */
 /* Vector-Jacobian product of the direct-path droplet velocity
  *   u_i = F_i / (stokes_factor r_i) + V_i    (euler_droplet_solver.py:121-125)

@@ -1,0 +1,979 @@
+// bh.cu -- Barnes-Hut octree from Morton keys, warp-cooperative FP32 walks.
+//
+// The reference's flat octree (dem/octree/flat_tree.py, octree_node.py) is
+// built by serial subdivision and walked per particle in FP64 (tree.cu keeps
+// that form for parity).  This file is the fast form of the same method:
+//
+//   build   30-bit Morton keys (10 bits per axis) of the positions in the root
+//           cube -> stable LSD radix sort (8-bit digits, warp-ranked scatter)
+//           -> particles gathered into key order -> octree level by level from
+//           key prefixes: a node is a run of keys sharing 3*level leading
+//           bits, split into its non-empty octants while it holds more than
+//           `leaf_size` droplets (and level < 10); nodes are contiguous runs
+//           of the sorted arrays, children stored consecutively.
+//   nodes   R^3 sum and R^3-weighted centre (flat_tree.py:544-554,
+//           octree_node.py:98-114), side = root side / 2^level, and the
+//           R^3-weighted second moment Q of the node about that centre; after the force
+//           walk, sum F and the dipole D = sum (x - c) F^T (= P - c F^T of
+//           flat_tree.py:556-777).
+//   walks   one warp per 32 consecutive sorted targets; the warp shares a
+//           shared-memory stack and opens a node when any of its lanes fails
+//           the reference's acceptance test s^2 < theta^2 D^2 (flat_tree.py:871),
+//           so every lane sees a tree cut at least as fine as its own; in a
+//           periodic box a node of level < window_level is also opened
+//           unless its whole cell lies in the target's minimum-image window
+//           (|D_axis| + s < L/2), where all its droplets take the image of its
+//           centre (the reference evaluates such a node at its centre's image).
+//           Accepted nodes: monopole force (:873-884) plus its quadrupole
+//           correction / Stokeslet + dipole correction (:1215-1265); leaves:
+//           exact pair terms with the
+//           contact cut r^2 >= (r_i + r_j)^2 (:835).  Separations are taken in
+//           FP64 from FP64 positions (minimum image), the terms in FP32.
+//
+// Quadrupole correction of the node force.  The pair force is f(d) = P(d)/|d|^7
+// = grad(phi)/3 with phi(d) = |d|^-3 - 3 dz^2 |d|^-5.  About the R^3-weighted
+// centre c the first-order term of sum_j r_j^3 f(D + delta_j) vanishes, so the
+// next term is (1/6) Q_ab d_a d_b d_c phi(D) with Q = sum_j r_j^3 delta_j delta_j^T;
+// with x = D, S_abc = delta_ab x_c + delta_ac x_b + delta_bc x_a, the third
+// derivatives of |d|^-n are n(n+2) [S_abc r^-(n+4) - (n+4) x_a x_b x_c r^-(n+6)]
+// and those of dz^2 |d|^-5 follow from the product rule; contracted with Q they
+// give the closed form of quad_force below.
+#include <algorithm>
+#include <vector>
+
+#include "mixed_common.cuh"
+#include "scan.cuh"
+
+namespace dem {
+
+constexpr int RS_T = 256, RS_ITEMS = 8, RS_TILE = RS_T * RS_ITEMS;
+constexpr int BH_T = 128;     // threads per walk CTA (4 warps)
+constexpr int BH_STACK = 96;  // stack entries per warp (depth <= 10, <= 8 children per node)
+constexpr int BH_MAX_LEVEL = 10;
+
+struct BhNodes {
+    int *start, *count, *first_child, *nchild, *level;
+    double *cx, *cy, *cz;  // R^3-weighted centre
+    float *r3;             // R^3 sum
+    float *q;              // [M][6] second moment Q = sum r^3 (x - c)(x - c)^T: xx xy xz yy yz zz
+    float *fs;             // [M][3] sum of forces
+    float *dp;             // [M][9] dipole D_ab = sum (x_a - c_a) F_b
+};
+
+}  // namespace dem
+
+using namespace dem;
+
+struct dem_bh {
+    dem_ctx *ctx = nullptr;
+    int capacity = 0, max_nodes = 0;
+    int n = 0, node_count = 0, leaf_size = 16, periodic = 0, nlevels = 0;
+    int window_level = 0;  // see dem_bh_set_window (0: the reference's acceptance rule)
+    double L = 1.0;
+    uint32_t *keys[2] = {nullptr, nullptr};
+    int32_t *idx[2] = {nullptr, nullptr};
+    int32_t *hist = nullptr;
+    double *ps = nullptr;       // [4][capacity] sorted x, y, z, r
+    double *fsort = nullptr;    // [3][capacity] forces in sorted order
+    int32_t *bounds = nullptr;  // [9][max_nodes] child split points of the current level
+    long long *bbox = nullptr;  // [6] min/max of an open box (order-preserving integers)
+    double *geom = nullptr;     // [4] root cube origin x, y, z and side
+    unsigned long long *counters = nullptr;       // [2] pair and node terms of the last walk
+    unsigned long long *scales = nullptr;         // [2] max r, max |F| (bit patterns)
+    int32_t *scan_in = nullptr, *coff = nullptr;  // [max_nodes + 1] children per node of a level, offsets
+    BhNodes nd{};
+    std::vector<int> level_off;
+};
+
+namespace {
+
+__device__ __forceinline__ uint32_t spread10(uint32_t v) {  // 10 bits -> every third bit
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000FFu;
+    v = (v | (v << 8)) & 0x0300F00Fu;
+    v = (v | (v << 4)) & 0x030C30C3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+__device__ __forceinline__ uint32_t compact10(uint32_t v) {  // inverse of spread10
+    v &= 0x09249249u;
+    v = (v | (v >> 2)) & 0x030C30C3u;
+    v = (v | (v >> 4)) & 0x0300F00Fu;
+    v = (v | (v >> 8)) & 0x030000FFu;
+    v = (v | (v >> 16)) & 0x3ffu;
+    return v;
+}
+
+__device__ __forceinline__ uint32_t cell10(double p, double o, double inv_side) {
+    const double t = (p - o) * inv_side * 1024.0;
+    int c = (int)floor(t);
+    c = c < 0 ? 0 : (c > 1023 ? 1023 : c);
+    return (uint32_t)c;
+}
+
+// Doubles as order-preserving signed integers (for atomicMin / atomicMax).
+__device__ __forceinline__ long long ord_of(double v) {
+    const long long b = __double_as_longlong(v);
+    return b >= 0 ? b : (long long)(0x8000000000000000ULL - (unsigned long long)b);
+}
+__device__ __forceinline__ double of_ord(long long m) {
+    return __longlong_as_double(m >= 0 ? m : (long long)(0x8000000000000000ULL - (unsigned long long)m));
+}
+
+__global__ void bbox_init_kernel(long long *bb) {
+    if (threadIdx.x < 3)
+        bb[threadIdx.x] = ord_of(1e300);
+    else if (threadIdx.x < 6)
+        bb[threadIdx.x] = ord_of(-1e300);
+}
+
+__global__ void bbox_kernel(int n, const double *__restrict__ x, const double *__restrict__ y,
+                            const double *__restrict__ z, long long *bb) {
+    double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double v[3] = {x[i], y[i], z[i]};
+        for (int c = 0; c < 3; ++c) {
+            mn[c] = fmin(mn[c], v[c]);
+            mx[c] = fmax(mx[c], v[c]);
+        }
+    }
+    for (int c = 0; c < 3; ++c) {
+        for (int o = 16; o; o >>= 1) {
+            mn[c] = fmin(mn[c], __shfl_xor_sync(0xffffffffu, mn[c], o));
+            mx[c] = fmax(mx[c], __shfl_xor_sync(0xffffffffu, mx[c], o));
+        }
+    }
+    if ((threadIdx.x & 31) == 0) {
+        for (int c = 0; c < 3; ++c) {
+            atomicMin(&bb[c], ord_of(mn[c]));
+            atomicMax(&bb[3 + c], ord_of(mx[c]));
+        }
+    }
+}
+
+// Root cube: [0, L)^3 for a periodic box, else the bounding cube of the droplets.
+__global__ void geom_kernel(int periodic, double L, const long long *bb, double *geom) {
+    if (threadIdx.x != 0) return;
+    if (periodic) {
+        geom[0] = geom[1] = geom[2] = 0.0;
+        geom[3] = L;
+        return;
+    }
+    double side = 0.0;
+    for (int c = 0; c < 3; ++c) {
+        geom[c] = of_ord(bb[c]);
+        side = fmax(side, of_ord(bb[3 + c]) - geom[c]);
+    }
+    geom[3] = side > 0.0 ? side * (1.0 + 1e-12) : 1.0;
+}
+
+__global__ void keys_kernel(int n, const double *__restrict__ x, const double *__restrict__ y,
+                            const double *__restrict__ z, const double *__restrict__ geom,
+                            uint32_t *__restrict__ keys, int32_t *__restrict__ idx) {
+    const double ox = geom[0], oy = geom[1], oz = geom[2], inv_side = 1.0 / geom[3];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t cx = cell10(x[i], ox, inv_side), cy = cell10(y[i], oy, inv_side),
+                       cz = cell10(z[i], oz, inv_side);
+        keys[i] = (spread10(cx) << 2) | (spread10(cy) << 1) | spread10(cz);
+        idx[i] = i;
+    }
+}
+
+// Per-tile digit histogram, digit-major: hist[d * tiles + tile].
+__global__ void __launch_bounds__(RS_T) rs_hist_kernel(int n, const uint32_t *__restrict__ keys, int shift,
+                                                       int tiles, int32_t *__restrict__ hist) {
+    __shared__ int h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const int base = blockIdx.x * RS_TILE;
+    for (int k = 0; k < RS_ITEMS; ++k) {
+        const int i = base + k * RS_T + threadIdx.x;
+        if (i < n) atomicAdd(&h[(keys[i] >> shift) & 255u], 1);
+    }
+    __syncthreads();
+    hist[threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
+}
+
+// Stable scatter: warp w ranks items [w * 256, (w + 1) * 256) of the tile in
+// order, 32 at a time, grouping equal digits with match.any.
+__global__ void __launch_bounds__(RS_T) rs_scatter_kernel(int n, const uint32_t *__restrict__ kin,
+                                                          const int32_t *__restrict__ vin, uint32_t *__restrict__ kout,
+                                                          int32_t *__restrict__ vout, int shift, int tiles,
+                                                          const int32_t *__restrict__ off) {
+    constexpr int W = RS_T / 32;
+    __shared__ int cnt[W][256];
+    __shared__ int run[W][256];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int d = threadIdx.x; d < W * 256; d += RS_T) (&cnt[0][0])[d] = 0;
+    __syncthreads();
+    const int base = blockIdx.x * RS_TILE + w * (32 * RS_ITEMS);
+    const unsigned lt = (1u << lane) - 1u;
+    for (int r = 0; r < RS_ITEMS; ++r) {
+        const int i = base + r * 32 + lane;
+        const bool valid = i < n;
+        const int d = valid ? (int)((kin[i] >> shift) & 255u) : 256 + lane;
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        if (valid && (peers & lt) == 0) cnt[w][d] += __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    {
+        const int d = threadIdx.x;  // RS_T == 256 digits
+        int acc = off[d * tiles + blockIdx.x];
+        for (int ww = 0; ww < W; ++ww) {
+            run[ww][d] = acc;
+            acc += cnt[ww][d];
+        }
+    }
+    __syncthreads();
+    for (int r = 0; r < RS_ITEMS; ++r) {
+        const int i = base + r * 32 + lane;
+        const bool valid = i < n;
+        const uint32_t key = valid ? kin[i] : 0u;
+        const int d = valid ? (int)((key >> shift) & 255u) : 256 + lane;
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        int pos = 0;
+        if (valid) pos = run[w][d] + __popc(peers & lt);
+        __syncwarp();
+        if (valid) {
+            kout[pos] = key;
+            vout[pos] = vin[i];
+            if ((peers & lt) == 0) run[w][d] += __popc(peers);
+        }
+        __syncwarp();
+    }
+}
+
+__global__ void gather_kernel(int n, int cap, const int32_t *__restrict__ idx, const double *__restrict__ x,
+                              const double *__restrict__ y, const double *__restrict__ z,
+                              const double *__restrict__ r, double *__restrict__ ps) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        const int i = idx[s];
+        ps[s] = x[i];
+        ps[cap + s] = y[i];
+        ps[2 * (size_t)cap + s] = z[i];
+        ps[3 * (size_t)cap + s] = r[i];
+    }
+}
+
+__global__ void root_kernel(BhNodes nd, int n) {
+    nd.start[0] = 0;
+    nd.count[0] = n;
+    nd.level[0] = 0;
+    nd.first_child[0] = -1;
+    nd.nchild[0] = 0;
+}
+
+// first index in [lo, hi) whose 3-bit digit at `shift` is >= o (digits are
+// non-decreasing inside a node's run)
+__device__ __forceinline__ int digit_lower_bound(const uint32_t *keys, int lo, int hi, int shift, uint32_t o) {
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (((keys[mid] >> shift) & 7u) < o)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__global__ void level_count_kernel(BhNodes nd, const uint32_t *__restrict__ keys, int ls, int le, int leaf_size,
+                                   int32_t *__restrict__ bounds, int M, int32_t *__restrict__ nchild_out) {
+    for (int k = ls + blockIdx.x * blockDim.x + threadIdx.x; k < le; k += gridDim.x * blockDim.x) {
+        const int s0 = nd.start[k], c = nd.count[k], lv = nd.level[k];
+        int nch = 0;
+        if (c > leaf_size && lv < BH_MAX_LEVEL) {
+            const int shift = 27 - 3 * lv;
+            int b[9];
+            b[0] = s0;
+            b[8] = s0 + c;
+            for (uint32_t o = 1; o < 8; ++o) b[o] = digit_lower_bound(keys, b[o - 1], s0 + c, shift, o);
+            for (int o = 0; o < 9; ++o) bounds[o * M + k] = b[o];
+            for (int o = 0; o < 8; ++o) nch += b[o + 1] > b[o];
+        }
+        nd.nchild[k] = nch;
+        nchild_out[k - ls] = nch;
+    }
+}
+
+__global__ void level_write_kernel(BhNodes nd, int ls, int le, const int32_t *__restrict__ bounds, int M,
+                                   const int32_t *__restrict__ child_off, int next0) {
+    for (int k = ls + blockIdx.x * blockDim.x + threadIdx.x; k < le; k += gridDim.x * blockDim.x) {
+        const int nch = nd.nchild[k];
+        if (nch == 0) {
+            nd.first_child[k] = -1;
+            continue;
+        }
+        int c = next0 + child_off[k - ls];
+        nd.first_child[k] = c;
+        const int lv = nd.level[k] + 1;
+        for (int o = 0; o < 8; ++o) {
+            const int a = bounds[o * M + k], b = bounds[(o + 1) * M + k];
+            if (b > a) {
+                nd.start[c] = a;
+                nd.count[c] = b - a;
+                nd.level[c] = lv;
+                nd.first_child[c] = -1;
+                nd.nchild[c] = 0;
+                ++c;
+            }
+        }
+    }
+}
+
+// R^3 and R^3-weighted centre of nodes [a, b), one CTA (big nodes) or one warp per node
+template <bool BLOCK>
+__global__ void node_r3_kernel(BhNodes nd, int a, int b, const double *__restrict__ ps, int cap,
+                               const double *__restrict__ geom, const uint32_t *__restrict__ keys) {
+    const double ox = geom[0], oy = geom[1], oz = geom[2], box = geom[3];
+    const int per = BLOCK ? 1 : blockDim.x / 32;
+    const int lane = BLOCK ? threadIdx.x : (threadIdx.x & 31);
+    const int stride = BLOCK ? blockDim.x : 32;
+    __shared__ double red[10][32];
+    for (int k = a + blockIdx.x * per + (BLOCK ? 0 : (int)(threadIdx.x >> 5)); k < b; k += gridDim.x * per) {
+        const int s0 = nd.start[k], c = nd.count[k];
+        // sums relative to the node's first droplet (keeps the second moment free of cancellation)
+        const double rx = c > 0 ? ps[s0] : 0.0, ry = c > 0 ? ps[cap + s0] : 0.0,
+                     rz = c > 0 ? ps[2 * (size_t)cap + s0] : 0.0;
+        double v[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};  // w, w d (3), w d d^T (6)
+        for (int t = lane; t < c; t += stride) {
+            const double r = ps[3 * (size_t)cap + s0 + t];
+            const double w = r * r * r;
+            const double dx = ps[s0 + t] - rx, dy = ps[cap + s0 + t] - ry, dz = ps[2 * (size_t)cap + s0 + t] - rz;
+            v[0] += w;
+            v[1] += w * dx;
+            v[2] += w * dy;
+            v[3] += w * dz;
+            v[4] += w * dx * dx;
+            v[5] += w * dx * dy;
+            v[6] += w * dx * dz;
+            v[7] += w * dy * dy;
+            v[8] += w * dy * dz;
+            v[9] += w * dz * dz;
+        }
+        for (int q = 0; q < 10; ++q)
+            for (int o = 16; o; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+        if (BLOCK) {
+            const int wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+            if ((threadIdx.x & 31) == 0)
+                for (int q = 0; q < 10; ++q) red[q][wp] = v[q];
+            __syncthreads();
+            if (threadIdx.x == 0)
+                for (int q = 0; q < 10; ++q) {
+                    v[q] = 0;
+                    for (int u = 0; u < nw; ++u) v[q] += red[q][u];
+                }
+            __syncthreads();
+        }
+        if (lane == 0) {
+            const double w = v[0];
+            nd.r3[k] = (float)w;
+            float *Q = nd.q + 6 * (size_t)k;
+            if (w > 0.0) {
+                const double mx = v[1] / w, my = v[2] / w, mz = v[3] / w;
+                nd.cx[k] = rx + mx;
+                nd.cy[k] = ry + my;
+                nd.cz[k] = rz + mz;
+                Q[0] = (float)(v[4] - w * mx * mx);
+                Q[1] = (float)(v[5] - w * mx * my);
+                Q[2] = (float)(v[6] - w * mx * mz);
+                Q[3] = (float)(v[7] - w * my * my);
+                Q[4] = (float)(v[8] - w * my * mz);
+                Q[5] = (float)(v[9] - w * mz * mz);
+            } else {  // geometric centre of the cell (octree_node.py:98-114)
+                const int lv = nd.level[k];
+                const uint32_t key = c > 0 ? keys[s0] : 0u;
+                const uint32_t pre = lv > 0 ? key >> (30 - 3 * lv) << (30 - 3 * lv) : 0u;
+                const double side = ldexp(box, -lv), cell = ldexp(box, -10);
+                nd.cx[k] = ox + compact10(pre >> 2) * cell + side * 0.5;
+                nd.cy[k] = oy + compact10(pre >> 1) * cell + side * 0.5;
+                nd.cz[k] = oz + compact10(pre) * cell + side * 0.5;
+                for (int q = 0; q < 6; ++q) Q[q] = 0.f;
+            }
+        }
+    }
+}
+
+// sum F and dipole D = sum (x - c) F^T of nodes [a, b)
+template <bool BLOCK>
+__global__ void node_force_kernel(BhNodes nd, int a, int b, const double *__restrict__ ps,
+                                  const double *__restrict__ fsort, int cap) {
+    const int per = BLOCK ? 1 : blockDim.x / 32;
+    const int lane = BLOCK ? threadIdx.x : (threadIdx.x & 31);
+    const int stride = BLOCK ? blockDim.x : 32;
+    __shared__ double red[12][32];
+    for (int k = a + blockIdx.x * per + (BLOCK ? 0 : (int)(threadIdx.x >> 5)); k < b; k += gridDim.x * per) {
+        const int s0 = nd.start[k], c = nd.count[k];
+        const double cx = nd.cx[k], cy = nd.cy[k], cz = nd.cz[k];
+        double v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int t = lane; t < c; t += stride) {
+            const int s = s0 + t;
+            const double F[3] = {fsort[s], fsort[cap + s], fsort[2 * (size_t)cap + s]};
+            const double d[3] = {ps[s] - cx, ps[cap + s] - cy, ps[2 * (size_t)cap + s] - cz};
+            for (int q = 0; q < 3; ++q) v[q] += F[q];
+            for (int p = 0; p < 3; ++p)
+                for (int q = 0; q < 3; ++q) v[3 + 3 * p + q] += d[p] * F[q];
+        }
+        for (int q = 0; q < 12; ++q)
+            for (int o = 16; o; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+        if (BLOCK) {
+            const int wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+            if ((threadIdx.x & 31) == 0)
+                for (int q = 0; q < 12; ++q) red[q][wp] = v[q];
+            __syncthreads();
+            if (threadIdx.x == 0)
+                for (int q = 0; q < 12; ++q) {
+                    v[q] = 0;
+                    for (int u = 0; u < nw; ++u) v[q] += red[q][u];
+                }
+            __syncthreads();
+        }
+        if (lane == 0) {  // node-major: one node's aggregates are contiguous for the walk
+            for (int q = 0; q < 3; ++q) nd.fs[3 * (size_t)k + q] = (float)v[q];
+            for (int q = 0; q < 9; ++q) nd.dp[9 * (size_t)k + q] = (float)v[3 + q];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// walks
+// ---------------------------------------------------------------------------
+// Scaled units in FP32: lengths / ell (ell = 2^e with 2^(e-1) <= max r), forces
+// * 2^-q (2^(q-1) <= max |F|).  Node aggregates are stored in these units:
+// r3 = R^3 / ell^3, fs = sum F 2^-q, dp = D 2^-q / ell.
+// (1/6) Q_ab d_a d_b d_c phi at x = D (see the file header); r7 = |x|^-7 etc.
+__device__ __forceinline__ void quad_force(float x, float y, float z, const float *__restrict__ Q, float rinv,
+                                           float rinv2, float &gx, float &gy, float &gz) {
+    const float r7 = (rinv2 * rinv2) * (rinv2 * rinv), r9 = r7 * rinv2, r11 = r9 * rinv2;
+    const float qxx = Q[0], qxy = Q[1], qxz = Q[2], qyy = Q[3], qyz = Q[4], qzz = Q[5];
+    const float tr = qxx + qyy + qzz;
+    const float Qx = fmaf(qxx, x, fmaf(qxy, y, qxz * z));
+    const float Qy = fmaf(qxy, x, fmaf(qyy, y, qyz * z));
+    const float Qz = fmaf(qxz, x, fmaf(qyz, y, qzz * z));
+    const float xQx = fmaf(x, Qx, fmaf(y, Qy, z * Qz));
+    // from |d|^-3: 15 [(tr x + 2 Q x) r^-7 - 7 (x.Qx) x r^-9]
+    const float a1 = 15.f * r7, a2 = -105.f * xQx * r9;
+    // from dz^2 |d|^-5 (times -3 below)
+    const float b1 = 35.f * z * z * r9;
+    const float b2 = -10.f * qzz * r7 + 140.f * z * Qz * r9 - 315.f * z * z * xQx * r11;
+    const float tx = fmaf(2.f, Qx, tr * x), ty = fmaf(2.f, Qy, tr * y), tz = fmaf(2.f, Qz, tr * z);
+    const float Bx = b1 * tx + b2 * x - 20.f * z * qxz * r7;
+    const float By = b1 * ty + b2 * y - 20.f * z * qyz * r7;
+    const float Bz = b1 * tz + b2 * z - 20.f * z * qzz * r7 - 20.f * Qz * r7 - 10.f * z * (tr * r7 - 7.f * xQx * r9);
+    gx += (a1 * tx + a2 * x - 3.f * Bx) * (1.f / 6.f);
+    gy += (a1 * ty + a2 * y - 3.f * By) * (1.f / 6.f);
+    gz += (a1 * tz + a2 * z - 3.f * Bz) * (1.f / 6.f);
+}
+
+struct BhWalk {
+    int n, cap, node_count;
+    const double *ps;                  // sorted x, y, z, r (FP64, metres)
+    const int32_t *idx;                // sorted -> caller order
+    BhNodes nd;
+    const double *geom;                // root cube origin and side
+    const unsigned long long *scales;  // [0] max r, [1] max |F|
+    const double *fsort;               // forces in sorted order (velocity walk)
+    float theta2;
+    int window_level;
+    double L, halfL;
+    unsigned long long *counters;  // [0] leaf pair terms, [1] accepted-node terms
+    uint32_t *err;
+};
+
+template <bool PER>
+__device__ __forceinline__ double bh_mic(double d, double L, double halfL) {
+    return PER ? mic64(d, L, halfL) : d;
+}
+
+// FORCE: F_i = m r_i^3 (sum_leaf r_j^3 P(d)/|d|^7 + sum_nodes R^3 P(D)/|D|^7), d = x_j - x_i, D = c - x_i
+// else:  u_i = [F_i / (stokes r_i)] + eta (sum_leaf G(e) F_j + sum_nodes G(e) F_node + dipole), e = x_i - x_j
+template <bool PER, bool FORCE>
+__global__ void __launch_bounds__(BH_T) bh_walk_kernel(const BhWalk w, double coeff, double stokes,
+                                                       double *__restrict__ ox, double *__restrict__ oy,
+                                                       double *__restrict__ oz, double *__restrict__ fsort_out) {
+    __shared__ int stack[BH_T / 32][BH_STACK];
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    const int n = w.n, cap = w.cap;
+    const double inv_ell = pow2_inv_of(w.scales[0]);
+    const double fsc = FORCE ? 1.0 : pow2_inv_of(w.scales[1]);
+    const double box = w.geom[3];
+    unsigned long long pairs = 0, nodes = 0;
+    const int warps = gridDim.x * (BH_T / 32);
+    for (int base = (blockIdx.x * (BH_T / 32) + wp) * 32; base < n; base += warps * 32) {
+        const int si = base + lane;
+        const bool valid = si < n;
+        const int sl = valid ? si : base;  // padding lanes shadow a real droplet, their results are dropped
+        const double xi = w.ps[sl], yi = w.ps[cap + sl], zi = w.ps[2 * (size_t)cap + sl],
+                     ri = w.ps[3 * (size_t)cap + sl];
+        float ax = 0.f, ay = 0.f, az = 0.f;
+        int sp = 1;
+        if (lane == 0) stack[wp][0] = 0;
+        __syncwarp();
+        int iters = 0;
+        bool broken = false;
+        while (sp > 0) {
+            if (++iters > w.node_count + 1) {  // a tree is visited at most once per node
+                broken = true;
+                break;
+            }
+            const int node = stack[wp][--sp];
+            __syncwarp();
+            const int cnt = w.nd.count[node];
+            if (cnt == 0) continue;
+            float fnx = 0.f, fny = 0.f, fnz = 0.f, r3n = 0.f;
+            if (FORCE) {
+                r3n = w.nd.r3[node];
+                if ((double)r3n / (inv_ell * inv_ell * inv_ell) < 1e-30) continue;  // :861
+            } else {
+                fnx = w.nd.fs[3 * (size_t)node];
+                fny = w.nd.fs[3 * (size_t)node + 1];
+                fnz = w.nd.fs[3 * (size_t)node + 2];
+                const double fx = fnx / fsc, fy = fny / fsc, fz = fnz / fsc;
+                if (fx * fx + fy * fy + fz * fz < 1e-60) continue;  // :1155
+            }
+            double Dx = w.nd.cx[node] - xi, Dy = w.nd.cy[node] - yi, Dz = w.nd.cz[node] - zi;
+            Dx = bh_mic<PER>(Dx, w.L, w.halfL);
+            Dy = bh_mic<PER>(Dy, w.L, w.halfL);
+            Dz = bh_mic<PER>(Dz, w.L, w.halfL);
+            const float dx = (float)(Dx * inv_ell), dy = (float)(Dy * inv_ell), dz = (float)(Dz * inv_ell);
+            const float D2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            const float side = (float)(ldexp(box, -w.nd.level[node]) * inv_ell);
+            bool accept = side * side < w.theta2 * D2 && D2 > 0.f;
+            if (PER && w.nd.level[node] < w.window_level) {
+                // cells larger than L / 2^window_level: the whole cell inside the target's
+                // minimum-image window (else its droplets take different images)
+                const float hw = (float)(w.halfL * inv_ell) - side;
+                accept = accept && fabsf(dx) < hw && fabsf(dy) < hw && fabsf(dz) < hw;
+            }
+            accept = accept || !valid;
+            if (__all_sync(0xffffffffu, accept)) {
+                if (valid) {
+                    ++nodes;
+                    const float rinv = rsqrtf(D2), rinv2 = rinv * rinv;
+                    if (FORCE) {  // D = c - x_i
+                        const float b = r3n * (rinv2 * rinv2) * (rinv2 * rinv);
+                        const float ang = fmaf(4.f * dz, dz, -fmaf(dx, dx, dy * dy));
+                        ax = fmaf(b * ang, dx, ax);
+                        ay = fmaf(b * ang, dy, ay);
+                        az = fmaf(b * fmaf(2.f * dz, dz, -3.f * fmaf(dx, dx, dy * dy)), dz, az);
+                        quad_force(dx, dy, dz, w.nd.q + 6 * (size_t)node, rinv, rinv2, ax, ay, az);
+                    } else {  // e = x_i - c = -D
+                        const float ex = -dx, ey = -dy, ez = -dz;
+                        const float dot = fmaf(ex, fnx, fmaf(ey, fny, ez * fnz));
+                        ax = fmaf(rinv, fmaf(ex, dot * rinv2, fnx), ax);
+                        ay = fmaf(rinv, fmaf(ey, dot * rinv2, fny), ay);
+                        az = fmaf(rinv, fmaf(ez, dot * rinv2, fnz), az);
+                        const float *Dm = w.nd.dp + 9 * (size_t)node;  // D_ab, row a, column b
+                        const float Ux = Dm[0] * ex + Dm[3] * ey + Dm[6] * ez;  // D^T e
+                        const float Uy = Dm[1] * ex + Dm[4] * ey + Dm[7] * ez;
+                        const float Uz = Dm[2] * ex + Dm[5] * ey + Dm[8] * ez;
+                        const float Wx = Dm[0] * ex + Dm[1] * ey + Dm[2] * ez;  // D e
+                        const float Wy = Dm[3] * ex + Dm[4] * ey + Dm[5] * ez;
+                        const float Wz = Dm[6] * ex + Dm[7] * ey + Dm[8] * ez;
+                        const float tr = Dm[0] + Dm[4] + Dm[8];
+                        const float q = ex * Wx + ey * Wy + ez * Wz;
+                        const float rinv3 = rinv * rinv2, rinv5 = rinv3 * rinv2;
+                        ax += rinv3 * (Ux - Wx - tr * ex) + 3.f * ex * q * rinv5;
+                        ay += rinv3 * (Uy - Wy - tr * ey) + 3.f * ey * q * rinv5;
+                        az += rinv3 * (Uz - Wz - tr * ez) + 3.f * ez * q * rinv5;
+                    }
+                }
+                continue;
+            }
+            const int nch = w.nd.nchild[node];
+            if (nch == 0) {  // leaf: exact pair terms (contact cut r^2 >= (r_i + r_j)^2)
+                const int s0 = w.nd.start[node];
+                if (valid) pairs += cnt;
+                for (int k = 0; k < cnt; ++k) {
+                    const int sj = s0 + k;
+                    const double xj = w.ps[sj], yj = w.ps[cap + sj], zj = w.ps[2 * (size_t)cap + sj],
+                                 rj = w.ps[3 * (size_t)cap + sj];
+                    const double ddx = bh_mic<PER>(xj - xi, w.L, w.halfL), ddy = bh_mic<PER>(yj - yi, w.L, w.halfL),
+                                 ddz = bh_mic<PER>(zj - zi, w.L, w.halfL);
+                    const double r2d = ddx * ddx + ddy * ddy + ddz * ddz, rs = ri + rj;
+                    if (!valid || sj == si || r2d < rs * rs) continue;
+                    const float dx = (float)(ddx * inv_ell), dy = (float)(ddy * inv_ell), dz = (float)(ddz * inv_ell);
+                    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                    const float rinv = rsqrtf(r2), rinv2 = rinv * rinv;
+                    if (FORCE) {
+                        const float rjs = (float)(rj * inv_ell);
+                        const float b = rjs * rjs * rjs * (rinv2 * rinv2) * (rinv2 * rinv);
+                        const float ang = fmaf(4.f * dz, dz, -fmaf(dx, dx, dy * dy));
+                        ax = fmaf(b * ang, dx, ax);
+                        ay = fmaf(b * ang, dy, ay);
+                        az = fmaf(b * fmaf(2.f * dz, dz, -3.f * fmaf(dx, dx, dy * dy)), dz, az);
+                    } else {  // e = x_i - x_j = -d
+                        const float fx = (float)(w.fsort[sj] * fsc), fy = (float)(w.fsort[cap + sj] * fsc),
+                                    fz = (float)(w.fsort[2 * (size_t)cap + sj] * fsc);
+                        const float ex = -dx, ey = -dy, ez = -dz;
+                        const float dot = fmaf(ex, fx, fmaf(ey, fy, ez * fz));
+                        ax = fmaf(rinv, fmaf(ex, dot * rinv2, fx), ax);
+                        ay = fmaf(rinv, fmaf(ey, dot * rinv2, fy), ay);
+                        az = fmaf(rinv, fmaf(ez, dot * rinv2, fz), az);
+                    }
+                }
+                continue;
+            }
+            if (sp + nch > BH_STACK) {  // cannot happen for depth <= 10; kept bounded anyway
+                broken = true;
+                break;
+            }
+            if (lane < nch) stack[wp][sp + lane] = w.nd.first_child[node] + lane;
+            sp += nch;
+            __syncwarp();
+        }
+        if (broken && lane == 0) raise_device_error(w.err, DEM_DEVERR_NODE_OVERFLOW);
+        if (valid) {
+            const int i = w.idx[si];
+            double vx, vy, vz;
+            if (FORCE) {  // F = m r_i^3 acc / ell
+                const double f = coeff * ri * ri * ri * inv_ell;
+                vx = f * ax;
+                vy = f * ay;
+                vz = f * az;
+                fsort_out[si] = vx;
+                fsort_out[cap + si] = vy;
+                fsort_out[2 * (size_t)cap + si] = vz;
+            } else {  // u = eta / (ell 2^-q) acc  (+ F / (stokes r))
+                const double f = coeff * inv_ell / fsc;
+                vx = f * ax;
+                vy = f * ay;
+                vz = f * az;
+                if (stokes > 0.0) {
+                    const double a = 1.0 / (stokes * ri);
+                    vx += w.fsort[si] * a;
+                    vy += w.fsort[cap + si] * a;
+                    vz += w.fsort[2 * (size_t)cap + si] * a;
+                }
+            }
+            ox[i] = vx;
+            oy[i] = vy;
+            oz[i] = vz;
+        }
+        __syncwarp();
+    }
+    for (int o = 16; o; o >>= 1) {  // per-target counts, summed over the warp
+        pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
+        nodes += __shfl_xor_sync(0xffffffffu, nodes, o);
+    }
+    if (lane == 0) {
+        atomicAdd(&w.counters[0], pairs);
+        atomicAdd(&w.counters[1], nodes);
+    }
+}
+
+__global__ void forces_to_sorted_kernel(int n, int cap, const int32_t *__restrict__ idx, const double *__restrict__ fx,
+                                        const double *__restrict__ fy, const double *__restrict__ fz,
+                                        double *__restrict__ fsort) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        const int i = idx[s];
+        fsort[s] = fx[i];
+        fsort[cap + s] = fy[i];
+        fsort[2 * (size_t)cap + s] = fz[i];
+    }
+}
+
+// node aggregates in walk units: r3 / ell^3, q / ell^5 (what = 0); fs * 2^-q, dp * 2^-q / ell (what = 1)
+__global__ void scale_nodes_kernel(BhNodes nd, int nc, const unsigned long long *scales, int what) {
+    const double inv_ell = pow2_inv_of(scales[0]);
+    const double fsc = pow2_inv_of(scales[1]);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nc; k += gridDim.x * blockDim.x) {
+        if (what == 0) {
+            const double s3 = inv_ell * inv_ell * inv_ell;
+            nd.r3[k] = (float)((double)nd.r3[k] * s3);
+            for (int q = 0; q < 6; ++q) nd.q[6 * (size_t)k + q] = (float)((double)nd.q[6 * (size_t)k + q] * s3 * inv_ell * inv_ell);
+        } else {
+            for (int q = 0; q < 3; ++q) nd.fs[3 * (size_t)k + q] = (float)((double)nd.fs[3 * (size_t)k + q] * fsc);
+            for (int q = 0; q < 9; ++q)
+                nd.dp[9 * (size_t)k + q] = (float)((double)nd.dp[9 * (size_t)k + q] * fsc * inv_ell);
+        }
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+template <typename T>
+static int bh_alloc(dem_ctx *ctx, T **p, size_t count, const char *what) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    return dem_check_cuda(ctx, cudaMalloc((void **)p, sizeof(T) * (count > 0 ? count : 1)), what);
+}
+
+static void bh_free_nodes(BhNodes &nd) {
+    void *ptrs[] = {nd.start, nd.count, nd.first_child, nd.nchild, nd.level, nd.cx,
+                    nd.cy,    nd.cz,    nd.r3,          nd.q,      nd.fs,    nd.dp};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    nd = BhNodes{};
+}
+
+// (Re)allocates node arrays for m nodes, keeping the first `keep` nodes' topology.
+static int bh_nodes_reserve(dem_bh *b, int m, int keep, cudaStream_t s) {
+    if (m <= b->max_nodes) return DEM_OK;
+    dem_ctx *ctx = b->ctx;
+    BhNodes nn{};
+    int rc;
+    if ((rc = bh_alloc(ctx, &nn.start, m, "bh nodes")) || (rc = bh_alloc(ctx, &nn.count, m, "bh nodes")) ||
+        (rc = bh_alloc(ctx, &nn.first_child, m, "bh nodes")) || (rc = bh_alloc(ctx, &nn.nchild, m, "bh nodes")) ||
+        (rc = bh_alloc(ctx, &nn.level, m, "bh nodes")) || (rc = bh_alloc(ctx, &nn.cx, m, "bh nodes")) ||
+        (rc = bh_alloc(ctx, &nn.cy, m, "bh nodes")) || (rc = bh_alloc(ctx, &nn.cz, m, "bh nodes")) ||
+        (rc = bh_alloc(ctx, &nn.r3, m, "bh nodes")) || (rc = bh_alloc(ctx, &nn.q, 6 * (size_t)m, "bh nodes")) ||
+        (rc = bh_alloc(ctx, &nn.fs, 3 * (size_t)m, "bh nodes")) ||
+        (rc = bh_alloc(ctx, &nn.dp, 9 * (size_t)m, "bh nodes"))) {
+        bh_free_nodes(nn);
+        return rc;
+    }
+    if (keep > 0) {
+        int *src[] = {b->nd.start, b->nd.count, b->nd.first_child, b->nd.nchild, b->nd.level};
+        int *dst[] = {nn.start, nn.count, nn.first_child, nn.nchild, nn.level};
+        for (int q = 0; q < 5; ++q)
+            if ((rc = dem_check_cuda(
+                     ctx, cudaMemcpyAsync(dst[q], src[q], sizeof(int) * keep, cudaMemcpyDeviceToDevice, s), "bh nodes")))
+                return rc;
+        if ((rc = dem_check_cuda(ctx, cudaStreamSynchronize(s), "bh nodes"))) return rc;
+    }
+    if ((rc = bh_alloc(ctx, &b->bounds, 9 * (size_t)m, "bh nodes")) ||
+        (rc = bh_alloc(ctx, &b->scan_in, (size_t)m + 1, "bh nodes")) ||
+        (rc = bh_alloc(ctx, &b->coff, (size_t)m + 1, "bh nodes"))) {
+        bh_free_nodes(nn);
+        return rc;
+    }
+    bh_free_nodes(b->nd);
+    b->nd = nn;
+    b->max_nodes = m;
+    return DEM_OK;
+}
+
+static void bh_free(dem_bh *b) {
+    cudaSetDevice(b->ctx->device);
+    bh_free_nodes(b->nd);
+    void *ptrs[] = {b->keys[0], b->keys[1], b->idx[0],   b->idx[1], b->hist,    b->ps,  b->fsort,
+                    b->bounds,  b->bbox,    b->geom,     b->counters, b->scales, b->scan_in, b->coff};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    delete b;
+}
+
+static inline int grid_of(dem_ctx *ctx, long long work, int threads = 256) {
+    long long g = (work + threads - 1) / threads;
+    if (g < 1) g = 1;
+    if (g > 8LL * ctx->sm_count) g = 8LL * ctx->sm_count;
+    return (int)g;
+}
+
+extern "C" {
+
+int dem_bh_create(dem_ctx *ctx, int capacity, dem_bh **out) {
+    if (!ctx || !out || capacity < 1) return dem_set_error(ctx, DEM_E_INVALID, "bh: bad arguments");
+    *out = nullptr;
+    int rc = dem_check_cuda(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+    if (rc) return rc;
+    dem_bh *b = new dem_bh();
+    b->ctx = ctx;
+    b->capacity = capacity;
+    const size_t n = (size_t)capacity;
+    const int tiles = (capacity + RS_TILE - 1) / RS_TILE;
+    if ((rc = bh_alloc(ctx, &b->keys[0], n, "bh")) || (rc = bh_alloc(ctx, &b->keys[1], n, "bh")) ||
+        (rc = bh_alloc(ctx, &b->idx[0], n, "bh")) || (rc = bh_alloc(ctx, &b->idx[1], n, "bh")) ||
+        (rc = bh_alloc(ctx, &b->hist, 2 * (256 * (size_t)tiles + 1), "bh")) ||
+        (rc = bh_alloc(ctx, &b->ps, 4 * n, "bh")) || (rc = bh_alloc(ctx, &b->fsort, 3 * n, "bh")) ||
+        (rc = bh_alloc(ctx, &b->bbox, 6, "bh")) || (rc = bh_alloc(ctx, &b->geom, 4, "bh")) ||
+        (rc = bh_alloc(ctx, &b->counters, 2, "bh")) || (rc = bh_alloc(ctx, &b->scales, 2, "bh")) ||
+        (rc = bh_nodes_reserve(b, std::max(4096, capacity / 4), 0, nullptr))) {
+        bh_free(b);
+        return rc;
+    }
+    *out = b;
+    return DEM_OK;
+}
+
+void dem_bh_destroy(dem_bh *b) {
+    if (b) bh_free(b);
+}
+
+int dem_bh_build(dem_bh *b, int n, const double *x, const double *y, const double *z, const double *r, double L,
+                 int periodic, int leaf_size, void *stream) {
+    if (!b) return DEM_E_INVALID;
+    dem_ctx *ctx = b->ctx;
+    if (n < 0 || leaf_size < 1) return dem_set_error(ctx, DEM_E_INVALID, "bh: n >= 0 and leaf_size >= 1");
+    if (n > b->capacity) return dem_set_error(ctx, DEM_E_CAPACITY, "bh: number of particles exceeds the capacity");
+    if (periodic && !(L > 0)) return dem_set_error(ctx, DEM_E_INVALID, "periodic boundaries need L > 0");
+    int rc = dem_check_cuda(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+    if (rc) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    b->n = n;
+    b->L = L;
+    b->periodic = periodic ? 1 : 0;
+    b->leaf_size = leaf_size;
+    b->level_off.assign(1, 0);
+    b->node_count = 0;
+    b->nlevels = 0;
+    if (n == 0) return DEM_OK;
+    dem_prof_begin(ctx, "bh_build", s);
+    if (!periodic) {
+        bbox_init_kernel<<<1, 32, 0, counted(s)>>>(b->bbox);
+        bbox_kernel<<<grid_of(ctx, n), 256, 0, counted(s)>>>(n, x, y, z, b->bbox);
+    }
+    geom_kernel<<<1, 32, 0, counted(s)>>>(b->periodic, L, b->bbox, b->geom);
+    keys_kernel<<<grid_of(ctx, n), 256, 0, counted(s)>>>(n, x, y, z, b->geom, b->keys[0], b->idx[0]);
+    // stable LSD radix sort of (key, index), 8-bit digits, 30-bit keys: 4 passes
+    const int tiles = (n + RS_TILE - 1) / RS_TILE;
+    int32_t *hist = b->hist, *off = b->hist + 256 * (size_t)tiles + 1;  // histogram, its exclusive scan
+    int cur = 0;
+    for (int pass = 0; pass < 4; ++pass) {
+        const int shift = 8 * pass;
+        rs_hist_kernel<<<tiles, RS_T, 0, counted(s)>>>(n, b->keys[cur], shift, tiles, hist);
+        if ((rc = exclusive_scan<int32_t, int32_t>(ctx, hist, off, 256LL * tiles, s))) return rc;
+        rs_scatter_kernel<<<tiles, RS_T, 0, counted(s)>>>(n, b->keys[cur], b->idx[cur], b->keys[1 - cur],
+                                                          b->idx[1 - cur], shift, tiles, off);
+        cur = 1 - cur;
+    }
+    // after an even number of passes the sorted arrays are back in buffer 0
+    gather_kernel<<<grid_of(ctx, n), 256, 0, counted(s)>>>(n, b->capacity, b->idx[0], x, y, z, r, b->ps);
+    if ((rc = dem_check_cuda(ctx, cudaMemsetAsync(b->scales, 0, 2 * sizeof(unsigned long long), s), "memset")))
+        return rc;
+    maxabs_kernel<<<grid_of(ctx, n), 256, 0, counted(s)>>>(n, r, nullptr, nullptr, b->scales);
+    // octree level by level (the host learns each level's size: one synchronisation per level)
+    root_kernel<<<1, 1, 0, counted(s)>>>(b->nd, n);
+    int ls = 0, le = 1;
+    while (le > ls) {
+        const int width = le - ls;
+        int total = 0;
+        for (int attempt = 0; attempt < 2; ++attempt) {
+            level_count_kernel<<<grid_of(ctx, width), 256, 0, counted(s)>>>(b->nd, b->keys[0], ls, le, leaf_size,
+                                                                           b->bounds, b->max_nodes, b->scan_in);
+            if ((rc = exclusive_scan<int32_t, int32_t>(ctx, b->scan_in, b->coff, width, s))) return rc;
+            if ((rc = dem_check_cuda(
+                     ctx, cudaMemcpyAsync(&total, b->coff + width, sizeof(int), cudaMemcpyDeviceToHost, s),
+                     "bh level size")) ||
+                (rc = dem_check_cuda(ctx, cudaStreamSynchronize(s), "bh level size")))
+                return rc;
+            if ((long long)le + total > 0x7fffffffLL) return dem_set_error(ctx, DEM_E_CAPACITY, "bh: too many nodes");
+            if (le + total <= b->max_nodes) break;
+            // grow the node arrays (the first le nodes are kept) and count this level again
+            if ((rc = bh_nodes_reserve(b, std::max(le + total, 2 * b->max_nodes), le, s))) return rc;
+        }
+        if (total == 0) break;
+        level_write_kernel<<<grid_of(ctx, width), 256, 0, counted(s)>>>(b->nd, ls, le, b->bounds, b->max_nodes,
+                                                                       b->coff, le);
+        b->level_off.push_back(le);
+        ls = le;
+        le += total;
+    }
+    b->node_count = le;
+    b->nlevels = (int)b->level_off.size();
+    // node R^3 and centres: one CTA per node on the top three levels, one warp per node below
+    const int top = b->nlevels > 3 ? b->level_off[3] : le;
+    node_r3_kernel<true><<<std::max(top, 1), 256, 0, counted(s)>>>(b->nd, 0, top, b->ps, b->capacity, b->geom,
+                                                                   b->keys[0]);
+    if (le > top)
+        node_r3_kernel<false><<<grid_of(ctx, 32LL * (le - top)), 256, 0, counted(s)>>>(b->nd, top, le, b->ps,
+                                                                                       b->capacity, b->geom,
+                                                                                       b->keys[0]);
+    scale_nodes_kernel<<<grid_of(ctx, le), 256, 0, counted(s)>>>(b->nd, le, b->scales, 0);
+    dem_prof_end(ctx, s);
+    return dem_check_launch(ctx, "bh build");
+}
+
+static BhWalk walk_args(dem_bh *b, float theta) {
+    BhWalk w;
+    w.n = b->n;
+    w.cap = b->capacity;
+    w.node_count = b->node_count;
+    w.ps = b->ps;
+    w.idx = b->idx[0];
+    w.nd = b->nd;
+    w.geom = b->geom;
+    w.scales = b->scales;
+    w.fsort = b->fsort;
+    w.theta2 = theta * theta;
+    w.window_level = b->window_level;
+    w.L = b->L;
+    w.halfL = 0.5 * b->L;
+    w.counters = b->counters;
+    w.err = b->ctx->d_err;
+    return w;
+}
+
+static int walk_grid(dem_bh *b) { return std::max(1, (b->n + BH_T - 1) / BH_T); }
+
+int dem_bh_forces(dem_bh *b, double m_const, double theta, double *fx, double *fy, double *fz, void *stream) {
+    if (!b || !(theta >= 0)) return DEM_E_INVALID;
+    dem_ctx *ctx = b->ctx;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (b->n == 0) return DEM_OK;
+    int rc = dem_check_cuda(ctx, cudaMemsetAsync(b->counters, 0, 2 * sizeof(unsigned long long), s), "memset");
+    if (rc) return rc;
+    const BhWalk w = walk_args(b, (float)theta);
+    dem_prof_begin(ctx, "bh_force_walk", s);
+    if (b->periodic)
+        bh_walk_kernel<true, true><<<walk_grid(b), BH_T, 0, counted(s)>>>(w, m_const, 0.0, fx, fy, fz, b->fsort);
+    else
+        bh_walk_kernel<false, true><<<walk_grid(b), BH_T, 0, counted(s)>>>(w, m_const, 0.0, fx, fy, fz, b->fsort);
+    dem_prof_end(ctx, s);
+    return dem_check_launch(ctx, "bh force walk");
+}
+
+int dem_bh_velocity(dem_bh *b, const double *fx, const double *fy, const double *fz, double eta_const, double theta,
+                    double stokes_factor, double *vx, double *vy, double *vz, void *stream) {
+    if (!b || !(theta >= 0)) return DEM_E_INVALID;
+    dem_ctx *ctx = b->ctx;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (b->n == 0) return DEM_OK;
+    const int n = b->n, le = b->node_count;
+    int rc;
+    if (fx)  // forces given in caller order (else: those of the last dem_bh_forces, already sorted)
+        forces_to_sorted_kernel<<<grid_of(ctx, n), 256, 0, counted(s)>>>(n, b->capacity, b->idx[0], fx, fy, fz,
+                                                                         b->fsort);
+    const double *fs = b->fsort;
+    if ((rc = dem_check_cuda(ctx, cudaMemsetAsync(b->scales + 1, 0, sizeof(unsigned long long), s), "memset")))
+        return rc;
+    maxabs_kernel<<<grid_of(ctx, n), 256, 0, counted(s)>>>(n, fs, fs + b->capacity, fs + 2 * (size_t)b->capacity,
+                                                           b->scales + 1);
+    const int top = b->nlevels > 3 ? b->level_off[3] : le;
+    node_force_kernel<true><<<std::max(top, 1), 256, 0, counted(s)>>>(b->nd, 0, top, b->ps, b->fsort, b->capacity);
+    if (le > top)
+        node_force_kernel<false><<<grid_of(ctx, 32LL * (le - top)), 256, 0, counted(s)>>>(b->nd, top, le, b->ps,
+                                                                                          b->fsort, b->capacity);
+    scale_nodes_kernel<<<grid_of(ctx, le), 256, 0, counted(s)>>>(b->nd, le, b->scales, 1);
+    if ((rc = dem_check_cuda(ctx, cudaMemsetAsync(b->counters, 0, 2 * sizeof(unsigned long long), s), "memset")))
+        return rc;
+    const BhWalk w = walk_args(b, (float)theta);
+    dem_prof_begin(ctx, "bh_velocity_walk", s);
+    if (b->periodic)
+        bh_walk_kernel<true, false><<<walk_grid(b), BH_T, 0, counted(s)>>>(w, eta_const, stokes_factor, vx, vy, vz,
+                                                                           nullptr);
+    else
+        bh_walk_kernel<false, false><<<walk_grid(b), BH_T, 0, counted(s)>>>(w, eta_const, stokes_factor, vx, vy, vz,
+                                                                            nullptr);
+    dem_prof_end(ctx, s);
+    return dem_check_launch(ctx, "bh velocity walk");
+}
+
+int dem_bh_set_window(dem_bh *b, int window_level) {
+    if (!b || window_level < 0) return DEM_E_INVALID;
+    b->window_level = window_level;
+    return DEM_OK;
+}
+
+int dem_bh_stats(dem_bh *b, int64_t *out) {
+    if (!b || !out) return DEM_E_INVALID;
+    unsigned long long c[2] = {0, 0};
+    int rc = dem_check_cuda(b->ctx, cudaMemcpy(c, b->counters, sizeof(c), cudaMemcpyDeviceToHost), "bh stats");
+    if (rc) return rc;
+    out[0] = b->node_count;
+    out[1] = b->nlevels;
+    out[2] = b->n;
+    out[3] = b->max_nodes;
+    out[4] = (int64_t)c[0];
+    out[5] = (int64_t)c[1];
+    out[6] = b->leaf_size;
+    out[7] = b->capacity;
+    return DEM_OK;
+}
+
+}  // extern "C"

@@ -57,6 +57,13 @@ SIGNATURES = {
     "dem_direct_plan": (_i, [_vp, _i, _i, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i), C.POINTER(C.c_longlong),
                              C.POINTER(_i)]),
     "dem_direct_vjp": (_i, [_vp, _i] + [_vp] * 10 + [_d, _d, _d, _d, _i] + [_vp] * 7 + [_vp]),
+    "dem_bh_create": (_i, [_vp, _i, C.POINTER(_vp)]),
+    "dem_bh_destroy": (None, [_vp]),
+    "dem_bh_build": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _d, _i, _i, _vp]),
+    "dem_bh_forces": (_i, [_vp, _d, _d, _vp, _vp, _vp, _vp]),
+    "dem_bh_velocity": (_i, [_vp, _vp, _vp, _vp, _d, _d, _d, _vp, _vp, _vp, _vp]),
+    "dem_bh_stats": (_i, [_vp, C.POINTER(_i64)]),
+    "dem_bh_set_window": (_i, [_vp, _i]),
     "dem_batch_create": (_i, [_vp, _i, C.POINTER(_i64), C.POINTER(_d), _i, C.POINTER(_vp)]),
     "dem_batch_destroy": (None, [_vp]),
     "dem_batch_info": (_i, [_vp, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i), C.POINTER(_i)]),
@@ -360,6 +367,50 @@ class Tree:
 
     def leaf_indices(self, out):
         self.ctx._check(lib().dem_tree_leaf_indices(self.handle, ptr(out), self.ctx.stream()), "tree_leaf_indices")
+
+
+class MortonTree:
+    """One ``dem_bh``: Barnes-Hut octree from Morton keys (FP32 walks)."""
+
+    def __init__(self, ctx: Context, capacity: int):
+        self.ctx = ctx
+        self.capacity = int(capacity)
+        self.handle = _vp()
+        ctx._check(lib().dem_bh_create(ctx.handle, self.capacity, C.byref(self.handle)), "bh_create")
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value and _lib is not None:
+            try:
+                _lib.dem_bh_destroy(h)
+            except Exception:  # pragma: no cover
+                pass
+            self.handle = None
+
+    def build(self, n, pos, r, L, periodic, leaf_size):
+        self.ctx._check(lib().dem_bh_build(self.handle, int(n), ptr(pos[0]), ptr(pos[1]), ptr(pos[2]), ptr(r),
+                                           float(L), int(bool(periodic)), int(leaf_size), self.ctx.stream()),
+                        "bh_build")
+
+    def forces(self, m_const, theta, out):
+        self.ctx._check(lib().dem_bh_forces(self.handle, float(m_const), float(theta), ptr(out[0]), ptr(out[1]),
+                                            ptr(out[2]), self.ctx.stream()), "bh_forces")
+
+    def velocity(self, F, eta_const, theta, stokes_factor, out):
+        a = (None, None, None) if F is None else (ptr(F[0]), ptr(F[1]), ptr(F[2]))
+        self.ctx._check(lib().dem_bh_velocity(self.handle, *a, float(eta_const), float(theta), float(stokes_factor),
+                                              ptr(out[0]), ptr(out[1]), ptr(out[2]), self.ctx.stream()),
+                        "bh_velocity")
+
+    def set_window(self, window_level):
+        self.ctx._check(lib().dem_bh_set_window(self.handle, int(window_level)), "bh_set_window")
+
+    def stats(self):
+        out = (_i64 * 8)()
+        self.ctx._check(lib().dem_bh_stats(self.handle, out), "bh_stats")
+        keys = ("node_count", "levels", "num_particles", "max_nodes", "leaf_pairs", "node_terms", "leaf_size",
+                "capacity")
+        return {k: int(v) for k, v in zip(keys, out)}
 
 
 class Batch:

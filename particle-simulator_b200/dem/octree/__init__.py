@@ -2,5 +2,6 @@
 
 from .flat_tree import FlatOctree, OctreeNode
 from .force_tree import TreeDropletForceCalculator
+from .morton_tree import MortonTreeForceCalculator
 
-__all__ = ["FlatOctree", "OctreeNode", "TreeDropletForceCalculator"]
+__all__ = ["FlatOctree", "OctreeNode", "TreeDropletForceCalculator", "MortonTreeForceCalculator"]

@@ -1,0 +1,113 @@
+"""Barnes-Hut on the Morton-key octree (csrc/bh.cu) against direct FP64 sums.
+
+* theta = 0 opens every node, so the walk reduces to exact leaf pairs: forces
+  and velocities equal the direct sums up to FP32 pair arithmetic;
+* theta = 0.5, leaf size 16: relative force error <= 1e-3 against the direct
+  FP64 sum on a subsample (quadrupole-corrected nodes); the tree velocity (Stokeslet + dipole of the
+  reference's method, flat_tree.py:1215-1265) against the direct Oseen sum of
+  the same forces is no worse than the reference-parity FP64 tree's on the same
+  state (that method leaves ~30 % at theta = 0.5: node force sums nearly
+  cancel, so the truncated expansion dominates);
+* edge sizes (0, 1, a few droplets, a deep leaf of identical keys), the open
+  box, capacity growth and torch inputs."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle as O
+from gpu_util import ETA_OIL, consts, lognormal_state, ref_metric, rel_norm
+
+pytestmark = pytest.mark.gpu
+
+
+def _calc(n, L, periodic=True, theta=0.5, leaf=16, window=0):
+    from dem.octree import MortonTreeForceCalculator
+
+    return MortonTreeForceCalculator(num_particles=n, theta=theta, mpl=leaf, eta_oil=ETA_OIL, L=L, periodic=periodic,
+                                     window_level=window)
+
+
+@pytest.mark.parametrize("periodic", [True, False])
+def test_theta_zero_is_the_direct_sum(periodic):
+    pos, r, L = lognormal_state(3000, seed=31, periodic=periodic)
+    m, eta, _ = consts()
+    tc = _calc(3000, L, periodic, theta=0.0)
+    F, V = tc.calculate_forces_and_convection(pos, r)
+    assert rel_norm(F, O.direct_forces(pos, r, m, L, periodic)) < 2e-5
+    assert rel_norm(V, O.direct_convection(pos, F, eta, L, periodic)) < 2e-5  # the same forces in
+    st = tc.stats()
+    assert st["node_terms"] == 0 and st["leaf_pairs"] == 3000 * 3000  # every target meets every leaf droplet
+
+
+def test_theta_half_leaf16_within_1e_3_of_direct():
+    # N = 20,000 is a small box for a leaf of 16 (5 levels): cells above level 4
+    # straddling the minimum-image window are opened (at N = 2^20 the reference's
+    # rule alone meets the bar; bench.py --workload tree measures it)
+    from dem.octree import TreeDropletForceCalculator
+
+    pos, r, L = lognormal_state(20000, seed=32)
+    m, eta, sf = consts()
+    tc = _calc(20000, L, theta=0.5, leaf=16, window=4)
+    F, V = tc.calculate_forces_and_convection(pos, r)
+    rows = (0, 2048)
+    F_ref = O.direct_forces(pos, r, m, L, True, rows=rows)[: rows[1]]
+    assert rel_norm(F[: rows[1]], F_ref) <= 1e-3
+    assert ref_metric(F[: rows[1]], F_ref)[0] <= 1e-3
+    F0 = _calc(20000, L, theta=0.5, leaf=16, window=0).calculate(pos, r)  # the reference's rule
+    assert rel_norm(F0[: rows[1]], F_ref) <= 1.5e-3
+    V_ref = O.direct_convection(pos, F, eta, L, True, rows=rows)[: rows[1]]
+    parity = TreeDropletForceCalculator(num_particles=20000, theta=0.5, mpl=16, eta_oil=ETA_OIL, L=L, periodic=True)
+    Fp, Vp = parity.calculate_forces_and_convection(pos, r)
+    Vp_ref = O.direct_convection(pos, Fp, eta, L, True, rows=rows)[: rows[1]]
+    assert rel_norm(V[: rows[1]], V_ref) <= 1.1 * rel_norm(Vp[: rows[1]], Vp_ref)
+    F2, V2 = tc.calculate_forces_and_convection(pos, r)
+    np.testing.assert_array_equal(F, F2)  # deterministic
+    np.testing.assert_array_equal(V, V2)
+    _, U = tc.calculate_forces_and_total_velocity(pos, r, sf)
+    np.testing.assert_allclose(U, V + F / (sf * r[:, None]), rtol=1e-12, atol=1e-30)
+    assert tc._ctx.device_errors() == 0
+
+
+@pytest.mark.parametrize("leaf", [1, 4, 64])
+def test_other_leaf_sizes(leaf):
+    pos, r, L = lognormal_state(8000, seed=34)
+    m, _, _ = consts()
+    F = _calc(8000, L, theta=0.5, leaf=leaf).calculate(pos, r)
+    F_ref = O.direct_forces(pos, r, m, L, True, rows=(0, 1024))[:1024]
+    assert rel_norm(F[:1024], F_ref) <= 2e-3
+
+
+def test_edge_sizes_and_duplicates():
+    tc = _calc(64, 1e-3, periodic=False, theta=0.5, leaf=2)
+    m, eta, _ = consts()
+    for n in (0, 1, 2, 17):
+        rng = np.random.default_rng(n)
+        pos = rng.uniform(0, 1e-3, (n, 3))
+        r = rng.uniform(1e-6, 3e-6, n)
+        F, V = tc.calculate_forces_and_convection(pos, r)
+        assert F.shape == (n, 3) and np.all(np.isfinite(F)) and np.all(np.isfinite(V))
+        if n > 1:
+            assert rel_norm(F, O.direct_forces(pos, r, m, 1e-3, False)) < 1e-2
+    # 40 droplets in one finest cell (~1 um) of a 1 mm periodic box (identical keys): a leaf of 40 at
+    # level 10; radii keep the node's R^3 sum above the reference's 1e-30 skip threshold (flat_tree.py:861)
+    tp = _calc(64, 1e-3, periodic=True, theta=0.5, leaf=2)
+    pos = np.full((40, 3), 5e-4) + np.arange(40)[:, None] * np.array([2e-8, 0, 0])
+    r = np.full(40, 5e-9)
+    F, V = tp.calculate_forces_and_convection(pos, r)
+    assert np.all(np.isfinite(F)) and np.all(np.isfinite(V))
+    assert rel_norm(F, O.direct_forces(pos, r, m, 1e-3, True)) < 1e-4
+    assert tp.stats()["levels"] == 11
+    assert tc._ctx.device_errors() == 0 and tp._ctx.device_errors() == 0
+
+
+def test_capacity_growth_and_torch_inputs():
+    import torch
+
+    pos, r, L = lognormal_state(5000, seed=33)
+    tc = _calc(100, L, theta=0.5)
+    F = tc.calculate(pos, r)  # grows
+    Ft = tc.calculate(torch.as_tensor(pos, device="cuda"), torch.as_tensor(r, device="cuda"))
+    assert Ft.is_cuda
+    np.testing.assert_array_equal(Ft.cpu().numpy(), F)
