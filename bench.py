@@ -57,9 +57,10 @@ def parse():
     ap.add_argument("--cpu-sample-seconds", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="direct", choices=["direct", "batched", "adjoint"],
+    ap.add_argument("--workload", default="direct", choices=["direct", "batched", "adjoint", "tree"],
                     help="direct: one box of --n droplets (default); batched: 64 boxes, N ~ U[1024, 32768] (seed 1); "
-                         "adjoint: gradients through 200 steps at N = 16,384")
+                         "adjoint: gradients through 200 steps at N = 16,384; tree: Barnes-Hut at N = 2^20")
+    ap.add_argument("--accuracy", action="store_true", help="tree: errors on 4,096 droplets against direct FP64 sums")
     ap.add_argument("--fd", type=int, default=0, help="adjoint: central-difference checks on this many coordinates")
     ap.add_argument("--boxes", type=int, default=64)
     return ap.parse_args()
@@ -574,6 +575,153 @@ def report_adjoint(args, res):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# Barnes-Hut step (main_tree.py-style) at N = 2^20
+# ---------------------------------------------------------------------------
+TREE_THETA, TREE_LEAF = 0.5, 16
+FLOPS_LEAF_PAIR = 33  # as a force pair
+FLOPS_NODE_TERM = 33 + 70  # monopole + quadrupole correction (force walk)
+
+
+def run_tree(args, device):
+    import torch
+
+    from dem.collision_detector import SpatialHashCollisionDetector
+    from dem.octree import MortonTreeForceCalculator
+
+    torch.cuda.set_device(device)
+    n = 1 << 20
+    pos, r, L = make_state(n, 0)
+    tc = MortonTreeForceCalculator(num_particles=n, theta=TREE_THETA, mpl=TREE_LEAF, L=L, periodic=True,
+                                   device=device, **PHYS)
+    det = SpatialHashCollisionDetector(num_particles=n, L=L, boundary_mode="periodic", device=device)
+    ctx = tc._ctx
+    eta_o, eta_w = PHYS["eta_oil"], PHYS["eta_water"]
+    stokes = 2 * np.pi * eta_o * (2 * eta_o + 3 * eta_w) / (eta_o + eta_w)
+    p = [torch.empty((3, n), dtype=torch.float64, device=device) for _ in range(2)]
+    rr = [torch.as_tensor(r, device=device).clone(), torch.empty(n, dtype=torch.float64, device=device)]
+    ctx.aos_to_soa(n, torch.as_tensor(pos, device=device), p[0])
+    n_out = torch.zeros(1, dtype=torch.int32, device=device)
+    state = dict(cur=0, rc=0, n=n, merges=0)
+
+    def step():
+        cur, rc, m = state["cur"], state["rc"], state["n"]
+        k, pairs, counts = det.detect_device(m, p[cur], rr[rc], L, True)
+        while k > 0:  # coalescence, then detect again (euler_droplet_solver.py:97-110)
+            ctx.merge(m, p[cur], rr[rc], pairs, counts, p[1 - cur], rr[1 - rc], n_out)
+            m = int(n_out.item())
+            cur, rc = 1 - cur, 1 - rc
+            state["merges"] += 1
+            k, pairs, counts = det.detect_device(m, p[cur], rr[rc], L, True)
+        V = tc.forces_and_total_velocity_soa(m, p[cur], rr[rc], stokes)
+        ctx.euler_update_total(m, p[cur], V, DT, L, True, p[1 - cur])
+        state.update(cur=1 - cur, rc=rc, n=m)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(torch.cuda.current_device())
+    sampler.start()
+    time.sleep(0.4)
+    from dem._native import launch_count
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    c0 = launch_count()
+    ctx.profile(True)
+    for k in range(args.steps):
+        ev[k][0].record()
+        step()
+        ev[k][1].record()
+    torch.cuda.synchronize()
+    launches = launch_count() - c0
+    kern = {}
+    for name in ("bh_build", "bh_force_walk", "bh_velocity_walk", "hash_detect"):
+        ms, cnt = ctx.profile_read(name)
+        if cnt:
+            kern[name] = ms / cnt
+    ctx.profile(False)
+    clocks = sampler.stop()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    st = tc.stats()  # counters of the last walk (velocity); the force walk visits the same tree
+    out = dict(n=n, n_final=state["n"], merges=state["merges"], total_ms=float(sum(step_ms)), kern=kern,
+               clocks=clocks, launches=launches, stats=st, L=L)
+    if args.accuracy:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle as O
+
+        m_const, eta, _ = O.physics_constants(**PHYS)
+        rows = (0, 4096)
+        tc0 = MortonTreeForceCalculator(num_particles=n, theta=TREE_THETA, mpl=TREE_LEAF, L=L, periodic=True,
+                                        device=device, **PHYS)
+        F, V = tc0.calculate_forces_and_convection(pos, r)
+        F_ref = O.direct_forces(pos, r, m_const, L, True, rows=rows)[: rows[1]]
+        V_ref = O.direct_convection(pos, F, eta, L, True, rows=rows)[: rows[1]]
+        d = np.linalg.norm(F[: rows[1]] - F_ref, axis=1)
+        nb = np.linalg.norm(F_ref, axis=1)
+        out["accuracy"] = {
+            "sample": "droplets 0..4095 of the seeded state (i.i.d. positions), direct FP64 sums over all 2^20",
+            "force_rel_norm": float(np.linalg.norm(F[: rows[1]] - F_ref) / np.linalg.norm(F_ref)),
+            "force_ref_metric_mean": float(np.mean(d / (nb + 0.01 * nb.mean()))),
+            "velocity_rel_norm_same_forces": float(np.linalg.norm(V[: rows[1]] - V_ref) / np.linalg.norm(V_ref)),
+        }
+    return out
+
+
+def report_tree(args, res):
+    K = args.steps
+    st = res["stats"]
+    n = res["n"]
+    step_ms = res["total_ms"] / K
+    inter = (st["leaf_pairs"] + st["node_terms"])  # per walk
+    clocks = res["clocks"] or {}
+    max_mhz = clocks.get("sm_max_mhz") or 1965.0
+    peak = SM_COUNT_B200 * FP32_LANES_PER_SM * 2 * max_mhz * 1e6 / 1e12
+    fw = res["kern"].get("bh_force_walk")
+    achieved = (st["leaf_pairs"] * FLOPS_LEAF_PAIR + st["node_terms"] * FLOPS_NODE_TERM) / (fw / 1000.0) / 1e12 \
+        if fw else None
+    line = {
+        "metric": "DEM Barnes-Hut steps/s (N=1048576, theta=0.5, leaf 16)",
+        "value": 1000.0 / step_ms,
+        "unit": "steps/s",
+        "n_gpus": 1,
+        "steps": K,
+        "warmup": args.warmup,
+        "ms_per_step": step_ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 terms, f64 positions and separations",
+        "data": "synthetic (seeded lognormal droplets, 2% volume fraction)",
+        "config": {
+            "workload": "Barnes-Hut step: hash detection + merge + Morton octree build + force walk + Stokeslet "
+                        "walk (total velocity) + Euler, N=2^20, periodic, dt=1e-4",
+            "interactions_per_walk": inter,
+            "leaf_pairs_per_droplet": st["leaf_pairs"] / n,
+            "node_terms_per_droplet": st["node_terms"] / n,
+            "tree_nodes": st["node_count"],
+            "tree_levels": st["levels"],
+            "kernel_ms_per_launch": res["kern"],
+            "merges": res["merges"],
+            "n_final": res["n_final"],
+            "l2": "not flushed: the step's inputs (2^20 droplets) and tree exceed the 126 MB L2",
+            **({"accuracy": res["accuracy"]} if "accuracy" in res else {}),
+        },
+        "roofline": {
+            "kernel": "bh_force_walk",
+            "bound": "fp32_pipe (latency-limited walk)",
+            "achieved": achieved,
+            "peak": peak,
+            "unit": "TFLOP/s",
+            "frac": achieved / peak if achieved else None,
+            "traffic": None,
+            "units_per_launch": "leaf pair terms x 33 flops + node terms x 103 flops (monopole + quadrupole)",
+        },
+        "clocks": clocks,
+        "gpu_launches": res["launches"],
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -599,6 +747,12 @@ def main():
     import torch
 
     device = torch.device("cuda", local)
+    if args.workload == "tree":
+        if rank == 0:
+            report_tree(args, run_tree(args, device))
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
     if args.workload == "adjoint":
         if rank == 0:
             report_adjoint(args, run_adjoint(args, device))
