@@ -483,17 +483,31 @@ __global__ void reduce_sym_kernel(const SymBoxes t, int B, const double *__restr
         const int l = d - o0;
         const int K = l / B, lb = l - K * B;
         double sx = 0.0, sy = 0.0, sz = 0.0;
-        for (int Jb = K; Jb < nbk; ++Jb) {
-            const double *P = pi + (size_t)(ib + rows_before(K, nbk) + (Jb - K)) * 3 * plane;
-            sx += P[lb];
-            sy += P[plane + lb];
-            sz += P[2 * plane + lb];
+        // i side: items (K, K), (K, K+1), ... are consecutive; the loads of
+        // several items are issued before their (ordered) additions
+        {
+            const double *P = pi + (size_t)(ib + rows_before(K, nbk)) * 3 * plane + lb;
+            const size_t step = 3 * plane;
+#pragma unroll 4
+            for (int Jb = K; Jb < nbk; ++Jb, P += step) {
+                const double a = P[0], b = P[plane], c = P[2 * plane];
+                sx += a;
+                sy += b;
+                sz += c;
+            }
         }
-        for (int Ib = 0; Ib < K; ++Ib) {
-            const double *P = pj + (size_t)(ib + rows_before(Ib, nbk) + (K - Ib)) * 3 * plane;
-            sx += P[lb];
-            sy += P[plane + lb];
-            sz += P[2 * plane + lb];
+        // j side: item (Ib, K) = rows_before(Ib) + K - Ib; the next row starts nbk - Ib items later
+        {
+            long long item = ib + K;  // (0, K)
+#pragma unroll 4
+            for (int Ib = 0; Ib < K; ++Ib) {
+                const double *P = pj + (size_t)item * 3 * plane + lb;
+                const double a = P[0], b = P[plane], c = P[2 * plane];
+                sx += a;
+                sy += b;
+                sz += c;
+                item += nbk - Ib - 1;
+            }
         }
         const double s = pow2_inv_of(sc[0]);
         double f;

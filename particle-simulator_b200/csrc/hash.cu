@@ -116,6 +116,56 @@ __device__ __forceinline__ void for_each_contact(int i, const double *__restrict
     const int32_t cx = cell_coord(xi, p.cell, p.grid, periodic);
     const int32_t cy = cell_coord(yi, p.cell, p.grid, periodic);
     const int32_t cz = cell_coord(zi, p.cell, p.grid, periodic);
+    auto bucket = [&](const double xj, const double yj, const double zj, const double rj, int32_t j, int m) {
+        double dx = xj - xi, dy = yj - yi, dz = zj - zi;
+        if (periodic) {
+            dx = mic64(dx, L, halfL);
+            dy = mic64(dy, L, halfL);
+            dz = mic64(dz, L, halfL);
+        }
+        const double dist = sqrt(dx * dx + dy * dy + dz * dz);
+        if (dist <= ri + rj) f(j, m);
+    };
+    // Neighbour cell c = 9 (di + 1) + 3 (dj + 1) + (dk + 1): its bucket, or -1 outside an open box.
+    auto cell_hash = [&](int c) -> int32_t {
+        int32_t nx = cx + c / 9 - 1, ny = cy + (c / 3) % 3 - 1, nz = cz + c % 3 - 1;
+        if (periodic) {
+            nx = floor_mod(nx, p.grid);
+            ny = floor_mod(ny, p.grid);
+            nz = floor_mod(nz, p.grid);
+        } else if (nx < 0 || ny < 0 || nz < 0 || nx >= p.grid || ny >= p.grid || nz >= p.grid) {
+            return -1;
+        }
+        return hash_cell(nx, ny, nz, mask);
+    };
+    // Usual case: the 27 cells map to distinct buckets (kept in registers: static indices).
+    {
+        int32_t h[27];
+#pragma unroll
+        for (int c = 0; c < 27; ++c) h[c] = cell_hash(c);
+        bool dup = false;
+#pragma unroll
+        for (int c = 1; c < 27; ++c)
+#pragma unroll
+            for (int m = 0; m < c; ++m) dup |= h[c] >= 0 && h[c] == h[m];
+        if (!dup) {
+            for (int c = 0; c < 27; ++c) {
+                const int32_t hc = cell_hash(c);
+                if (hc < 0) continue;
+                const int32_t start = bstart[hc];
+                int32_t end = bstart[hc + 1];
+                if (end > n) end = n;  // :199-201
+                for (int32_t s = start; s < end; ++s) {
+                    const int32_t j = sorted_idx[s];
+                    if (!(i < j)) continue;
+                    bucket(x[j], y[j], z[j], r[j], j, 1);
+                }
+            }
+            return;
+        }
+    }
+    // Tiny grids or colliding buckets: a bucket seen from several cells is
+    // scanned once, its contacts counted with that multiplicity.
     int32_t hs[27];
     int nh = 0;
     int mult[27];
@@ -148,14 +198,7 @@ __device__ __forceinline__ void for_each_contact(int i, const double *__restrict
         for (int32_t s = start; s < end; ++s) {
             const int32_t j = sorted_idx[s];
             if (!(i < j)) continue;
-            double dx = x[j] - xi, dy = y[j] - yi, dz = z[j] - zi;
-            if (periodic) {
-                dx = mic64(dx, L, halfL);
-                dy = mic64(dy, L, halfL);
-                dz = mic64(dz, L, halfL);
-            }
-            const double dist = sqrt(dx * dx + dy * dy + dz * dz);
-            if (dist <= ri + r[j]) f(j, mult[q]);
+            bucket(x[j], y[j], z[j], r[j], j, mult[q]);
         }
     }
 }
