@@ -54,6 +54,7 @@ constexpr int BH_MAX_LEVEL = 10;
 struct BhNodes {
     int *start, *count, *first_child, *nchild, *level;
     double *cx, *cy, *cz;  // R^3-weighted centre
+    float4 *cs;            // walk copy: centre relative to the root cube origin / ell, and side / ell
     float *r3;             // R^3 sum
     float *q;              // [M][6] second moment Q = sum r^3 (x - c)(x - c)^T: xx xy xz yy yz zz
     float *fs;             // [M][3] sum of forces
@@ -497,7 +498,8 @@ __global__ void __launch_bounds__(BH_T) bh_walk_kernel(const BhWalk w, double co
     const int n = w.n, cap = w.cap;
     const double inv_ell = pow2_inv_of(w.scales[0]);
     const double fsc = FORCE ? 1.0 : pow2_inv_of(w.scales[1]);
-    const double box = w.geom[3];
+    const float Ls = (float)(w.L * inv_ell), invLs = (float)(1.0 / (w.L * inv_ell));
+    const double gox = w.geom[0], goy = w.geom[1], goz = w.geom[2];
     unsigned long long pairs = 0, nodes = 0;
     const int warps = gridDim.x * (BH_T / 32);
     for (int base = (blockIdx.x * (BH_T / 32) + wp) * 32; base < n; base += warps * 32) {
@@ -506,6 +508,9 @@ __global__ void __launch_bounds__(BH_T) bh_walk_kernel(const BhWalk w, double co
         const int sl = valid ? si : base;  // padding lanes shadow a real droplet, their results are dropped
         const double xi = w.ps[sl], yi = w.ps[cap + sl], zi = w.ps[2 * (size_t)cap + sl],
                      ri = w.ps[3 * (size_t)cap + sl];
+        // target in the nodes' FP32 frame (node separations: FP32, ~1e-6 relative for any accepted node)
+        const float xs = (float)((xi - gox) * inv_ell), ys = (float)((yi - goy) * inv_ell),
+                    zs = (float)((zi - goz) * inv_ell);
         float ax = 0.f, ay = 0.f, az = 0.f;
         int sp = 1;
         if (lane == 0) stack[wp][0] = 0;
@@ -532,13 +537,15 @@ __global__ void __launch_bounds__(BH_T) bh_walk_kernel(const BhWalk w, double co
                 const double fx = fnx / fsc, fy = fny / fsc, fz = fnz / fsc;
                 if (fx * fx + fy * fy + fz * fz < 1e-60) continue;  // :1155
             }
-            double Dx = w.nd.cx[node] - xi, Dy = w.nd.cy[node] - yi, Dz = w.nd.cz[node] - zi;
-            Dx = bh_mic<PER>(Dx, w.L, w.halfL);
-            Dy = bh_mic<PER>(Dy, w.L, w.halfL);
-            Dz = bh_mic<PER>(Dz, w.L, w.halfL);
-            const float dx = (float)(Dx * inv_ell), dy = (float)(Dy * inv_ell), dz = (float)(Dz * inv_ell);
+            const float4 cs = w.nd.cs[node];
+            float dx = cs.x - xs, dy = cs.y - ys, dz = cs.z - zs;
+            if (PER) {  // minimum image
+                dx = fmaf(-Ls, rintf(dx * invLs), dx);
+                dy = fmaf(-Ls, rintf(dy * invLs), dy);
+                dz = fmaf(-Ls, rintf(dz * invLs), dz);
+            }
             const float D2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            const float side = (float)(ldexp(box, -w.nd.level[node]) * inv_ell);
+            const float side = cs.w;
             bool accept = side * side < w.theta2 * D2 && D2 > 0.f;
             if (PER && w.nd.level[node] < w.window_level) {
                 // cells larger than L / 2^window_level: the whole cell inside the target's
@@ -674,12 +681,17 @@ __global__ void forces_to_sorted_kernel(int n, int cap, const int32_t *__restric
     }
 }
 
-// node aggregates in walk units: r3 / ell^3, q / ell^5 (what = 0); fs * 2^-q, dp * 2^-q / ell (what = 1)
-__global__ void scale_nodes_kernel(BhNodes nd, int nc, const unsigned long long *scales, int what) {
+// node aggregates in walk units: centre and side / ell, r3 / ell^3, q / ell^5 (what = 0);
+// fs * 2^-q, dp * 2^-q / ell (what = 1)
+__global__ void scale_nodes_kernel(BhNodes nd, int nc, const unsigned long long *scales, const double *geom,
+                                   int what) {
     const double inv_ell = pow2_inv_of(scales[0]);
     const double fsc = pow2_inv_of(scales[1]);
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nc; k += gridDim.x * blockDim.x) {
         if (what == 0) {
+            nd.cs[k] = make_float4((float)((nd.cx[k] - geom[0]) * inv_ell), (float)((nd.cy[k] - geom[1]) * inv_ell),
+                                   (float)((nd.cz[k] - geom[2]) * inv_ell),
+                                   (float)(ldexp(geom[3], -nd.level[k]) * inv_ell));
             const double s3 = inv_ell * inv_ell * inv_ell;
             nd.r3[k] = (float)((double)nd.r3[k] * s3);
             for (int q = 0; q < 6; ++q) nd.q[6 * (size_t)k + q] = (float)((double)nd.q[6 * (size_t)k + q] * s3 * inv_ell * inv_ell);
@@ -705,7 +717,7 @@ static int bh_alloc(dem_ctx *ctx, T **p, size_t count, const char *what) {
 
 static void bh_free_nodes(BhNodes &nd) {
     void *ptrs[] = {nd.start, nd.count, nd.first_child, nd.nchild, nd.level, nd.cx,
-                    nd.cy,    nd.cz,    nd.r3,          nd.q,      nd.fs,    nd.dp};
+                    nd.cy,    nd.cz,    nd.cs,          nd.r3,     nd.q,     nd.fs, nd.dp};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     nd = BhNodes{};
@@ -721,6 +733,7 @@ static int bh_nodes_reserve(dem_bh *b, int m, int keep, cudaStream_t s) {
         (rc = bh_alloc(ctx, &nn.first_child, m, "bh nodes")) || (rc = bh_alloc(ctx, &nn.nchild, m, "bh nodes")) ||
         (rc = bh_alloc(ctx, &nn.level, m, "bh nodes")) || (rc = bh_alloc(ctx, &nn.cx, m, "bh nodes")) ||
         (rc = bh_alloc(ctx, &nn.cy, m, "bh nodes")) || (rc = bh_alloc(ctx, &nn.cz, m, "bh nodes")) ||
+        (rc = bh_alloc(ctx, &nn.cs, m, "bh nodes")) ||
         (rc = bh_alloc(ctx, &nn.r3, m, "bh nodes")) || (rc = bh_alloc(ctx, &nn.q, 6 * (size_t)m, "bh nodes")) ||
         (rc = bh_alloc(ctx, &nn.fs, 3 * (size_t)m, "bh nodes")) ||
         (rc = bh_alloc(ctx, &nn.dp, 9 * (size_t)m, "bh nodes"))) {
@@ -874,7 +887,7 @@ int dem_bh_build(dem_bh *b, int n, const double *x, const double *y, const doubl
         node_r3_kernel<false><<<grid_of(ctx, 32LL * (le - top)), 256, 0, counted(s)>>>(b->nd, top, le, b->ps,
                                                                                        b->capacity, b->geom,
                                                                                        b->keys[0]);
-    scale_nodes_kernel<<<grid_of(ctx, le), 256, 0, counted(s)>>>(b->nd, le, b->scales, 0);
+    scale_nodes_kernel<<<grid_of(ctx, le), 256, 0, counted(s)>>>(b->nd, le, b->scales, b->geom, 0);
     dem_prof_end(ctx, s);
     return dem_check_launch(ctx, "bh build");
 }
@@ -939,7 +952,7 @@ int dem_bh_velocity(dem_bh *b, const double *fx, const double *fy, const double 
     if (le > top)
         node_force_kernel<false><<<grid_of(ctx, 32LL * (le - top)), 256, 0, counted(s)>>>(b->nd, top, le, b->ps,
                                                                                           b->fsort, b->capacity);
-    scale_nodes_kernel<<<grid_of(ctx, le), 256, 0, counted(s)>>>(b->nd, le, b->scales, 1);
+    scale_nodes_kernel<<<grid_of(ctx, le), 256, 0, counted(s)>>>(b->nd, le, b->scales, b->geom, 1);
     if ((rc = dem_check_cuda(ctx, cudaMemsetAsync(b->counters, 0, 2 * sizeof(unsigned long long), s), "memset")))
         return rc;
     const BhWalk w = walk_args(b, (float)theta);
