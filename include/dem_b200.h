@@ -52,6 +52,7 @@ extern "C" {
 #define DEM_DEVERR_NONFINITE 8u     /* a non-finite value was produced            */
 
 typedef struct dem_ctx dem_ctx;
+typedef struct dem_corr dem_corr; /* periodic-image correction grid (dem_corr_create) */
 
 /* ---- context --------------------------------------------------------- */
 /* Creates a context on `device` with room for `capacity` particles.
@@ -116,7 +117,8 @@ DEM_API int dem_direct_plan(const dem_ctx *ctx, int n, int periodic, int *schedu
  * test s^2 < theta^2 D^2 (flat_tree.py:871), opened per warp of 32 spatially
  * adjacent targets, with monopole forces (:873-884), Stokeslet + dipole
  * velocities (:1215-1265) and exact leaf pairs with the contact cut
- * r^2 >= (r_i + r_j)^2 (:835); separations in FP64, terms in FP32.  Results
+ * r^2 >= (r_i + r_j)^2 (:835); leaf separations in FP64, node separations
+ * and all terms in FP32.  Results
  * approximate the direct sums; the FP64 reference-parity tree is dem_tree_*.
  * dem_bh_build synchronises `stream` once per tree level (level sizes). */
 typedef struct dem_bh dem_bh;
@@ -137,6 +139,13 @@ DEM_API int dem_bh_velocity(dem_bh *bh, const double *fx, const double *fy, cons
  * image, as the reference does for every node (flat_tree.py:871).
  * 0 (the default) = the reference's rule. */
 DEM_API int dem_bh_set_window(dem_bh *bh, int window_level);
+/* Attaches a periodic-image correction (dem_corr_create) to the velocity
+ * walk, NULL detaches it: FP32 correction terms at every exact leaf pair and
+ * every accepted node (at the node's R^3 centre with its force sum), and
+ * the self term self_coeff * F_i when stokes_factor <= 0 (the reference's
+ * walks, flat_tree.py:1070-1131, :1171-1213, :1271-1276).  The grid must
+ * outlive its use by the tree. */
+DEM_API int dem_bh_set_correction(dem_bh *bh, const dem_corr *corr);
 /* out (host, 8): nodes, levels, droplets, node capacity, leaf pair terms and
  * accepted-node terms of the last walk (summed over targets), leaf size,
  * droplet capacity. */
@@ -236,6 +245,43 @@ DEM_API int dem_direct_convection(dem_ctx *ctx, int n, const double *x, const do
                           const double *fx, const double *fy, const double *fz, double eta_const, double L,
                           int periodic, int precision, double *vx, double *vy, double *vz, void *stream);
 
+/* ---- periodic-image Oseen correction (COMSOL lattice grid) ------------ */
+/* A correction grid uploaded to the device.  grid_u/v/w: HOST arrays of n^3
+ * doubles in C order [ix][iy][iz], the velocity of the periodic images of a
+ * unit z-force on the nodes grid_min + k / inv_dx (k = 0..n-1) of every axis
+ * (COMSOLLatticeCorrection.get_grid_data).  The scalars are those of
+ * load_periodic_correction:
+ *   Fz_inv = 1 / Fz_comsol, L_ratio = L_comsol / L_sim,
+ *   eta_ratio = eta_comsol / eta_sim, self_coeff = w(0,0,0) * Fz_inv * eta_ratio * L_ratio.
+ * 2 <= n <= DEM_CORR_MAX_GRID.  Device memory: 288 (n-1)^3 bytes.
+ * Replaces the correction fields and load_periodic_correction of
+ * dem/force_calculator/direct_droplet_force_calculator.py:56-120 and
+ * dem/octree/flat_tree.py:125-167. */
+#define DEM_CORR_MAX_GRID 256
+DEM_API int dem_corr_create(dem_ctx *ctx, int n, const double *grid_u, const double *grid_v, const double *grid_w,
+                            double grid_min, double inv_dx, double Fz_inv, double L_ratio, double eta_ratio,
+                            double self_coeff, dem_corr **out);
+DEM_API void dem_corr_destroy(dem_corr *corr);
+/* Host scalars: grid points per axis, the per-pair factor
+ * Fz_inv * eta_ratio * L_ratio, the self coefficient (NULL skips). */
+DEM_API int dem_corr_info(const dem_corr *corr, int *n, double *common, double *self_coeff);
+
+/* Oseen convection with the periodic-image correction: as
+ * dem_direct_convection, plus for every pair j != i the correction of
+ * d = MIC(x_i - x_j) (three permuted trilinear lookups contracted with F_j)
+ * and after the sum the self term self_coeff * F_i.  DEM_PREC_FP64 adds each
+ * pair's correction right after its Stokeslet term, bit-identical to the
+ * reference's order; DEM_PREC_MIXED runs the mixed Oseen pass and an FP32
+ * correction pass (FP32 trilinear forms, FP64 tile sums).  corr == NULL is
+ * DEM_E_NOT_ALLOCATED.
+ * Replaces DirectDropletForceCalculator._calculate_convection_velocities with
+ * corr_enabled == 1, dem/force_calculator/direct_droplet_force_calculator.py:354-464
+ * (lookups _precompute_grid_idx / _interp_precomp :146-182). */
+DEM_API int dem_direct_convection_corr(dem_ctx *ctx, const dem_corr *corr, int n, const double *x, const double *y,
+                                       const double *z, const double *r, const double *fx, const double *fy,
+                                       const double *fz, double eta_const, double L, int periodic, int precision,
+                                       double *vx, double *vy, double *vz, void *stream);
+
 /* Explicit Euler update of the direct path, out of place (xo may equal x):
  *   x_o = (x + (F / (stokes_factor * r) + v) * dt) mod L   (numpy remainder when periodic)
  * Replaces dem/solver/euler_droplet_solver.py:121-131. */
@@ -332,6 +378,16 @@ DEM_API int dem_tree_propagate_forces(dem_tree *tree, const double *fx, const do
 DEM_API int dem_tree_velocity(dem_tree *tree, const double *fx, const double *fy, const double *fz, double eta_const,
                               double theta_sq, double stokes_factor, double *vx, double *vy, double *vz,
                               void *stream);
+
+/* Attaches a periodic-image correction (dem_corr_create) to the velocity
+ * walks, NULL detaches it.  Then the Stokeslet walk adds each leaf pair's and
+ * each accepted node's correction term right after its Stokeslet term and
+ * the self term self_coeff * F_i after the walk; the total-velocity walk
+ * adds the pair and node terms only, as the reference does
+ * (flat_tree.py:1070-1131, :1171-1213, :1271-1276; bit-identical).  The grid
+ * must outlive its use by the tree.
+ * Replaces FlatOctree.load_periodic_correction, flat_tree.py:141-167. */
+DEM_API int dem_tree_set_correction(dem_tree *tree, const dem_corr *corr);
 
 /* Host int64[8]: node_count, parent_count, leaf_slot_count, max_nodes,
  * levels, num_particles, pool_exhausted, capacity. */

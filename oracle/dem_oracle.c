@@ -15,6 +15,8 @@
  *   spatial hash        dem/collision_detector/spatial_hash_collision_detector.py:74-316
  *   merge               dem/solution/droplet_solution.py:208-287 (numpy semantics)
  *   flat octree         dem/octree/flat_tree.py:180-1612, dem/octree/octree_node.py:72-114
+ *   periodic-image      dem/force_calculator/direct_droplet_force_calculator.py:128-182, :413-464
+ *   Oseen correction    dem/octree/flat_tree.py:1070-1131, :1171-1213, :1271-1276
  *
  * Integer powers inside the reference's Taichi kernels (x**2, x**3, x**7) are
  * evaluated by exponentiation by squaring, the way Taichi lowers them:
@@ -104,6 +106,68 @@ EXPORT void dem_oracle_direct_forces(int n, const double *x, const double *y, co
 }
 
 /* ------------------------------------------------------------------------ */
+/* Periodic-image Oseen correction on a regular n^3 grid (COMSOL lattice).   */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+    int n;                    /* grid points per axis */
+    const double *u, *v, *w;  /* n^3 values each, C order [ix][iy][iz] */
+    double gmin, ginv;        /* first node, 1 / spacing */
+    double Fz_inv, cL, eta_r; /* 1/Fz_comsol, L_comsol/L_sim, eta_comsol/eta_sim */
+    double g_self;            /* self-image coefficient */
+} ocorr;
+
+/* _precompute_grid_idx, direct_droplet_force_calculator.py:146-163 (one axis) */
+static inline void grid_idx(double x, double gmin, double inv_dx, int n, int *i, double *t) {
+    double f = (x - gmin) * inv_dx;
+    const double n_max = (double)(n - 1);
+    f = f <= n_max ? f : n_max; /* ti.min(fx, n_max) */
+    f = 0.0 >= f ? 0.0 : f;     /* ti.max(0.0, .)   */
+    int k = (int)floor(f);
+    if (k > n - 2) k = n - 2;
+    *i = k;
+    *t = f - (double)k;
+}
+
+/* _interp_precomp, :165-182: the eight corner terms summed in source order */
+static inline double interp(const double *g, int n, int ix, int iy, int iz, double tx, double ty, double tz) {
+#define G(a, b, c) g[((size_t)(ix + (a)) * n + (iy + (b))) * n + (iz + (c))]
+    return G(0, 0, 0) * (1 - tx) * (1 - ty) * (1 - tz) + G(0, 0, 1) * (1 - tx) * (1 - ty) * tz +
+           G(0, 1, 0) * (1 - tx) * ty * (1 - tz) + G(0, 1, 1) * (1 - tx) * ty * tz +
+           G(1, 0, 0) * tx * (1 - ty) * (1 - tz) + G(1, 0, 1) * tx * (1 - ty) * tz +
+           G(1, 1, 0) * tx * ty * (1 - tz) + G(1, 1, 1) * tx * ty * tz;
+#undef G
+}
+
+/* The pair term, :413-457 (and flat_tree.py:1070-1131 / 1171-1213): the
+ * full tensor from three permuted lookups, G_z(x,y,z), G_x(z,y,x),
+ * G_y(x,z,y), contracted with F_j / Fz_comsol.  Adds to v in source order. */
+static inline void corr_pair(const ocorr *c, double x, double y, double z, double fx, double fy, double fz,
+                             double *v) {
+    const double cL = c->cL;
+    const double xc = x * cL, yc = y * cL, zc = z * cL;
+    int ax, ay, az;
+    double tx, ty, tz;
+    grid_idx(xc, c->gmin, c->ginv, c->n, &ax, &tx);
+    grid_idx(yc, c->gmin, c->ginv, c->n, &ay, &ty);
+    grid_idx(zc, c->gmin, c->ginv, c->n, &az, &tz);
+    const int n = c->n;
+    const double gz_x = interp(c->u, n, ax, ay, az, tx, ty, tz);
+    const double gz_y = interp(c->v, n, ax, ay, az, tx, ty, tz);
+    const double gz_z = interp(c->w, n, ax, ay, az, tx, ty, tz);
+    const double gx_x = interp(c->w, n, az, ay, ax, tz, ty, tx);
+    const double gx_y = interp(c->v, n, az, ay, ax, tz, ty, tx);
+    const double gx_z = interp(c->u, n, az, ay, ax, tz, ty, tx);
+    const double gy_x = interp(c->u, n, ax, az, ay, tx, tz, ty);
+    const double gy_y = interp(c->w, n, ax, az, ay, tx, tz, ty);
+    const double gy_z = interp(c->v, n, ax, az, ay, tx, tz, ty);
+    const double common = c->Fz_inv * c->eta_r * cL;
+    const double sx = fx * common, sy = fy * common, sz = fz * common;
+    v[0] += gx_x * sx + gy_x * sy + gz_x * sz;
+    v[1] += gx_y * sx + gy_y * sy + gz_y * sz;
+    v[2] += gx_z * sx + gy_z * sy + gz_z * sz;
+}
+
+/* ------------------------------------------------------------------------ */
 /* Direct O(N^2) Oseen convection, direct_droplet_force_calculator.py:354-411 */
 /* d = x_i - x_j, no contact cut, COMSOL correction off.                     */
 /* ------------------------------------------------------------------------ */
@@ -140,6 +204,46 @@ EXPORT void dem_oracle_direct_convection(int n, const double *x, const double *y
         vx[i] = Cx;
         vy[i] = Cy;
         vz[i] = Cz;
+    }
+}
+
+/* The same with the periodic-image correction enabled, :354-464: per pair the
+ * Stokeslet term, then the correction term; after the loop the self term
+ * g_self * F_i. */
+EXPORT void dem_oracle_direct_convection_corr(int n, const double *x, const double *y, const double *z,
+                                              const double *fx, const double *fy, const double *fz,
+                                              double eta_const, double L, int periodic, int gn,
+                                              const double *gu, const double *gv, const double *gw, double gmin,
+                                              double ginv, double Fz_inv, double cL, double eta_r, double g_self,
+                                              double *vx, double *vy, double *vz, int i0, int i1, int nthreads) {
+    const ocorr c = {gn, gu, gv, gw, gmin, ginv, Fz_inv, cL, eta_r, g_self};
+    set_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int i = i0; i < i1; ++i) {
+        double C[3] = {0.0, 0.0, 0.0};
+        const double xi = x[i], yi = y[i], zi = z[i];
+        for (int j = 0; j < n; ++j) {
+            if (i == j) continue;
+            double X = xi - x[j], Y = yi - y[j], Z = zi - z[j];
+            if (periodic) {
+                X = mic(X, L);
+                Y = mic(Y, L);
+                Z = mic(Z, L);
+            }
+            const double rr = sqrt(ipow2(X) + ipow2(Y) + ipow2(Z));
+            const double Fx = fx[j], Fy = fy[j], Fz = fz[j];
+            const double r3 = ipow3(rr);
+            C[0] += eta_const * ((1 / rr + (ipow2(X)) / r3) * Fx + (X * Y) / r3 * Fy + (X * Z) / r3 * Fz);
+            C[1] += eta_const * ((X * Y) / r3 * Fx + (1 / rr + (ipow2(Y)) / r3) * Fy + (Y * Z) / r3 * Fz);
+            C[2] += eta_const * ((X * Z) / r3 * Fx + (Y * Z) / r3 * Fy + (1 / rr + (ipow2(Z)) / r3) * Fz);
+            corr_pair(&c, X, Y, Z, Fx, Fy, Fz, C);
+        }
+        C[0] += g_self * fx[i];
+        C[1] += g_self * fy[i];
+        C[2] += g_self * fz[i];
+        vx[i] = C[0];
+        vy[i] = C[1];
+        vz[i] = C[2];
     }
 }
 
@@ -381,6 +485,8 @@ typedef struct {
     int level_off[64];
     int n_levels;
     double *px, *py, *pz, *pr, *pf; /* particles; pf (n,3) forces */
+    int corr_on;                    /* load_periodic_correction, flat_tree.py:141-167 */
+    ocorr corr;
 } otree;
 
 EXPORT void *dem_oracle_tree_create(int num_particles, int mpl, double theta, int max_nodes_override) {
@@ -416,6 +522,17 @@ EXPORT void dem_oracle_tree_destroy(void *h) {
                     t->part_oct, t->px, t->py, t->pz, t->pr, t->pf};
     for (size_t k = 0; k < sizeof(ptrs) / sizeof(ptrs[0]); ++k) free(ptrs[k]);
     free(t);
+}
+
+/* load_periodic_correction, flat_tree.py:141-167 (gn == 0 switches it off).
+ * The grids are borrowed: they must outlive the tree's use of them. */
+EXPORT void dem_oracle_tree_set_correction(void *h, int gn, const double *gu, const double *gv, const double *gw,
+                                           double gmin, double ginv, double Fz_inv, double cL, double eta_r,
+                                           double g_self) {
+    otree *t = h;
+    const ocorr c = {gn, gu, gv, gw, gmin, ginv, Fz_inv, cL, eta_r, g_self};
+    t->corr = c;
+    t->corr_on = gn > 0;
 }
 
 EXPORT void dem_oracle_tree_set_params(void *h, double theta, int mpl) {
@@ -783,7 +900,9 @@ EXPORT void dem_oracle_tree_propagate_forces(void *h, const double *forces) {
 
 /* _compute_stokeslet_kernel (:1000-1280) when stokes_factor <= 0, else
  * _compute_total_velocity_kernel (:1326-1588).  forces (n,3): the array
- * passed as forces_np.  Correction off.  Rows [i0, i1). */
+ * passed as forces_np.  With a correction set (dem_oracle_tree_set_correction)
+ * its pair terms follow every leaf pair and accepted node; the self term is
+ * added by the Stokeslet walk only, as in the reference.  Rows [i0, i1). */
 EXPORT void dem_oracle_tree_velocity(void *h, const double *forces, double eta_const,
                                      double stokes_factor, double *v, int i0, int i1, int nthreads) {
     otree *t = h;
@@ -831,6 +950,13 @@ EXPORT void dem_oracle_tree_velocity(void *h, const double *forces, double eta_c
                             vx += coeff * (Fx + dx * inv_r2 * dot);
                             vy += coeff * (Fy + dy * inv_r2 * dot);
                             vz += coeff * (Fz + dz * inv_r2 * dot);
+                            if (t->corr_on) { /* :1070-1131 */
+                                double acc[3] = {vx, vy, vz};
+                                corr_pair(&t->corr, dx, dy, dz, Fx, Fy, Fz, acc);
+                                vx = acc[0];
+                                vy = acc[1];
+                                vz = acc[2];
+                            }
                         }
                     }
                 }
@@ -857,6 +983,13 @@ EXPORT void dem_oracle_tree_velocity(void *h, const double *forces, double eta_c
                 vx += coeff * (Fx + dx * inv_r2 * dot);
                 vy += coeff * (Fy + dy * inv_r2 * dot);
                 vz += coeff * (Fz + dz * inv_r2 * dot);
+                if (t->corr_on) { /* monopole term of the correction, :1171-1213 */
+                    double acc[3] = {vx, vy, vz};
+                    corr_pair(&t->corr, dx, dy, dz, Fx, Fy, Fz, acc);
+                    vx = acc[0];
+                    vy = acc[1];
+                    vz = acc[2];
+                }
                 /* dipole correction :1215-1265 */
                 const double r3s = t->R3[node];
                 double cmx, cmy, cmz;
@@ -892,6 +1025,11 @@ EXPORT void dem_oracle_tree_velocity(void *h, const double *forces, double eta_c
             } else {
                 node = t->first_child[node];
             }
+        }
+        if (t->corr_on && !(stokes_factor > 0)) { /* self term, Stokeslet walk only (:1271-1276) */
+            vx += t->corr.g_self * forces[3 * i];
+            vy += t->corr.g_self * forces[3 * i + 1];
+            vz += t->corr.g_self * forces[3 * i + 2];
         }
         v[3 * i] = vx;
         v[3 * i + 1] = vy;

@@ -47,6 +47,9 @@ def lib():
         L.dem_oracle_max_threads.restype = i
         L.dem_oracle_direct_forces.argtypes = [i, pd, pd, pd, pd, d, d, i, pd, pd, pd, i, i, i]
         L.dem_oracle_direct_convection.argtypes = [i, pd, pd, pd, pd, pd, pd, d, d, i, pd, pd, pd, i, i, i]
+        L.dem_oracle_direct_convection_corr.argtypes = [i, pd, pd, pd, pd, pd, pd, d, d, i, i, pd, pd, pd, d, d, d,
+                                                        d, d, d, pd, pd, pd, i, i, i]
+        L.dem_oracle_tree_set_correction.argtypes = [vp, i, pd, pd, pd, d, d, d, d, d, d]
         L.dem_oracle_euler_direct.argtypes = [i, pd, pd, pd, pd, d, d, d, i]
         L.dem_oracle_euler_total.argtypes = [i, pd, pd, d, d, i]
         L.dem_oracle_hash_detect.argtypes = [i, pd, pd, d, i, i, pi32, i64, pi64]
@@ -131,6 +134,54 @@ def direct_convection(pos, F, eta_const, L, periodic, rows=None, threads=0):
     return np.ascontiguousarray(out.T)
 
 
+class Correction:
+    """Parameters of the periodic-image Oseen correction as the reference loads
+    them (direct_droplet_force_calculator.py:74-120, flat_tree.py:141-167):
+    the regular n^3 grids and
+
+        ginv = 1 / grid_dx,  Fz_inv = 1 / Fz_comsol,  cL = L_comsol / L_sim,
+        eta_r = eta_comsol / eta_sim,  g_self = w(0,0,0) / Fz_comsol * eta_r * cL.
+    """
+
+    def __init__(self, grid_u, grid_v, grid_w, grid_min, grid_dx, Fz_comsol, L_comsol, eta_comsol, L_sim, eta_sim,
+                 self_coeff):
+        self.u, self.v, self.w = (np.ascontiguousarray(g, dtype=np.float64) for g in (grid_u, grid_v, grid_w))
+        self.n = int(self.u.shape[0])
+        self.gmin = float(grid_min)
+        self.ginv = 1.0 / float(grid_dx)
+        self.Fz_inv = 1.0 / float(Fz_comsol)
+        self.cL = float(L_comsol) / float(L_sim)
+        self.eta_r = float(eta_comsol) / float(eta_sim)
+        self.g_self = float(self_coeff)
+
+    @classmethod
+    def from_golden(cls, g):
+        """From a tests/golden corr_* case (the grid and the reference's own self coefficient)."""
+        return cls(g["grid_u"], g["grid_v"], g["grid_w"], g["grid_min"], g["grid_dx"], g["Fz_comsol"],
+                   g["L_comsol"], g["eta_comsol"], g["L"], g["eta_oil"], g["corr_self_coeff"])
+
+    def args(self):
+        return (self.n, _pd(self.u), _pd(self.v), _pd(self.w), self.gmin, self.ginv, self.Fz_inv, self.cL,
+                self.eta_r, self.g_self)
+
+
+def direct_convection_corr(pos, F, eta_const, L, periodic, corr: Correction, rows=None, threads=0):
+    """_calculate_convection_velocities with the periodic-image correction on,
+    direct_droplet_force_calculator.py:354-464."""
+    pos = _f64(pos).reshape(-1, 3)
+    F = _f64(F).reshape(-1, 3)
+    n = len(pos)
+    x, y, z = (_f64(pos[:, k]) for k in range(3))
+    fx, fy, fz = (_f64(F[:, k]) for k in range(3))
+    out = np.zeros((3, n))
+    i0, i1 = _rows(n, rows)
+    lib().dem_oracle_direct_convection_corr(
+        n, _pd(x), _pd(y), _pd(z), _pd(fx), _pd(fy), _pd(fz), eta_const, L, int(periodic), *corr.args(),
+        _pd(out[0]), _pd(out[1]), _pd(out[2]), i0, i1, threads,
+    )
+    return np.ascontiguousarray(out.T)
+
+
 def euler_direct(pos, r, F, V, stokes_factor, dt, L, periodic):
     """euler_droplet_solver.py:121-131 on a copy of ``pos``."""
     p = _f64(pos).reshape(-1, 3).copy()
@@ -200,7 +251,7 @@ def merge(pos, r, pairs):
 
 
 class Tree:
-    """FlatOctree, flat_tree.py:36-1630 (correction off)."""
+    """FlatOctree, flat_tree.py:36-1630 (periodic-image correction optional)."""
 
     def __init__(self, num_particles, theta=0.5, mpl=1, max_nodes=0):
         self.h = lib().dem_oracle_tree_create(int(num_particles), int(mpl), float(theta), int(max_nodes))
@@ -214,6 +265,14 @@ class Tree:
     def update_params(self, theta, mpl):
         self.theta, self.mpl = theta, mpl
         lib().dem_oracle_tree_set_params(self.h, float(theta), int(mpl))
+
+    def set_correction(self, corr: Correction | None):
+        """load_periodic_correction, flat_tree.py:141-167 (None switches it off)."""
+        self._corr = corr  # the C side borrows the grids
+        if corr is None:
+            lib().dem_oracle_tree_set_correction(self.h, 0, None, None, None, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0)
+        else:
+            lib().dem_oracle_tree_set_correction(self.h, *corr.args())
 
     def build(self, pos, r, L, periodic=False):
         pos = _f64(pos).reshape(-1, 3)

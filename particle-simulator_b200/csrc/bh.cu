@@ -41,6 +41,7 @@
 #include <algorithm>
 #include <vector>
 
+#include "corr.cuh"
 #include "mixed_common.cuh"
 #include "scan.cuh"
 
@@ -84,6 +85,7 @@ struct dem_bh {
     int32_t *scan_in = nullptr, *coff = nullptr;  // [max_nodes + 1] children per node of a level, offsets
     BhNodes nd{};
     std::vector<int> level_off;
+    const dem_corr *corr = nullptr;  // periodic-image correction of the velocity walk (borrowed), or none
 };
 
 namespace {
@@ -480,6 +482,10 @@ struct BhWalk {
     double L, halfL;
     unsigned long long *counters;  // [0] leaf pair terms, [1] accepted-node terms
     uint32_t *err;
+    // periodic-image correction (velocity walk with CORR): FP32 grid view whose
+    // slope corr.A is set per launch from corr_A (metres -> grid) and ell
+    CorrF32 corr;
+    double corr_A, corr_common, corr_self;
 };
 
 template <bool PER>
@@ -489,7 +495,9 @@ __device__ __forceinline__ double bh_mic(double d, double L, double halfL) {
 
 // FORCE: F_i = m r_i^3 (sum_leaf r_j^3 P(d)/|d|^7 + sum_nodes R^3 P(D)/|D|^7), d = x_j - x_i, D = c - x_i
 // else:  u_i = [F_i / (stokes r_i)] + eta (sum_leaf G(e) F_j + sum_nodes G(e) F_node + dipole), e = x_i - x_j
-template <bool PER, bool FORCE>
+// CORR (velocity): + the periodic-image correction of every leaf pair and
+// accepted node (FP32, summed apart) and, when stokes <= 0, the self term.
+template <bool PER, bool FORCE, bool CORR = false>
 __global__ void __launch_bounds__(BH_T) bh_walk_kernel(const BhWalk w, double coeff, double stokes,
                                                        double *__restrict__ ox, double *__restrict__ oy,
                                                        double *__restrict__ oz, double *__restrict__ fsort_out) {
@@ -498,6 +506,8 @@ __global__ void __launch_bounds__(BH_T) bh_walk_kernel(const BhWalk w, double co
     const int n = w.n, cap = w.cap;
     const double inv_ell = pow2_inv_of(w.scales[0]);
     const double fsc = FORCE ? 1.0 : pow2_inv_of(w.scales[1]);
+    CorrF32 cf = w.corr;
+    if (CORR) cf.A = (float)(w.corr_A / inv_ell);  // separations are in units of ell
     const float Ls = (float)(w.L * inv_ell), invLs = (float)(1.0 / (w.L * inv_ell));
     const double gox = w.geom[0], goy = w.geom[1], goz = w.geom[2];
     unsigned long long pairs = 0, nodes = 0;
@@ -512,6 +522,7 @@ __global__ void __launch_bounds__(BH_T) bh_walk_kernel(const BhWalk w, double co
         const float xs = (float)((xi - gox) * inv_ell), ys = (float)((yi - goy) * inv_ell),
                     zs = (float)((zi - goz) * inv_ell);
         float ax = 0.f, ay = 0.f, az = 0.f;
+        float cx = 0.f, cy = 0.f, cz = 0.f;  // correction sums (CORR)
         int sp = 1;
         if (lane == 0) stack[wp][0] = 0;
         __syncwarp();
@@ -584,6 +595,7 @@ __global__ void __launch_bounds__(BH_T) bh_walk_kernel(const BhWalk w, double co
                         ax += rinv3 * (Ux - Wx - tr * ex) + 3.f * ex * q * rinv5;
                         ay += rinv3 * (Uy - Wy - tr * ey) + 3.f * ey * q * rinv5;
                         az += rinv3 * (Uz - Wz - tr * ez) + 3.f * ez * q * rinv5;
+                        if (CORR) corr_pair32(cf, ex, ey, ez, fnx, fny, fnz, cx, cy, cz);
                     }
                 }
                 continue;
@@ -618,6 +630,7 @@ __global__ void __launch_bounds__(BH_T) bh_walk_kernel(const BhWalk w, double co
                         ax = fmaf(rinv, fmaf(ex, dot * rinv2, fx), ax);
                         ay = fmaf(rinv, fmaf(ey, dot * rinv2, fy), ay);
                         az = fmaf(rinv, fmaf(ez, dot * rinv2, fz), az);
+                        if (CORR) corr_pair32(cf, ex, ey, ez, fx, fy, fz, cx, cy, cz);
                     }
                 }
                 continue;
@@ -652,6 +665,17 @@ __global__ void __launch_bounds__(BH_T) bh_walk_kernel(const BhWalk w, double co
                     vx += w.fsort[si] * a;
                     vy += w.fsort[cap + si] * a;
                     vz += w.fsort[2 * (size_t)cap + si] * a;
+                }
+                if (CORR) {  // sum of G F_scaled -> G F common
+                    const double g = w.corr_common / fsc;
+                    vx += g * cx;
+                    vy += g * cy;
+                    vz += g * cz;
+                    if (!(stokes > 0.0)) {  // self term (Stokeslet walk only, flat_tree.py:1271-1276)
+                        vx += w.corr_self * w.fsort[si];
+                        vy += w.corr_self * w.fsort[cap + si];
+                        vz += w.corr_self * w.fsort[2 * (size_t)cap + si];
+                    }
                 }
             }
             ox[i] = vx;
@@ -909,6 +933,14 @@ static BhWalk walk_args(dem_bh *b, float theta) {
     w.halfL = 0.5 * b->L;
     w.counters = b->counters;
     w.err = b->ctx->d_err;
+    w.corr = CorrF32{};
+    w.corr_A = w.corr_common = w.corr_self = 0.0;
+    if (b->corr) {
+        w.corr = corr_f32(b->corr, 1.0);
+        w.corr_A = b->corr->cL * b->corr->ginv;
+        w.corr_common = b->corr->common;
+        w.corr_self = b->corr->g_self;
+    }
     return w;
 }
 
@@ -957,14 +989,30 @@ int dem_bh_velocity(dem_bh *b, const double *fx, const double *fy, const double 
         return rc;
     const BhWalk w = walk_args(b, (float)theta);
     dem_prof_begin(ctx, "bh_velocity_walk", s);
-    if (b->periodic)
+    if (b->corr) {
+        if (b->periodic)
+            bh_walk_kernel<true, false, true><<<walk_grid(b), BH_T, 0, counted(s)>>>(w, eta_const, stokes_factor, vx,
+                                                                                     vy, vz, nullptr);
+        else
+            bh_walk_kernel<false, false, true><<<walk_grid(b), BH_T, 0, counted(s)>>>(w, eta_const, stokes_factor, vx,
+                                                                                      vy, vz, nullptr);
+    } else if (b->periodic) {
         bh_walk_kernel<true, false><<<walk_grid(b), BH_T, 0, counted(s)>>>(w, eta_const, stokes_factor, vx, vy, vz,
                                                                            nullptr);
-    else
+    } else {
         bh_walk_kernel<false, false><<<walk_grid(b), BH_T, 0, counted(s)>>>(w, eta_const, stokes_factor, vx, vy, vz,
                                                                             nullptr);
+    }
     dem_prof_end(ctx, s);
     return dem_check_launch(ctx, "bh velocity walk");
+}
+
+int dem_bh_set_correction(dem_bh *b, const dem_corr *corr) {
+    if (!b) return DEM_E_INVALID;
+    if (corr && corr->ctx && corr->ctx->device != b->ctx->device)
+        return dem_set_error(b->ctx, DEM_E_INVALID, "correction grid lives on another device");
+    b->corr = corr;
+    return DEM_OK;
 }
 
 int dem_bh_set_window(dem_bh *b, int window_level) {

@@ -10,7 +10,12 @@
 //
 // j-tiles (x, y, z, r, r^3) are staged in shared memory and read as
 // broadcasts; the pair work is FP64-pipe bound (IEEE sqrt / division).
+//
+// With the periodic-image correction loaded, the convection kernel adds each
+// pair's correction term right after its Stokeslet term and the self term
+// after the loop (:413-464), bit-identical to the CPU restatement.
 #include "common.cuh"
+#include "corr.cuh"
 
 namespace dem {
 
@@ -78,11 +83,12 @@ __global__ void __launch_bounds__(F64_THREADS) direct_force_fp64_kernel(int n, c
     }
 }
 
-template <bool PERIODIC>
+template <bool PERIODIC, bool CORR>
 __global__ void __launch_bounds__(F64_THREADS) direct_convection_fp64_kernel(
     int n, const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ z,
     const double *__restrict__ fx, const double *__restrict__ fy, const double *__restrict__ fz, double eta,
-    double L, double halfL, double *__restrict__ vx, double *__restrict__ vy, double *__restrict__ vz) {
+    double L, double halfL, CorrDev corr, double *__restrict__ vx, double *__restrict__ vy,
+    double *__restrict__ vz) {
     __shared__ double sx[F64_TILE], sy[F64_TILE], sz[F64_TILE], sfx[F64_TILE], sfy[F64_TILE], sfz[F64_TILE];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = i < n;
@@ -125,7 +131,13 @@ __global__ void __launch_bounds__(F64_THREADS) direct_convection_fp64_kernel(
             Cx += eta * ((inv_r + (X * X) / r3) * Fx + xy * Fy + xz * Fz);
             Cy += eta * (xy * Fx + (inv_r + (Y * Y) / r3) * Fy + yz * Fz);
             Cz += eta * (xz * Fx + yz * Fy + (inv_r + (Z * Z) / r3) * Fz);
+            if (CORR) corr_pair64(corr, X, Y, Z, Fx, Fy, Fz, Cx, Cy, Cz);
         }
+    }
+    if (CORR && active) {
+        Cx += corr.g_self * fx[i];
+        Cy += corr.g_self * fy[i];
+        Cz += corr.g_self * fz[i];
     }
     if (active) {
         vx[i] = Cx;
@@ -152,14 +164,32 @@ int launch_direct_convection_fp64(dem_ctx *ctx, int n, const double *x, const do
                                   int periodic, double *vx, double *vy, double *vz, cudaStream_t s) {
     const int grid = ceil_div(n, F64_THREADS);
     dem_prof_begin(ctx, "fp64_convection_pass", s);
+    const CorrDev none{};
     if (periodic)
-        direct_convection_fp64_kernel<true>
-            <<<grid, F64_THREADS, 0, counted(s)>>>(n, x, y, z, fx, fy, fz, eta, L, L * 0.5, vx, vy, vz);
+        direct_convection_fp64_kernel<true, false>
+            <<<grid, F64_THREADS, 0, counted(s)>>>(n, x, y, z, fx, fy, fz, eta, L, L * 0.5, none, vx, vy, vz);
     else
-        direct_convection_fp64_kernel<false>
-            <<<grid, F64_THREADS, 0, counted(s)>>>(n, x, y, z, fx, fy, fz, eta, L, L * 0.5, vx, vy, vz);
+        direct_convection_fp64_kernel<false, false>
+            <<<grid, F64_THREADS, 0, counted(s)>>>(n, x, y, z, fx, fy, fz, eta, L, L * 0.5, none, vx, vy, vz);
     dem_prof_end(ctx, s);
     return dem_check_launch(ctx, "direct_convection_fp64");
+}
+
+int launch_direct_convection_fp64_corr(dem_ctx *ctx, const dem_corr *c, int n, const double *x, const double *y,
+                                       const double *z, const double *fx, const double *fy, const double *fz,
+                                       double eta, double L, int periodic, double *vx, double *vy, double *vz,
+                                       cudaStream_t s) {
+    const int grid = ceil_div(n, F64_THREADS);
+    const CorrDev cv = corr_view(c);
+    dem_prof_begin(ctx, "fp64_convection_corr_pass", s);
+    if (periodic)
+        direct_convection_fp64_kernel<true, true>
+            <<<grid, F64_THREADS, 0, counted(s)>>>(n, x, y, z, fx, fy, fz, eta, L, L * 0.5, cv, vx, vy, vz);
+    else
+        direct_convection_fp64_kernel<false, true>
+            <<<grid, F64_THREADS, 0, counted(s)>>>(n, x, y, z, fx, fy, fz, eta, L, L * 0.5, cv, vx, vy, vz);
+    dem_prof_end(ctx, s);
+    return dem_check_launch(ctx, "direct_convection_fp64_corr");
 }
 
 }  // namespace dem

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "corr.cuh"
 #include "scan.cuh"
 
 struct dem_tree {
@@ -44,6 +45,7 @@ struct dem_tree {
     double *pf = nullptr;                  // [3][N]: forces of the last force walk
     int32_t *part_node = nullptr, *part_oct = nullptr, *leaf_idx = nullptr;
     int32_t *h_total = nullptr;            // pinned
+    const dem_corr *corr = nullptr;        // periodic-image correction (borrowed), or none
 };
 
 namespace dem {
@@ -471,13 +473,16 @@ __global__ void __launch_bounds__(128) force_walk_kernel(TreeDev t, double m_con
 }
 
 // _compute_stokeslet_kernel :1000-1280 (stokes <= 0) and
-// _compute_total_velocity_kernel :1326-1588 (stokes > 0); correction off.
-template <bool PER>
+// _compute_total_velocity_kernel :1326-1588 (stokes > 0); with CORR the
+// periodic-image correction after every leaf pair (:1070-1131) and accepted
+// node (:1171-1213), and the self term of the Stokeslet walk (:1271-1276).
+template <bool PER, bool CORR>
 __global__ void __launch_bounds__(128) velocity_walk_kernel(TreeDev t, const double *__restrict__ Fx_,
                                                             const double *__restrict__ Fy_,
                                                             const double *__restrict__ Fz_, double eta,
-                                                            double theta_sq, double stokes, double *__restrict__ vx,
-                                                            double *__restrict__ vy, double *__restrict__ vz) {
+                                                            double theta_sq, double stokes, CorrDev corr,
+                                                            double *__restrict__ vx, double *__restrict__ vy,
+                                                            double *__restrict__ vz) {
     const int M = t.max_nodes, N = t.cap, n = t.n;
     const double L = t.L, halfL = 0.5 * t.L;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -526,6 +531,7 @@ __global__ void __launch_bounds__(128) velocity_walk_kernel(TreeDev t, const dou
                             ux += coeff * (Fx + dx * inv_r2 * dot);
                             uy += coeff * (Fy + dy * inv_r2 * dot);
                             uz += coeff * (Fz + dz * inv_r2 * dot);
+                            if (CORR) corr_pair64(corr, dx, dy, dz, Fx, Fy, Fz, ux, uy, uz);
                         }
                     }
                 }
@@ -552,6 +558,7 @@ __global__ void __launch_bounds__(128) velocity_walk_kernel(TreeDev t, const dou
                 ux += coeff * (Fx + dx * inv_r2 * dot);
                 uy += coeff * (Fy + dy * inv_r2 * dot);
                 uz += coeff * (Fz + dz * inv_r2 * dot);
+                if (CORR) corr_pair64(corr, dx, dy, dz, Fx, Fy, Fz, ux, uy, uz);
                 // dipole correction :1215-1265, R^3-weighted centre (same as get_center)
                 const double cmx = cx, cmy = cy, cmz = cz;
                 const double *P = t.fs + 3 * (size_t)M;
@@ -578,6 +585,11 @@ __global__ void __launch_bounds__(128) velocity_walk_kernel(TreeDev t, const dou
             } else {
                 node = t.first_child[node];
             }
+        }
+        if (CORR && !(stokes > 0)) {  // self term, Stokeslet walk only
+            ux += corr.g_self * Fx_[i];
+            uy += corr.g_self * Fy_[i];
+            uz += corr.g_self * Fz_[i];
         }
         vx[i] = ux;
         vy[i] = uy;
@@ -787,12 +799,34 @@ int dem_tree_velocity(dem_tree *t, const double *fx, const double *fy, const dou
     cudaStream_t s = (cudaStream_t)stream;
     dem_prof_begin(t->ctx, "tree_velocity_walk", s);
     const int grid = ceil_div(t->n, 128);
-    if (t->periodic)
-        velocity_walk_kernel<true><<<grid, 128, 0, counted(s)>>>(view(t), fx, fy, fz, eta_const, theta_sq, stokes_factor, vx, vy, vz);
-    else
-        velocity_walk_kernel<false><<<grid, 128, 0, counted(s)>>>(view(t), fx, fy, fz, eta_const, theta_sq, stokes_factor, vx, vy, vz);
+    const TreeDev tv = view(t);
+    if (t->corr) {
+        const CorrDev cv = corr_view(t->corr);
+        if (t->periodic)
+            velocity_walk_kernel<true, true><<<grid, 128, 0, counted(s)>>>(tv, fx, fy, fz, eta_const, theta_sq,
+                                                                           stokes_factor, cv, vx, vy, vz);
+        else
+            velocity_walk_kernel<false, true><<<grid, 128, 0, counted(s)>>>(tv, fx, fy, fz, eta_const, theta_sq,
+                                                                            stokes_factor, cv, vx, vy, vz);
+    } else {
+        const CorrDev none{};
+        if (t->periodic)
+            velocity_walk_kernel<true, false><<<grid, 128, 0, counted(s)>>>(tv, fx, fy, fz, eta_const, theta_sq,
+                                                                            stokes_factor, none, vx, vy, vz);
+        else
+            velocity_walk_kernel<false, false><<<grid, 128, 0, counted(s)>>>(tv, fx, fy, fz, eta_const, theta_sq,
+                                                                             stokes_factor, none, vx, vy, vz);
+    }
     dem_prof_end(t->ctx, s);
     return dem_check_launch(t->ctx, "tree velocity walk");
+}
+
+int dem_tree_set_correction(dem_tree *t, const dem_corr *corr) {
+    if (!t) return DEM_E_INVALID;
+    if (corr && corr->ctx && corr->ctx->device != t->device)
+        return dem_set_error(t->ctx, DEM_E_INVALID, "correction grid lives on another device");
+    t->corr = corr;
+    return DEM_OK;
 }
 
 int dem_tree_stats(const dem_tree *t, int64_t *out) {

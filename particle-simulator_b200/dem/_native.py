@@ -64,6 +64,11 @@ SIGNATURES = {
     "dem_bh_velocity": (_i, [_vp, _vp, _vp, _vp, _d, _d, _d, _vp, _vp, _vp, _vp]),
     "dem_bh_stats": (_i, [_vp, C.POINTER(_i64)]),
     "dem_bh_set_window": (_i, [_vp, _i]),
+    "dem_bh_set_correction": (_i, [_vp, _vp]),
+    "dem_corr_create": (_i, [_vp, _i, _vp, _vp, _vp, _d, _d, _d, _d, _d, _d, C.POINTER(_vp)]),
+    "dem_corr_destroy": (None, [_vp]),
+    "dem_corr_info": (_i, [_vp, C.POINTER(_i), C.POINTER(_d), C.POINTER(_d)]),
+    "dem_direct_convection_corr": (_i, [_vp, _vp, _i] + [_vp] * 7 + [_d, _d, _i, _i, _vp, _vp, _vp, _vp]),
     "dem_batch_create": (_i, [_vp, _i, C.POINTER(_i64), C.POINTER(_d), _i, C.POINTER(_vp)]),
     "dem_batch_destroy": (None, [_vp]),
     "dem_batch_info": (_i, [_vp, C.POINTER(_i), C.POINTER(_i), C.POINTER(_i), C.POINTER(_i)]),
@@ -92,6 +97,7 @@ SIGNATURES = {
     "dem_tree_propagate_forces": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "dem_tree_velocity": (_i, [_vp, _vp, _vp, _vp, _d, _d, _d, _vp, _vp, _vp, _vp]),
     "dem_tree_stats": (_i, [_vp, C.POINTER(_i64)]),
+    "dem_tree_set_correction": (_i, [_vp, _vp]),
     "dem_tree_nodes": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "dem_tree_leaf_indices": (_i, [_vp, _vp, _vp]),
 }
@@ -274,6 +280,15 @@ class Context:
             "direct_convection",
         )
 
+    def direct_convection_corr(self, corr: "Correction", n, pos, r, F, eta_const, L, periodic, precision, out):
+        self._check(
+            lib().dem_direct_convection_corr(self.handle, corr.handle, n, ptr(pos[0]), ptr(pos[1]), ptr(pos[2]),
+                                             ptr(r), ptr(F[0]), ptr(F[1]), ptr(F[2]), float(eta_const), float(L),
+                                             int(periodic), int(precision), ptr(out[0]), ptr(out[1]),
+                                             ptr(out[2]), self.stream()),
+            "direct_convection_corr",
+        )
+
     def direct_vjp(self, n, pos, r, F, lam, m_const, eta_const, stokes, L, periodic, mu, g, gr):
         self._check(
             lib().dem_direct_vjp(self.handle, n, ptr(pos[0]), ptr(pos[1]), ptr(pos[2]), ptr(r), ptr(F[0]), ptr(F[1]),
@@ -316,6 +331,41 @@ class Context:
         )
 
 
+class Correction:
+    """One ``dem_corr``: a periodic-image correction grid on the device.
+
+    Grids: (n, n, n) float64 host arrays (C order), nodes grid_min + k / inv_dx.
+    Scalars as load_periodic_correction computes them."""
+
+    def __init__(self, ctx: Context, grid_u, grid_v, grid_w, grid_min, inv_dx, Fz_inv, L_ratio, eta_ratio,
+                 self_coeff):
+        grids = [np.ascontiguousarray(g, dtype=np.float64) for g in (grid_u, grid_v, grid_w)]
+        n = grids[0].shape[0] if grids[0].ndim == 3 else -1
+        if any(g.shape != (n, n, n) for g in grids):
+            raise ValueError("correction grids must be three (n, n, n) arrays")
+        self.ctx = ctx  # the grid lives on ctx's device; keep the context alive
+        self.n = n
+        self.handle = _vp()
+        ctx._check(lib().dem_corr_create(ctx.handle, n, grids[0].ctypes.data, grids[1].ctypes.data,
+                                         grids[2].ctypes.data, float(grid_min), float(inv_dx), float(Fz_inv),
+                                         float(L_ratio), float(eta_ratio), float(self_coeff),
+                                         C.byref(self.handle)), "corr_create")
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value and _lib is not None:
+            try:
+                _lib.dem_corr_destroy(h)
+            except Exception:  # pragma: no cover
+                pass
+            self.handle = None
+
+    def info(self):
+        n, c, g = _i(), _d(), _d()
+        self.ctx._check(lib().dem_corr_info(self.handle, C.byref(n), C.byref(c), C.byref(g)), "corr_info")
+        return dict(n=n.value, common=c.value, self_coeff=g.value)
+
+
 class Tree:
     """One ``dem_tree`` (FP64 flat octree) owned by a Context."""
 
@@ -353,6 +403,11 @@ class Tree:
         self.ctx._check(lib().dem_tree_velocity(self.handle, *a, float(eta_const), float(theta_sq),
                                                 float(stokes_factor), ptr(out[0]), ptr(out[1]), ptr(out[2]),
                                                 self.ctx.stream()), "tree_velocity")
+
+    def set_correction(self, corr: Correction | None):
+        self._corr = corr  # the tree borrows the grid
+        self.ctx._check(lib().dem_tree_set_correction(self.handle, None if corr is None else corr.handle),
+                        "tree_set_correction")
 
     def stats(self):
         out = (_i64 * 8)()
@@ -404,6 +459,11 @@ class MortonTree:
 
     def set_window(self, window_level):
         self.ctx._check(lib().dem_bh_set_window(self.handle, int(window_level)), "bh_set_window")
+
+    def set_correction(self, corr: Correction | None):
+        self._corr = corr  # the tree borrows the grid
+        self.ctx._check(lib().dem_bh_set_correction(self.handle, None if corr is None else corr.handle),
+                        "bh_set_correction")
 
     def stats(self):
         out = (_i64 * 8)()

@@ -11,6 +11,11 @@ csrc/direct_mixed.cu):
 * ``precision="mixed"`` evaluates pair terms in FP32 with compensated sums and
   recomputes near-contact pairs in FP64 (relative force error ~1e-7 norm-wise).
 
+With ``load_periodic_correction`` the convection adds the periodic-image
+correction of every pair and the self term (:413-464), in FP64 bit-identical
+to the reference's order or, with ``precision="mixed"``, as an FP32 pass
+(csrc/corr.cu).
+
 Inputs may be numpy arrays (results come back as numpy, as in the reference)
 or CUDA torch tensors (results stay on the device as torch tensors).
 """
@@ -21,6 +26,7 @@ import numpy as np
 
 from .. import _native as N
 from .._io import Stager
+from ..periodic_correction.comsol_lattice_correction import correction_fields, to_device
 from .force_calculator_base import ForceCalculator
 
 EPS0 = 8.85418781762039e-12  # reference value, direct_droplet_force_calculator.py:23
@@ -61,16 +67,21 @@ class DirectDropletForceCalculator(ForceCalculator):
         self.precision = precision
         self._ctx = N.Context(max(int(num_particles), 1), device)
         self._io = Stager(self._ctx)
+        self._corr = None  # device grid of the periodic-image correction
+        self.__dict__.update(correction_fields(None))
 
     # -- reference API ------------------------------------------------------
     def load_periodic_correction(self, correction, L_sim: float):
-        """dem/force_calculator/direct_droplet_force_calculator.py:74-120."""
+        """dem/force_calculator/direct_droplet_force_calculator.py:74-120: uploads the
+        grid; from then on every convection call adds the correction."""
         if self.correction_grid_resolution == 0:
             raise RuntimeError(
                 "correction_grid_resolution=0: correction grids were not allocated; "
                 "re-create DirectDropletForceCalculator with correction_grid_resolution > 0."
             )
-        raise NotImplementedError("the COMSOL periodic correction is not part of this build")
+        self._corr, scalars = to_device(self._ctx, correction, L_sim, self.eta_oil,
+                                        max(self.correction_grid_resolution, 2))
+        self.__dict__.update(correction_fields(scalars))
 
     @property
     def periodic(self) -> bool:
@@ -88,8 +99,12 @@ class DirectDropletForceCalculator(ForceCalculator):
 
     def _convection_dev(self, st, F):
         V = self._io.buf.dev("velocities", (3, st.n))
-        self._ctx.direct_convection(st.n, st.pos, st.r, F, self.eta_const, self.L, self.periodic,
-                                    N.PRECISIONS[self.precision], V)
+        if self._corr is not None:
+            self._ctx.direct_convection_corr(self._corr, st.n, st.pos, st.r, F, self.eta_const, self.L,
+                                             self.periodic, N.PRECISIONS[self.precision], V)
+        else:
+            self._ctx.direct_convection(st.n, st.pos, st.r, F, self.eta_const, self.L, self.periodic,
+                                        N.PRECISIONS[self.precision], V)
         return V
 
     def calculate(self, positions, radii):

@@ -16,6 +16,7 @@ import numpy as np
 
 from .. import _native as N
 from .._io import Stager
+from ..periodic_correction.comsol_lattice_correction import correction_fields, to_device
 
 _FIELDS_I32 = ("count", "first_child", "next", "leaf_start")
 
@@ -100,6 +101,8 @@ class FlatOctree:
         self.nodes = OctreeNode(self, max_nodes)
         self.leaf_indices = _Field(lambda: me()._leaf_indices())
         self._F = None  # device SoA forces of the last force walk
+        self._corr = None  # device grid of the periodic-image correction
+        self.__dict__.update(correction_fields(None))
 
     # -- parameters (flat_tree.py:169-174) ------------------------------------
     def update_params(self, theta: float, mpl: int) -> None:
@@ -108,9 +111,13 @@ class FlatOctree:
         self._theta_sq = theta * theta
 
     def load_periodic_correction(self, correction, L_sim: float, eta_sim: float = None):
+        """flat_tree.py:141-167: the velocity walks add the correction from now on."""
         if self.correction_grid_resolution == 0:
             raise RuntimeError("correction_grid_resolution=0: correction grids were not allocated.")
-        raise NotImplementedError("the COMSOL periodic correction is not part of this build")
+        self._corr, scalars = to_device(self._ctx, correction, L_sim, eta_sim,
+                                        max(self.correction_grid_resolution, 2))
+        self._tree.set_correction(self._corr)
+        self.__dict__.update(correction_fields(scalars))
 
     # -- build ----------------------------------------------------------------
     def build(self, positions, radii, L: float, periodic: bool = False):

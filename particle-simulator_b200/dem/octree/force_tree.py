@@ -57,6 +57,8 @@ class TreeDropletForceCalculator(ForceCalculator):
                                      device=self._device)
             self._ctx = self.octree._ctx
             self.num_particles = n
+            if self._correction is not None:  # :103-106
+                self.octree.load_periodic_correction(self._correction, self._correction_L_sim, eta_sim=self.eta_oil)
 
     def load_periodic_correction(self, correction, L_sim: float):
         self._correction = correction

@@ -9,7 +9,8 @@ key prefixes, warp-cooperative FP32 walks with FP64 separations.  ``mpl`` is
 the leaf size (droplets per leaf; default 16).  ``window_level`` (periodic
 boxes): cells larger than L / 2^window_level are opened unless they lie wholly
 inside the target's minimum-image window (0, the default: the reference's
-rule).  Results
+rule).  ``load_periodic_correction`` adds the periodic-image correction to
+the velocity walk (FP32 terms at leaf pairs and accepted nodes).  Results
 approximate the direct sums; the reference-parity FP64 tree is
 ``TreeDropletForceCalculator``.
 """
@@ -21,6 +22,7 @@ import numpy as np
 from .. import _native as N
 from .._io import Stager
 from ..force_calculator.force_calculator_base import ForceCalculator
+from ..periodic_correction.comsol_lattice_correction import correction_fields, to_device
 
 EPS0 = 8.85418781762039e-12  # force_tree.py:44
 
@@ -30,8 +32,6 @@ class MortonTreeForceCalculator(ForceCalculator):
                  eta_oil: float = 0.065, eta_water: float = 0.001, E: float = 3e5, L: float = 1.0,
                  periodic: bool = False, correction_grid_resolution: int = 0, *, window_level: int = 0,
                  device=None):
-        if correction_grid_resolution:
-            raise ValueError("the periodic Oseen correction is not available on the Morton tree")
         self.eps0 = EPS0
         self.eps_oil, self.eta_oil, self.eta_water, self.E = eps_oil, eta_oil, eta_water, E
         self.L = L
@@ -42,12 +42,23 @@ class MortonTreeForceCalculator(ForceCalculator):
         self.num_particles = num_particles
         self.theta = theta
         self.mpl = mpl
-        self.correction_grid_resolution = 0
+        self.correction_grid_resolution = correction_grid_resolution
         self._ctx = N.Context(max(num_particles, 1), device)
         self._io = Stager(self._ctx)
         self.window_level = window_level
         self.tree = N.MortonTree(self._ctx, max(num_particles, 1))
         self.tree.set_window(window_level)
+        self._corr = None
+        self.__dict__.update(correction_fields(None))
+
+    def load_periodic_correction(self, correction, L_sim: float):
+        """force_tree.py:108-112 (eta ratio from this calculator's eta_oil)."""
+        if self.correction_grid_resolution == 0:
+            raise RuntimeError("correction_grid_resolution=0: correction grids were not allocated.")
+        self._corr, scalars = to_device(self._ctx, correction, L_sim, self.eta_oil,
+                                        max(self.correction_grid_resolution, 2))
+        self.tree.set_correction(self._corr)
+        self.__dict__.update(correction_fields(scalars))
 
     def update_params(self, theta: float, mpl: int) -> None:
         self.theta = theta
@@ -58,6 +69,7 @@ class MortonTreeForceCalculator(ForceCalculator):
             self._ctx.reserve(n)
             self.tree = N.MortonTree(self._ctx, n)
             self.tree.set_window(self.window_level)
+            self.tree.set_correction(self._corr)
             self.num_particles = n
 
     def _box(self, L, periodic):

@@ -18,6 +18,10 @@ Cases (reference call in brackets):
   solver_*   Euler loop with merges [EulerDropletSolver.solve]
   tree_*     flat octree            [FlatOctree.build / compute_forces_and_stokeslet /
                                      compute_forces_and_total_velocity]
+  corr_*     periodic-image Oseen correction
+                                    [COMSOLLatticeCorrection (shipped data, small grid),
+                                     DirectDropletForceCalculator / FlatOctree with
+                                     load_periodic_correction]
 """
 
 from __future__ import annotations
@@ -49,7 +53,11 @@ def _import_reference(ref: Path):
     from dem.solution.droplet_solution import DropletSolution
     from dem.solver.euler_droplet_solver import EulerDropletSolver
 
+    from dem.periodic_correction.comsol_lattice_correction import COMSOLLatticeCorrection
+
     return dict(
+        Corr=COMSOLLatticeCorrection,
+        Ref=ref,
         Direct=DirectDropletForceCalculator,
         Hash=SpatialHashCollisionDetector,
         Tree=FlatOctree,
@@ -329,13 +337,107 @@ def gen_tree(R, out):
         print(f"{name}: nodes={t.node_count[None]} parents={t.parent_count[None]}")
 
 
+def _synthetic_correction(R, rng, n, L_comsol, Fz, eta):
+    """A COMSOLLatticeCorrection whose regular grid is a seeded smooth field with
+    no symmetry (exercises every corner weight, the clamping and the permuted
+    lookups); built around the reference's own evaluate()."""
+    c = object.__new__(R["Corr"])
+    c.L_comsol, c.Fz_comsol, c.eta_comsol, c.grid_resolution = L_comsol, Fz, eta, n
+    c.grid_coords = np.linspace(-L_comsol / 2, L_comsol / 2, n)
+    g = np.meshgrid(c.grid_coords, c.grid_coords, c.grid_coords, indexing="ij")
+    fields = []
+    for k in range(3):
+        a = rng.normal(size=(4, 3))
+        f = sum(a[m, 0] * np.sin((m + 1) * 2.1 * g[0] / L_comsol + a[m, 1]) * np.cos((m + 2) * 1.7 * g[1] / L_comsol)
+                * np.cos(m * 2.9 * g[2] / L_comsol + a[m, 2]) for m in range(4))
+        fields.append(1e-9 * (f + 0.05 * rng.normal(size=f.shape)))
+    c.grid_u, c.grid_v, c.grid_w = fields
+    c._interp_u, c._interp_v, c._interp_w = c._build_interpolators()
+    return c
+
+
+def gen_correction(R, out):
+    rng = np.random.default_rng(16)
+    data = Path(R["Ref"]) / "dem" / "periodic_correction" / "data"
+    import json
+
+    prm = json.loads((data / "comsol_params.json").read_text())
+    Fz = 4 * np.pi * prm["R"] ** 2 * prm["eps_0"] * prm["eps_r"] * prm["E0"] ** 2  # comsol_lattice_correction.py:46
+    with contextlib.redirect_stdout(io.StringIO()):
+        comsol = R["Corr"](data_path=str(data / prm["velocity_file"]), L_comsol=prm["L"], Fz_comsol=Fz,
+                           eta_comsol=prm["eta"], grid_resolution=12)
+    gd = comsol.get_grid_data()
+    probe = rng.uniform(-0.6, 0.6, (40, 3)) * prm["L"]  # some outside the cell (fill value 0)
+    probe_F = rng.normal(size=(40, 3)) * 1e-9
+    np.savez(out / "corr_grid_comsol_r12.npz", **{k: gd[k] for k in gd}, probe=probe, probe_F=probe_F,
+             eval_raw=comsol.evaluate(probe), eval_F=comsol.evaluate(probe, probe_F),
+             eval_origin=comsol.evaluate(np.zeros((1, 3))))
+    print(f"corr_grid_comsol_r12: |w|max={np.abs(gd['grid_w']).max():.3e}")
+    synth = _synthetic_correction(R, rng, 7, 2e-4, 3.3e-12, 0.05)
+
+    def save_grid(payload, c):
+        g = c.get_grid_data()
+        payload.update(grid_u=g["grid_u"], grid_v=g["grid_v"], grid_w=g["grid_w"], grid_min=g["grid_min"],
+                       grid_dx=g["grid_dx"], grid_resolution=g["grid_resolution"], L_comsol=g["L_comsol"],
+                       Fz_comsol=g["Fz_comsol"], eta_comsol=g["eta_comsol"])
+
+    # direct: shipped data (periodic) and the synthetic grid (periodic, open: clamped lookups)
+    pos, r, L = lognormal_box(rng, 64)
+    pos2, r2, L2 = lognormal_box(rng, 40, periodic=False)
+    for name, c, pos, r, L, mode in (("corr_direct_comsol_periodic_n64", comsol, pos, r, L, "periodic"),
+                                     ("corr_direct_synth_periodic_n64", synth, pos, r, L, "periodic"),
+                                     ("corr_direct_synth_open_n40", synth, pos2, r2, L2, "open")):
+        n = len(r)
+        fc = R["Direct"](num_particles=n, L=L, boundary_mode=mode, correction_grid_resolution=c.grid_resolution,
+                         **PHYS)
+        with contextlib.redirect_stdout(io.StringIO()):
+            fc.load_periodic_correction(c, L_sim=L)
+        F, V = fc.calculate_forces_and_convection(pos, r)
+        payload = dict(positions=pos, radii=r, L=L, periodic=int(mode == "periodic"), m_const=fc.m_const,
+                       eta_const=fc.eta_const, eta_oil=fc.eta_oil, forces=F, velocities=V,
+                       corr_self_coeff=fc.corr_self_coeff[None], corr_L_ratio=fc.corr_L_ratio[None],
+                       corr_eta_ratio=fc.corr_eta_ratio[None], corr_Fz_inv=fc.corr_Fz_inv[None])
+        save_grid(payload, c)
+        np.savez(out / f"{name}.npz", **payload)
+        print(f"{name}: n={n} |V|max={np.abs(V).max():.3e} self={fc.corr_self_coeff[None]:.3e}")
+
+    # tree: Stokeslet and total-velocity walks with the correction at leaf pairs and accepted nodes
+    m_const = 12 * np.pi * 8.85418781762039e-12 * PHYS["eps_oil"] * PHYS["E"] ** 2
+    eta_const = 1 / (8 * np.pi * PHYS["eta_oil"])
+    sf = 2 * np.pi * PHYS["eta_oil"] * (2 * PHYS["eta_oil"] + 3 * PHYS["eta_water"]) / (
+        PHYS["eta_oil"] + PHYS["eta_water"]
+    )
+    pos, r, L = lognormal_box(rng, 120, phi=0.05)
+    for name, c, periodic, theta, mpl in (("corr_tree_comsol_periodic_mpl2_t05_n120", comsol, True, 0.5, 2),
+                                          ("corr_tree_synth_open_mpl1_t07_n120", synth, False, 0.7, 1)):
+        n = len(r)
+        t = R["Tree"](theta=theta, mpl=mpl, num_particles=n, correction_grid_resolution=c.grid_resolution)
+        t.load_periodic_correction(c, L, eta_sim=PHYS["eta_oil"])
+        t.build(pos, r, L, periodic)
+        F, V = t.compute_forces_and_stokeslet(m_const, eta_const)
+        F, V = F.copy(), V.copy()
+        t.build(pos, r, L, periodic)
+        F2, VT = t.compute_forces_and_total_velocity(m_const, eta_const, sf)
+        VT = VT.copy()
+        assert np.array_equal(F, F2)
+        payload = dict(positions=pos, radii=r, L=L, periodic=int(periodic), theta=theta, mpl=mpl, m_const=m_const,
+                       eta_const=eta_const, eta_oil=PHYS["eta_oil"], stokes_factor=sf, forces=F, velocities=V,
+                       total_velocities=VT, corr_self_coeff=t.corr_self_coeff[None],
+                       corr_L_ratio=t.corr_L_ratio[None], corr_eta_ratio=t.corr_eta_ratio[None],
+                       corr_Fz_inv=t.corr_Fz_inv[None])
+        save_grid(payload, c)
+        np.savez(out / f"{name}.npz", **payload)
+        print(f"{name}: nodes={t.node_count[None]} |V|max={np.abs(V).max():.3e}")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("DEM_REFERENCE", "/root/reference"))
     ap.add_argument("--only", default="")
     args = ap.parse_args()
     R = _import_reference(Path(args.reference))
-    gens = dict(direct=gen_direct, hash=gen_hash, merge=gen_merge, solver=gen_solver, tree=gen_tree)
+    gens = dict(direct=gen_direct, hash=gen_hash, merge=gen_merge, solver=gen_solver, tree=gen_tree,
+                correction=gen_correction)
     for k, g in gens.items():
         if args.only and k not in args.only.split(","):
             continue

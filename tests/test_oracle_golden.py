@@ -94,3 +94,37 @@ def test_physics_constants_match_reference_eps0():
     assert abs(m - 85.6184) < 1e-3
     assert abs(eta - 0.66315) < 1e-4
     assert abs(sf - 0.76016) < 1e-4
+
+
+CORR_DIRECT = sorted(p.name for p in GOLDEN.glob("corr_direct_*.npz"))
+CORR_TREE = sorted(p.name for p in GOLDEN.glob("corr_tree_*.npz"))
+
+
+@pytest.mark.parametrize("name", CORR_DIRECT)
+def test_direct_convection_with_correction_bit_exact(golden, name):
+    g = golden(name)
+    c = O.Correction.from_golden(g)
+    assert (c.Fz_inv, c.cL, c.eta_r) == (float(g["corr_Fz_inv"]), float(g["corr_L_ratio"]), float(g["corr_eta_ratio"]))
+    L, per = float(g["L"]), int(g["periodic"])
+    F = O.direct_forces(g["positions"], g["radii"], float(g["m_const"]), L, per)
+    V = O.direct_convection_corr(g["positions"], F, float(g["eta_const"]), L, per, c)
+    np.testing.assert_array_equal(F, g["forces"])
+    np.testing.assert_array_equal(V, g["velocities"])
+    # the correction is not negligible in these cases
+    V0 = O.direct_convection(g["positions"], F, float(g["eta_const"]), L, per)
+    assert np.linalg.norm(V - V0) > 1e-3 * np.linalg.norm(V)
+
+
+@pytest.mark.parametrize("name", CORR_TREE)
+def test_tree_velocity_with_correction_bit_exact(golden, name):
+    g = golden(name)
+    t = O.Tree(len(g["radii"]), float(g["theta"]), int(g["mpl"]))
+    t.set_correction(O.Correction.from_golden(g))
+    args = (g["positions"], g["radii"], float(g["L"]), bool(g["periodic"]))
+    t.build(*args)
+    F, V = t.forces_and_stokeslet(float(g["m_const"]), float(g["eta_const"]))
+    t.build(*args)
+    _, VT = t.forces_and_total_velocity(float(g["m_const"]), float(g["eta_const"]), float(g["stokes_factor"]))
+    np.testing.assert_array_equal(F, g["forces"])
+    np.testing.assert_array_equal(V, g["velocities"])
+    np.testing.assert_array_equal(VT, g["total_velocities"])
