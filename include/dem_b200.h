@@ -253,7 +253,7 @@ DEM_API int dem_direct_convection(dem_ctx *ctx, int n, const double *x, const do
  * load_periodic_correction:
  *   Fz_inv = 1 / Fz_comsol, L_ratio = L_comsol / L_sim,
  *   eta_ratio = eta_comsol / eta_sim, self_coeff = w(0,0,0) * Fz_inv * eta_ratio * L_ratio.
- * 2 <= n <= DEM_CORR_MAX_GRID.  Device memory: 288 (n-1)^3 bytes.
+ * 2 <= n <= DEM_CORR_MAX_GRID.  Device memory: 320 (n-1)^3 bytes.
  * Replaces the correction fields and load_periodic_correction of
  * dem/force_calculator/direct_droplet_force_calculator.py:56-120 and
  * dem/octree/flat_tree.py:125-167. */
@@ -265,6 +265,13 @@ DEM_API void dem_corr_destroy(dem_corr *corr);
 /* Host scalars: grid points per axis, the per-pair factor
  * Fz_inv * eta_ratio * L_ratio, the self coefficient (NULL skips). */
 DEM_API int dem_corr_info(const dem_corr *corr, int *n, double *common, double *self_coeff);
+
+/* Roofline probe of the FP32 correction pass (no counterpart in the
+ * reference): ctas x 256 threads each read per_thread cells of the FP32 table
+ * at pseudo-random positions, 96 bytes per cell in three 256-bit loads, and
+ * write one float each to out (device, ctas * 256 floats).  Time it on
+ * `stream` to get the table's random-gather bandwidth. */
+DEM_API int dem_corr_gather_probe(const dem_corr *corr, int ctas, int per_thread, float *out, void *stream);
 
 /* Oseen convection with the periodic-image correction: as
  * dem_direct_convection, plus for every pair j != i the correction of

@@ -3,8 +3,9 @@
 // walks take it in tree.cu and bh.cu).
 //
 // Direct FP32 pass: one thread per target i, j in shared-memory tiles split
-// over blockIdx.y; per pair three cell-block lookups (6 float4 each, L2/L1
-// resident: (n-1)^3 x 96 B) and 63 FMA of trilinear forms.  Runs of 32 terms
+// over blockIdx.y; per pair three cell lookups (three 256-bit loads each from
+// one 128-byte line; the table, (n-1)^3 x 128 B, stays in L2) and 63 FMA of
+// trilinear forms.  Runs of 32 terms
 // are summed in FP32 and added in FP64; the j-chunk partials are reduced in a
 // fixed order, so results are deterministic.
 //
@@ -145,6 +146,29 @@ int launch_corr_direct_fp32(dem_ctx *ctx, const dem_corr *c, int n, const double
     return dem_check_launch(ctx, "corr_direct_fp32");
 }
 
+// Roofline probe: every thread reads `per_thread` cells at pseudo-random
+// (xorshift) positions of the FP32 table, 96 bytes each (the three 256-bit
+// component loads of one lookup), and writes one sum.
+__global__ void corr_gather_probe_kernel(const float *__restrict__ c32, int cells, int per_thread,
+                                         float *__restrict__ out) {
+    const unsigned tid = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t h = tid * 2654435761u + 12345u;
+    float acc = 0.f;
+    for (int k = 0; k < per_thread; ++k) {
+        h ^= h << 13;
+        h ^= h >> 17;
+        h ^= h << 5;
+        const float *p = c32 + (size_t)(h % (uint32_t)cells) * CORR_CELL32;
+        float u[8], v[8], w[8];
+        corr_ld8(p, u);
+        corr_ld8(p + 8, v);
+        corr_ld8(p + 16, w);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) acc += u[q] + v[q] + w[q];
+    }
+    out[tid] = acc;
+}
+
 int launch_direct_convection_fp64_corr(dem_ctx *, const dem_corr *, int, const double *, const double *,
                                        const double *, const double *, const double *, const double *, double,
                                        double, int, double *, double *, double *, cudaStream_t);
@@ -159,7 +183,7 @@ static void build_cells(int n, const double *u, const double *v, const double *w
                         std::vector<float> &c32) {
     const size_t m = (size_t)n - 1;
     c64.assign(m * m * m * 24, 0.0);
-    c32.assign(m * m * m * 24, 0.f);
+    c32.assign(m * m * m * CORR_CELL32, 0.f);
     const double *g[3] = {u, v, w};
     for (size_t a = 0; a < m; ++a)
         for (size_t b = 0; b < m; ++b)
@@ -178,7 +202,7 @@ static void build_cells(int n, const double *u, const double *v, const double *w
                                  b2 = (k[6] - k[4]) - (k[2] - k[0]),
                                  b3 = ((k[7] - k[6]) - (k[5] - k[4])) - ((k[3] - k[2]) - (k[1] - k[0]));
                     const double coef[8] = {a0, a1, a2, a3, b0, b1, b2, b3};
-                    for (int q = 0; q < 8; ++q) c32[cell * 24 + comp * 8 + q] = (float)coef[q];
+                    for (int q = 0; q < 8; ++q) c32[cell * CORR_CELL32 + comp * 8 + q] = (float)coef[q];
                 }
             }
 }
@@ -242,6 +266,14 @@ int dem_corr_info(const dem_corr *c, int *n, double *common, double *self_coeff)
     if (common) *common = c->common;
     if (self_coeff) *self_coeff = c->g_self;
     return DEM_OK;
+}
+
+int dem_corr_gather_probe(const dem_corr *c, int ctas, int per_thread, float *out, void *stream) {
+    if (!c || !out || ctas < 1 || per_thread < 1) return DEM_E_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int m = c->n - 1;
+    dem::corr_gather_probe_kernel<<<ctas, 256, 0, counted(s)>>>(c->c32, m * m * m, per_thread, out);
+    return cudaGetLastError() == cudaSuccess ? DEM_OK : DEM_E_CUDA;
 }
 
 int dem_direct_convection_corr(dem_ctx *ctx, const dem_corr *corr, int n, const double *x, const double *y,

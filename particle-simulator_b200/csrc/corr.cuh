@@ -17,9 +17,10 @@
 // Device layout: cell-major.  Cell (a, b, c) of the (n-1)^3 cells holds what
 // one lookup needs, so a lookup reads one contiguous block:
 //   c64: 24 doubles  u[8] v[8] w[8]   corner values, corner k = (k>>2, (k>>1)&1, k&1)
-//   c32: 24 floats   u[8] v[8] w[8]   monomial coefficients of the same trilinear
-//        form (a0 a1 a2 a3 b0 b1 b2 b3, evaluated by corr_eval32), rounded once
-//        from FP64 differences
+//   c32: 32 floats   u[8] v[8] w[8] pad[8]   monomial coefficients of the same
+//        trilinear form (a0 a1 a2 a3 b0 b1 b2 b3, evaluated by corr_eval32),
+//        rounded once from FP64 differences; one 128-byte line per cell, one
+//        256-bit load per component
 // The FP64 functions restate the reference's expressions in its order and must
 // be compiled without multiply-add contraction (-fmad=false).
 #pragma once
@@ -30,7 +31,7 @@ struct dem_corr {
     dem_ctx *ctx = nullptr;
     int n = 0;                  // grid points per axis
     double2 *c64 = nullptr;     // (n-1)^3 cells x 12 double2
-    float4 *c32 = nullptr;      // (n-1)^3 cells x 6 float4
+    float *c32 = nullptr;       // (n-1)^3 cells x 32 floats (128-byte aligned)
     double gmin = 0, ginv = 0;  // first node, 1 / spacing
     double Fz_inv = 0, cL = 0, eta_r = 0;
     double common = 0;          // Fz_inv * eta_r * cL, the reference's per-pair factor
@@ -41,7 +42,7 @@ struct dem_corr {
 struct CorrDev {
     int n;
     const double2 *c64;
-    const float4 *c32;
+    const float *c32;
     double gmin, ginv, cL, common, g_self;
 };
 
@@ -114,8 +115,10 @@ __device__ __forceinline__ void corr_pair64(const CorrDev &c, double x, double y
 // ---- FP32 (mixed-precision passes and the Morton-tree walk) ------------------
 // Grid coordinate f = d * A + B of a separation d in the caller's frame
 // (A = scale * cL * ginv, B = -gmin * ginv), clamped like the reference.
+constexpr int CORR_CELL32 = 32;  // floats per cell in the FP32 table
+
 struct CorrF32 {
-    const float4 *c32;
+    const float *c32;
     int m;        // cells per axis (n - 1)
     float A, B;   // frame -> grid coordinate
     float fmax;   // n - 1
@@ -133,11 +136,19 @@ __device__ __forceinline__ void corr_axis32(const CorrF32 &c, float d, int &i, f
     t = f - (float)k;
 }
 
+// 32 contiguous bytes (32-byte aligned, read-only for the kernel's lifetime)
+// in one 256-bit load.
+__device__ __forceinline__ void corr_ld8(const float *p, float (&a)[8]) {
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(a[0]), "=f"(a[1]), "=f"(a[2]), "=f"(a[3]), "=f"(a[4]), "=f"(a[5]), "=f"(a[6]), "=f"(a[7])
+        : "l"(p));
+}
+
 // a0 + t3 a1 + t2 (a2 + t3 a3) + t1 (b0 + t3 b1 + t2 (b2 + t3 b3)): the trilinear
 // form, 7 FMA.
-__device__ __forceinline__ float corr_eval32(float4 a, float4 b, float t1, float t2, float t3) {
-    const float A = fmaf(t2, fmaf(t3, a.w, a.z), fmaf(t3, a.y, a.x));
-    const float B = fmaf(t2, fmaf(t3, b.w, b.z), fmaf(t3, b.y, b.x));
+__device__ __forceinline__ float corr_eval32(const float (&c)[8], float t1, float t2, float t3) {
+    const float A = fmaf(t2, fmaf(t3, c[3], c[2]), fmaf(t3, c[1], c[0]));
+    const float B = fmaf(t2, fmaf(t3, c[7], c[6]), fmaf(t3, c[5], c[4]));
     return fmaf(t1, B, A);
 }
 
@@ -151,22 +162,25 @@ __device__ __forceinline__ void corr_pair32(const CorrF32 &c, float dx, float dy
     corr_axis32(c, dy, ay, ty);
     corr_axis32(c, dz, az, tz);
     const int m = c.m;
-    const float4 *p1 = c.c32 + ((ax * m + ay) * m + az) * 6;  // G_z at (xc, yc, zc)
-    const float4 *p2 = c.c32 + ((az * m + ay) * m + ax) * 6;  // G_x at (zc, yc, xc)
-    const float4 *p3 = c.c32 + ((ax * m + az) * m + ay) * 6;  // G_y at (xc, zc, yc)
-    float4 q[18];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) {
-        q[k] = __ldg(p1 + k);
-        q[6 + k] = __ldg(p2 + k);
-        q[12 + k] = __ldg(p3 + k);
-    }
-    const float gz_x = corr_eval32(q[0], q[1], tx, ty, tz), gz_y = corr_eval32(q[2], q[3], tx, ty, tz),
-                gz_z = corr_eval32(q[4], q[5], tx, ty, tz);
-    const float gx_x = corr_eval32(q[10], q[11], tz, ty, tx), gx_y = corr_eval32(q[8], q[9], tz, ty, tx),
-                gx_z = corr_eval32(q[6], q[7], tz, ty, tx);
-    const float gy_x = corr_eval32(q[12], q[13], tx, tz, ty), gy_y = corr_eval32(q[16], q[17], tx, tz, ty),
-                gy_z = corr_eval32(q[14], q[15], tx, tz, ty);
+    const float *p1 = c.c32 + ((ax * m + ay) * m + az) * CORR_CELL32;  // G_z at (xc, yc, zc)
+    const float *p2 = c.c32 + ((az * m + ay) * m + ax) * CORR_CELL32;  // G_x at (zc, yc, xc)
+    const float *p3 = c.c32 + ((ax * m + az) * m + ay) * CORR_CELL32;  // G_y at (xc, zc, yc)
+    float u1[8], v1[8], w1[8], u2[8], v2[8], w2[8], u3[8], v3[8], w3[8];
+    corr_ld8(p1, u1);
+    corr_ld8(p1 + 8, v1);
+    corr_ld8(p1 + 16, w1);
+    corr_ld8(p2, u2);
+    corr_ld8(p2 + 8, v2);
+    corr_ld8(p2 + 16, w2);
+    corr_ld8(p3, u3);
+    corr_ld8(p3 + 8, v3);
+    corr_ld8(p3 + 16, w3);
+    const float gz_x = corr_eval32(u1, tx, ty, tz), gz_y = corr_eval32(v1, tx, ty, tz),
+                gz_z = corr_eval32(w1, tx, ty, tz);
+    const float gx_x = corr_eval32(w2, tz, ty, tx), gx_y = corr_eval32(v2, tz, ty, tx),
+                gx_z = corr_eval32(u2, tz, ty, tx);
+    const float gy_x = corr_eval32(u3, tx, tz, ty), gy_y = corr_eval32(w3, tx, tz, ty),
+                gy_z = corr_eval32(v3, tx, tz, ty);
     cx = fmaf(gx_x, sx, fmaf(gy_x, sy, fmaf(gz_x, sz, cx)));
     cy = fmaf(gx_y, sx, fmaf(gy_y, sy, fmaf(gz_y, sz, cy)));
     cz = fmaf(gx_z, sx, fmaf(gy_z, sy, fmaf(gz_z, sz, cz)));

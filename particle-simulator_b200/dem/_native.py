@@ -68,6 +68,7 @@ SIGNATURES = {
     "dem_corr_create": (_i, [_vp, _i, _vp, _vp, _vp, _d, _d, _d, _d, _d, _d, C.POINTER(_vp)]),
     "dem_corr_destroy": (None, [_vp]),
     "dem_corr_info": (_i, [_vp, C.POINTER(_i), C.POINTER(_d), C.POINTER(_d)]),
+    "dem_corr_gather_probe": (_i, [_vp, _i, _i, _vp, _vp]),
     "dem_direct_convection_corr": (_i, [_vp, _vp, _i] + [_vp] * 7 + [_d, _d, _i, _i, _vp, _vp, _vp, _vp]),
     "dem_batch_create": (_i, [_vp, _i, C.POINTER(_i64), C.POINTER(_d), _i, C.POINTER(_vp)]),
     "dem_batch_destroy": (None, [_vp]),
@@ -359,6 +360,11 @@ class Correction:
             except Exception:  # pragma: no cover
                 pass
             self.handle = None
+
+    def gather_probe(self, ctas, per_thread, out):
+        """Random 96-byte cell gathers from the FP32 table (see dem_corr_gather_probe)."""
+        self.ctx._check(lib().dem_corr_gather_probe(self.handle, int(ctas), int(per_thread), ptr(out),
+                                                    self.ctx.stream()), "corr_gather_probe")
 
     def info(self):
         n, c, g = _i(), _d(), _d()
