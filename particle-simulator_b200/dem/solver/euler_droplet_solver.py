@@ -15,8 +15,10 @@ When the force calculator and the detector are the B200 classes of this
 package, the state stays on the device for the whole run: detection, merge,
 both O(N^2) passes and the Euler update are CUDA kernels, and only the pair
 count (every step), the saved trajectory frames and the merged state cross
-PCIe.  Any other (duck-typed) calculator or detector runs the reference's host
-loop unchanged.
+PCIe.  Saved frames are copied on a separate stream into pinned host slots
+(``dem.solution.snapshot.SnapshotWriter``) while the next steps run, and are
+appended to the solution in order.  Any other (duck-typed) calculator or
+detector runs the reference's host loop unchanged.
 """
 
 from __future__ import annotations
@@ -25,12 +27,13 @@ import time
 
 import numpy as np
 
+from ..solution.snapshot import SnapshotWriter
 from .solver_base import Solver
 
 
 class EulerDropletSolver(Solver):
     def __init__(self, force_calculator, solution, post_processor, collision_detector=None, save_interval: int = 1,
-                 pbm_coupling=None, verbose: bool = True):
+                 pbm_coupling=None, verbose: bool = True, snapshot_depth: int = 4):
         self.force_calculator = force_calculator
         self.solution = solution
         self.post_processor = post_processor
@@ -43,6 +46,7 @@ class EulerDropletSolver(Solver):
         eta_water = self.force_calculator.eta_water
         self.stokes_factor = 2 * np.pi * eta_oil * (2 * eta_oil + 3 * eta_water) / (eta_oil + eta_water)  # :39-41
         self.steps_taken = 0
+        self.snapshot_depth = snapshot_depth  # frames in flight on the device path (0: copy synchronously)
 
     # ------------------------------------------------------------------
     def _device_capable(self) -> bool:
@@ -174,6 +178,14 @@ class EulerDropletSolver(Solver):
             torch.cuda.current_stream(dev).synchronize()
             return host_frame[:nn].numpy()
 
+        writer = SnapshotWriter(ctx, n, self.snapshot_depth) if self.snapshot_depth > 0 else None
+
+        def save(tt, nn):
+            if writer is None:
+                self.solution.save_step(tt, frame(nn))
+            else:
+                writer.push(self.solution, tt, pos_bufs[cur], nn)
+
         while (t < t_end) and not is_aborted:
             if self.post_processor.stop_simulation:
                 break
@@ -187,6 +199,8 @@ class EulerDropletSolver(Solver):
                 if det is not None and n > 0:
                     k, pairs, counts = det.detect_device(n, pos, r, L, periodic)
                     if k > 0:
+                        if writer is not None:
+                            writer.flush()  # this solution's frames first
                         pairs_host = pairs.cpu().numpy()
                         if self.pbm_coupling is not None:
                             self.pbm_coupling.on_collision(pairs_host, radii_host)
@@ -219,9 +233,13 @@ class EulerDropletSolver(Solver):
                 t += dt
                 self.steps_taken += 1
                 if self.save_interval <= 1 or step % self.save_interval == 0 or step == remaining_steps - 1:
-                    self.solution.save_step(t, frame(n))
+                    save(t, n)
                 if self.solution.should_update_visualization():
+                    if writer is not None:
+                        writer.flush()
                     self.post_processor.live_plot()
+        if writer is not None:
+            writer.flush()
         # the reference integrates in place into initial_droplet_state.positions
         if n > 0:
             self.solution.initial_droplet_state.positions[...] = frame(n)

@@ -28,7 +28,8 @@ class _Post:
         pass
 
 
-def _run(pos, r, L, dt, total_time, precision="fp64", eta_oil=ETA_OIL, eps_oil=2.85, eta_water=0.001, E=3e5):
+def _run(pos, r, L, dt, total_time, precision="fp64", eta_oil=ETA_OIL, eps_oil=2.85, eta_water=0.001, E=3e5,
+         snapshot_depth=4, save_interval=1, correction=None, host_loop=False):
     from dem.collision_detector import SpatialHashCollisionDetector
     from dem.force_calculator import DirectDropletForceCalculator
     from dem.particle_state import DropletState
@@ -37,11 +38,18 @@ def _run(pos, r, L, dt, total_time, precision="fp64", eta_oil=ETA_OIL, eps_oil=2
 
     n = len(r)
     fc = DirectDropletForceCalculator(num_particles=n, eps_oil=eps_oil, eta_oil=eta_oil, eta_water=eta_water, E=E,
-                                      L=L, boundary_mode="periodic", precision=precision)
+                                      L=L, boundary_mode="periodic", precision=precision,
+                                      correction_grid_resolution=0 if correction is None else correction.grid_resolution)
+    if correction is not None:
+        fc.load_periodic_correction(correction, L_sim=L)
     det = SpatialHashCollisionDetector(num_particles=n, L=L, boundary_mode="periodic")
     sol = DropletSolution(initial_droplet_state=DropletState(pos.copy(), r.copy(), time=0.0), length=4)
-    solver = EulerDropletSolver(fc, sol, _Post(), collision_detector=det, verbose=False)
-    solver.solve(dt, total_time)
+    solver = EulerDropletSolver(fc, sol, _Post(), collision_detector=det, verbose=False, save_interval=save_interval,
+                                snapshot_depth=snapshot_depth)
+    if host_loop:
+        solver._solve_host(dt, total_time)  # the reference's loop through the numpy API
+    else:
+        solver.solve(dt, total_time)
     chain = []
     s = solver.solution.get_first_solution()
     while s is not None:
@@ -86,3 +94,46 @@ def test_mixed_trajectory_tracks_fp64():
     d0 -= L * np.rint(d0 / L)
     dm -= L * np.rint(dm / L)
     assert np.linalg.norm(dm - d0) <= 1e-5 * np.linalg.norm(d0)
+
+
+def _same_chain(a, b):
+    assert len(a) == len(b)
+    for s, q in zip(a, b):
+        np.testing.assert_array_equal(s.radii, q.radii)
+        np.testing.assert_array_equal(s.get_times(), q.get_times())
+        np.testing.assert_array_equal(s.get_trajectories(), q.get_trajectories())
+        np.testing.assert_array_equal(np.asarray(s.collided_droplets).reshape(-1, 2),
+                                      np.asarray(q.collided_droplets).reshape(-1, 2))
+
+
+@pytest.mark.parametrize("save_interval", [1, 3])
+def test_snapshot_writer_frames_equal_synchronous_frames(golden, save_interval):
+    """Frames copied on the side stream (1 or 4 slots in flight) land in the same
+    solutions, in the same order, with the same values as synchronous copies,
+    across the six merges of the golden run."""
+    g = golden("solver_direct_periodic_n48.npz")
+    args = (g["positions"], g["radii"], float(g["L"]), float(g["dt"]), float(g["total_time"]))
+    kw = dict(eta_oil=float(g["eta_oil"]), eps_oil=float(g["eps_oil"]), eta_water=float(g["eta_water"]),
+              E=float(g["E"]), save_interval=save_interval)
+    _, sync = _run(*args, snapshot_depth=0, **kw)
+    for depth in (1, 4):
+        solver, chain = _run(*args, snapshot_depth=depth, **kw)
+        _same_chain(chain, sync)
+    assert len(sync) == int(g["n_solutions"])
+
+
+def test_solver_with_periodic_correction_matches_host_loop(golden):
+    """The device-resident loop with the periodic-image correction (FP64)
+    equals the reference's host loop driving the same calculator."""
+    from dem.periodic_correction import COMSOLLatticeCorrection
+
+    c = golden("corr_grid_comsol_r12.npz")
+    corr = COMSOLLatticeCorrection.from_grid(c["grid_u"], c["grid_v"], c["grid_w"], float(c["L_comsol"]),
+                                             float(c["Fz_comsol"]), float(c["eta_comsol"]))
+    pos, r, L = lognormal_state(600, seed=5)
+    dt = 1e-4
+    _, dev = _run(pos, r, L, dt, 9 * dt, correction=corr)
+    _, host = _run(pos, r, L, dt, 9 * dt, correction=corr, host_loop=True)
+    _same_chain(dev, host)
+    _, plain = _run(pos, r, L, dt, 9 * dt)
+    assert not np.array_equal(dev[-1].get_trajectories()[-1], plain[-1].get_trajectories()[-1])
