@@ -283,16 +283,29 @@ int run_sym_pass(dem_ctx *ctx, int n, int ipt, bool per, const MixedArgs &m, dou
                  double coeff, double *ox, double *oy, double *oz, cudaStream_t s);
 
 // Symmetric schedule: 0 when the split schedule is used, else the i-per-thread
-// blocking of the symmetric kernel.  Auto picks it when its partial sums (which
-// grow as N^2 / block^2) fit in SYM_BUDGET bytes.
+// blocking of the symmetric kernel.  Auto picks the largest blocking (4, then
+// 2 rows per thread, at most the tuned i_per_thread) that still gives every SM
+// several block pairs -- one CTA per block pair, nb (nb + 1) / 2 of them -- and
+// whose partial sums (N^2 / block^2 growth) fit in SYM_BUDGET bytes; with fewer
+// block pairs the split schedule, which evaluates every ordered pair but fills
+// the GPU, is faster.  Measured on B200 (force + convection pass, N = 1,000 ..
+// 65,536): split best to N = 4,096 (sym4 4.3x slower at N = 2,000), sym2 at
+// 8,192 - 12,288, sym4 from 16,384 on; the crossovers sit at ~3.5 block pairs
+// per SM.
 constexpr size_t SYM_BUDGET = size_t(4) << 30;
+static long long sym_block_pairs(int n, int ipt) {
+    const long long nb = (n + 128LL * ipt - 1) / (128LL * ipt);
+    return nb * (nb + 1) / 2;
+}
 static int symmetric_ipt(const dem_ctx *ctx, int n) {
     const int sched = ctx->tuning.schedule;
     if (sched == DEM_SCHED_SPLIT) return 0;
-    const int ipt = ctx->tuning.i_per_thread >= 4 ? 4 : 2;  // two i's per packed FP32x2 operation
-    if (sched == DEM_SCHED_SYMMETRIC) return ipt;
-    if (n < 256 || sym_partial_bytes(n, ipt) > SYM_BUDGET) return 0;
-    return ipt;
+    const int max_ipt = ctx->tuning.i_per_thread >= 4 ? 4 : 2;  // two i's per packed FP32x2 operation
+    if (sched == DEM_SCHED_SYMMETRIC) return max_ipt;
+    const long long enough = (long long)(3.5 * ctx->sm_count);
+    for (int ipt = max_ipt; ipt >= 2; ipt /= 2)
+        if (sym_block_pairs(n, ipt) >= enough && sym_partial_bytes(n, ipt) <= SYM_BUDGET) return ipt;
+    return 0;
 }
 
 // The plan the mixed passes would run for n droplets (no launch).

@@ -171,6 +171,10 @@ def test_plan_and_launch_counter():
     fc = _calc(1000, L, precision="mixed")
     assert fc._ctx.plan(65536)["schedule"] == "symmetric"
     assert fc._ctx.plan(100)["schedule"] == "split"  # auto: too small for block pairs
+    # auto keeps >= 3.5 block pairs per SM (148 SMs): split up to ~4k, 2 rows per thread, then 4
+    assert fc._ctx.plan(2000)["schedule"] == "split"
+    assert (fc._ctx.plan(8192)["schedule"], fc._ctx.plan(8192)["i_per_thread"]) == ("symmetric", 2)
+    assert (fc._ctx.plan(16384)["schedule"], fc._ctx.plan(16384)["i_per_thread"]) == ("symmetric", 4)
     fc.set_tuning(schedule="split")
     p = fc._ctx.plan(65536)
     assert p["schedule"] == "split" and p["j_splits"] >= 1 and p["ctas"] >= 148
