@@ -319,6 +319,18 @@ DEM_API int dem_hash_detect(dem_ctx *ctx, int n, const double *x, const double *
                     double L, int periodic, int table_size, int32_t *pairs, int64_t pair_capacity, int64_t *counts,
                     void *stream);
 
+/* Every pair with (minimum-image when periodic) distance <= r_i + r_j, with
+ * the same outputs as dem_hash_detect, but on a grid of whole cells
+ * (floor(L / 2 max r) cells of side L / grid), so that no touching pair
+ * across the periodic faces is skipped.  (dem_hash_detect keeps the
+ * reference's grid, ceil(L / 2 max r) cells with a partial last one.)  Used by
+ * the droplet generators' overlap rejection with radii inflated by half the
+ * minimum gap; L > 0 also in open boxes (positions in [0, L)).  No reference
+ * counterpart. */
+DEM_API int dem_overlap_pairs(dem_ctx *ctx, int n, const double *x, const double *y, const double *z,
+                              const double *r, double L, int periodic, int table_size, int32_t *pairs,
+                              int64_t pair_capacity, int64_t *counts, void *stream);
+
 /* Allocation-free spatial-hash detection.  This entry point has no
  * counterpart in the reference: it is for callers that cannot call
  * cudaMalloc when they detect collisions (a fixed device-memory budget handed
@@ -337,6 +349,30 @@ DEM_API int dem_hash_detect(dem_ctx *ctx, int n, const double *x, const double *
 DEM_API int dem_hash_detect_noalloc(int n, const double *x, const double *y, const double *z, const double *r,
                                     double L, int periodic, int table_size, int32_t *pairs, int64_t pair_capacity,
                                     int64_t *counts, void *stream);
+
+/* Collision counts between volume classes from detected pairs (dem_hash_detect
+ * output: pairs, counts[0]): matrix[b_i][b_j] += 1 and matrix[b_j][b_i] += 1 for
+ * each of the first min(counts[0], pair_capacity) pairs.  bins: device
+ * int32[n]; matrix: device uint32[nbins^2], zeroed here.
+ * Replaces DirectCollisionFrequency.compute, pbm/collision_frequency/direct_collision_freq.py:17-41. */
+DEM_API int dem_pair_bin_matrix(dem_ctx *ctx, const int32_t *pairs, const int64_t *num_pairs, int64_t pair_capacity,
+                                const int32_t *bins, int nbins, uint32_t *matrix, void *stream);
+
+/* ---- droplet generator ------------------------------------------------ */
+/* Seeded droplets with overlap rejection, written to DEVICE x, y, z, r:
+ * radii uniform in [rmin, rmax], positions uniform in [lo, hi)^3; then, round
+ * by round, the droplets just drawn that overlap any droplet (distance <=
+ * r_i + r_j + minimum_distance; minimum image when periodic, with period
+ * hi - lo) are drawn again, until none is left.  More than max_rounds rounds:
+ * DEM_E_INVALID (the reference raises ValueError after 1,000).  Random numbers
+ * are a counter-based SplitMix64 stream of (seed, purpose, round, droplet).
+ * *rounds_out (host, may be NULL): rounds used.  Synchronises `stream`.
+ * Replaces UniformDropletGenerator.generate / reseed_overlaping_droplets,
+ * dem/particle_generator/uniform_droplet_generator.py:45-164 (whose overlap
+ * test is the plain distance: periodic = 0). */
+DEM_API int dem_generate_droplets(dem_ctx *ctx, int n, unsigned long long seed, double lo, double hi, double rmin,
+                                  double rmax, double minimum_distance, int periodic, int max_rounds, double *x,
+                                  double *y, double *z, double *r, int *rounds_out, void *stream);
 
 /* ---- coalescence ------------------------------------------------------ */
 /* Greedy merge of the colliding pairs in (i, j) order; survivors keep their
@@ -395,6 +431,16 @@ DEM_API int dem_tree_velocity(dem_tree *tree, const double *fx, const double *fy
  * must outlive its use by the tree.
  * Replaces FlatOctree.load_periodic_correction, flat_tree.py:141-167. */
 DEM_API int dem_tree_set_correction(dem_tree *tree, const dem_corr *corr);
+
+/* Collision counts between volume classes over the built tree: every pair
+ * j > i with |MIC(x_j - x_i)|^2 <= (r_i + r_j)^2 adds 1 to matrix[b_i][b_j] and
+ * to matrix[b_j][b_i]; nodes are pruned when the squared distance to their box
+ * exceeds (r_i + max radius in the node)^2, with the reference's periodic box
+ * distance (per axis: gap > L/2 -> L - gap).  bins: device int32[n] class of
+ * each droplet (caller order), 0 <= b < nbins; matrix: device uint32[nbins^2],
+ * zeroed here.
+ * Replaces TreeCollisionFrequency.compute, pbm/collision_frequency/tree_collision_freq.py:43-175. */
+DEM_API int dem_tree_collision_matrix(dem_tree *tree, const int32_t *bins, int nbins, uint32_t *matrix, void *stream);
 
 /* Host int64[8]: node_count, parent_count, leaf_slot_count, max_nodes,
  * levels, num_particles, pool_exhausted, capacity. */

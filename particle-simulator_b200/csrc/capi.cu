@@ -19,7 +19,7 @@ int launch_euler_direct(dem_ctx *, int, const double *, const double *, const do
 int launch_euler_total(dem_ctx *, int, const double *, const double *, const double *, const double *, const double *,
                        const double *, double, double, int, double *, double *, double *, cudaStream_t);
 int launch_hash_detect(dem_ctx *, int, const double *, const double *, const double *, const double *, double, int,
-                       int, int32_t *, int64_t, int64_t *, cudaStream_t);
+                       int, int32_t *, int64_t, int64_t *, cudaStream_t, int);
 int launch_merge(dem_ctx *, int, const double *, const double *, const double *, const double *, const int32_t *,
                  const int64_t *, double *, double *, double *, double *, int32_t *, int32_t *, cudaStream_t);
 int launch_direct_vjp(dem_ctx *, int, const double *, const double *, const double *, const double *, const double *,
@@ -108,7 +108,21 @@ int dem_hash_detect(dem_ctx *ctx, int n, const double *x, const double *y, const
     if (!counts || (pair_capacity > 0 && !pairs) || pair_capacity < 0)
         return dem_set_error(ctx, DEM_E_INVALID, "bad pair buffer");
     return dem::launch_hash_detect(ctx, n, x, y, z, r, L, periodic, table_size, pairs, pair_capacity, counts,
-                                   (cudaStream_t)stream);
+                                   (cudaStream_t)stream, 0);
+}
+
+int dem_overlap_pairs(dem_ctx *ctx, int n, const double *x, const double *y, const double *z, const double *r,
+                      double L, int periodic, int table_size, int32_t *pairs, int64_t pair_capacity, int64_t *counts,
+                      void *stream) {
+    int rc = check_n(ctx, n);
+    if (rc) return rc;
+    if (!(L > 0)) return dem_set_error(ctx, DEM_E_INVALID, "L must be > 0");
+    if (table_size < 1 || (table_size & (table_size - 1)))
+        return dem_set_error(ctx, DEM_E_INVALID, "table_size must be a power of two");
+    if (!counts || (pair_capacity > 0 && !pairs) || pair_capacity < 0)
+        return dem_set_error(ctx, DEM_E_INVALID, "bad pair buffer");
+    return dem::launch_hash_detect(ctx, n, x, y, z, r, L, periodic, table_size, pairs, pair_capacity, counts,
+                                   (cudaStream_t)stream, 1);
 }
 
 int dem_merge(dem_ctx *ctx, int n, const double *x, const double *y, const double *z, const double *r,

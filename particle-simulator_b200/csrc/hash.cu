@@ -51,15 +51,23 @@ __global__ void max_kernel(int n, const double *__restrict__ r, unsigned long lo
     if ((threadIdx.x & 31) == 0) atomicMax(slot, m);
 }
 
-__global__ void hash_params_kernel(const unsigned long long *__restrict__ slot, double L, HashParams *__restrict__ hp) {
+// even_cells = 0: the reference's grid, cell = 2 max r and grid = ceil(L / cell)
+// (a periodic box whose side is not a whole number of cells gets a partial last
+// cell, across which touching pairs one cell apart are not compared -- the
+// reference's pair set, kept bit-exact).  even_cells = 1 (the generator's own
+// use): grid = floor(L / (2 max r)) whole cells of side L / grid >= 2 max r, so
+// every touching pair is compared across the periodic faces too.
+__global__ void hash_params_kernel(const unsigned long long *__restrict__ slot, double L, int even_cells,
+                                   HashParams *__restrict__ hp) {
     const double max_radius = from_ordered_bits(*slot);
-    const double cell = 2.0 * max_radius;  // :258
+    double cell = 2.0 * max_radius;  // :258
     HashParams p;
-    p.cell = cell;
     p.valid = cell > 0 ? 1 : 0;  // :259-260
-    double g = p.valid ? ceil(L / cell) : 1.0;
+    double g = p.valid ? (even_cells ? floor(L / cell) : ceil(L / cell)) : 1.0;
     if (!(g >= 1.0)) g = 1.0;
     if (g > 1073741824.0) g = 1073741824.0;
+    if (even_cells && p.valid) cell = L / g;
+    p.cell = cell;
     p.grid = (int32_t)g;  // :262
     *hp = p;
 }
@@ -260,9 +268,22 @@ __global__ void write_pairs_kernel(int n, const double *__restrict__ x, const do
     }
 }
 
+// DirectCollisionFrequency.compute, pbm/collision_frequency/direct_collision_freq.py:17-41, on the
+// detected pairs: matrix[b_i][b_j] += 1 and matrix[b_j][b_i] += 1 for every pair.
+__global__ void pair_bin_kernel(const int32_t *__restrict__ pairs, const int64_t *__restrict__ num_pairs,
+                                int64_t cap, const int32_t *__restrict__ bins, int nbins,
+                                unsigned int *__restrict__ matrix) {
+    const int64_t k = min(num_pairs[0], cap);
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < k; p += (int64_t)gridDim.x * blockDim.x) {
+        const int bi = bins[pairs[2 * p]], bj = bins[pairs[2 * p + 1]];
+        atomicAdd(&matrix[bi * nbins + bj], 1u);
+        atomicAdd(&matrix[bj * nbins + bi], 1u);
+    }
+}
+
 int launch_hash_detect(dem_ctx *ctx, int n, const double *x, const double *y, const double *z, const double *r,
                        double L, int periodic, int table_size, int32_t *pairs, int64_t cap, int64_t *counts,
-                       cudaStream_t s) {
+                       cudaStream_t s, int even_cells) {
     int rc = dem_ensure_table(ctx, table_size);
     if (rc) return rc;
     unsigned long long *slot = reinterpret_cast<unsigned long long *>(ctx->dscratch) + 2;
@@ -276,7 +297,7 @@ int launch_hash_detect(dem_ctx *ctx, int n, const double *x, const double *y, co
     if (n == 0) return DEM_OK;
     dem_prof_begin(ctx, "hash_detect", s);
     max_kernel<<<grid, 256, 0, counted(s)>>>(n, r, slot);
-    hash_params_kernel<<<1, 1, 0, counted(s)>>>(slot, L, hp);
+    hash_params_kernel<<<1, 1, 0, counted(s)>>>(slot, L, even_cells, hp);
     assign_kernel<<<grid, 256, 0, counted(s)>>>(n, x, y, z, hp, periodic, mask, ctx->cell_hash, ctx->bucket_count);
     rc = dem_check_launch(ctx, "hash assign");
     if (rc) return rc;
@@ -400,7 +421,7 @@ extern "C" int dem_hash_detect_noalloc(int n, const double *x, const double *y, 
     if (cudaMemsetAsync(bucket_count, 0, sizeof(int32_t) * table_size, s) != cudaSuccess) return DEM_E_CUDA;
     if (n == 0) return DEM_OK;
     max_kernel<<<grid, 256, 0, counted(s)>>>(n, r, slot);
-    hash_params_kernel<<<1, 1, 0, counted(s)>>>(slot, L, hp);
+    hash_params_kernel<<<1, 1, 0, counted(s)>>>(slot, L, 0, hp);
     assign_kernel<<<grid, 256, 0, counted(s)>>>(n, x, y, z, hp, periodic, mask, cell_hash, bucket_count);
     if (cudaGetLastError() != cudaSuccess) return DEM_E_CUDA;
     if (exclusive_scan_into<int32_t, int32_t>(bucket_count, bucket_start, table_size, static_cast<int32_t *>(sums),
@@ -420,4 +441,16 @@ extern "C" int dem_hash_detect_noalloc(int n, const double *x, const double *y, 
     write_pairs_kernel<<<dgrid, 128, 0, counted(s)>>>(n, x, y, z, r, hp, periodic, L, mask, bucket_start, sorted_idx,
                                              pair_offset, pairs, pair_capacity, counts, err);
     return cudaGetLastError() == cudaSuccess ? DEM_OK : DEM_E_CUDA;
+}
+
+extern "C" int dem_pair_bin_matrix(dem_ctx *ctx, const int32_t *pairs, const int64_t *num_pairs, int64_t pair_capacity,
+                                   const int32_t *bins, int nbins, uint32_t *matrix, void *stream) {
+    if (!ctx || nbins < 1 || !matrix || !num_pairs || pair_capacity < 0) return DEM_E_INVALID;
+    if (pair_capacity > 0 && (!pairs || !bins)) return DEM_E_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    int rc = dem_check_cuda(ctx, cudaMemsetAsync(matrix, 0, sizeof(uint32_t) * nbins * nbins, s), "memset");
+    if (rc || pair_capacity == 0) return rc;
+    const int grid = (int)std::min<int64_t>((pair_capacity + 255) / 256, 8LL * ctx->sm_count);
+    dem::pair_bin_kernel<<<grid, 256, 0, counted(s)>>>(pairs, num_pairs, pair_capacity, bins, nbins, matrix);
+    return dem_check_launch(ctx, "pair bin matrix");
 }

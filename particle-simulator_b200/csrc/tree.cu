@@ -597,6 +597,74 @@ __global__ void __launch_bounds__(128) velocity_walk_kernel(TreeDev t, const dou
     }
 }
 
+// TreeCollisionFrequency._count_collisions, pbm/collision_frequency/tree_collision_freq.py:62-135:
+// every pair j > i with |MIC(x_j - x_i)|^2 <= (r_i + r_j)^2 adds 1 to matrix[b_i][b_j]
+// and to matrix[b_j][b_i]; a node is skipped when the squared distance from x_i to
+// its box exceeds (r_i + max radius in the node)^2, the box distance taken per
+// axis as the gap to the nearer face and, when periodic, replaced by L - gap
+// when the gap exceeds L/2 (:137-175), as the reference does.
+template <bool PER>
+__global__ void collision_walk_kernel(TreeDev t, const int32_t *__restrict__ bins, int nbins,
+                                      unsigned int *__restrict__ matrix) {
+    const int M = t.max_nodes, N = t.cap, n = t.n;
+    const double L = t.L, halfL = 0.5 * t.L;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double xi = t.p[i], yi = t.p[N + i], zi = t.p[2 * N + i], ri = t.p[3 * N + i];
+        const int bi = bins[i];
+        int node = 0, steps = 0;
+        while (node >= 0) {
+            if (++steps > t.node_count + 1) {
+                raise_device_error(t.err, DEM_DEVERR_NODE_OVERFLOW);
+                break;
+            }
+            const int cnt = t.count[node];
+            if (cnt == 0) {
+                node = t.next[node];
+                continue;
+            }
+            if (t.first_child[node] < 0) {
+                const int l0 = t.leaf_start[node];
+                for (int k = 0; k < cnt; ++k) {
+                    const int j = t.leaf_idx[l0 + k];
+                    if (j >= 0 && j > i) {
+                        double dx = t.p[j] - xi, dy = t.p[N + j] - yi, dz = t.p[2 * N + j] - zi;
+                        if (PER) {
+                            dx = mic64(dx, L, halfL);
+                            dy = mic64(dy, L, halfL);
+                            dz = mic64(dz, L, halfL);
+                        }
+                        const double dist_sq = dx * dx + dy * dy + dz * dz;
+                        const double contact = ri + t.p[3 * N + j];
+                        if (dist_sq <= contact * contact) {
+                            const int bj = bins[j];
+                            atomicAdd(&matrix[bi * nbins + bj], 1u);
+                            atomicAdd(&matrix[bj * nbins + bi], 1u);
+                        }
+                    }
+                }
+                node = t.next[node];
+                continue;
+            }
+            const double max_contact = ri + t.maxr[node];
+            double g[3];
+            const double p3[3] = {xi, yi, zi};
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                const double lo = t.mn[a * (size_t)M + node], hi = t.mx[a * (size_t)M + node];
+                double d = 0.0;
+                if (p3[a] < lo)
+                    d = lo - p3[a];
+                else if (p3[a] > hi)
+                    d = p3[a] - hi;
+                if (PER && L > 0.0 && d > halfL) d = L - d;
+                g[a] = d;
+            }
+            const double min_dist_sq = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
+            node = min_dist_sq > max_contact * max_contact ? t.next[node] : t.first_child[node];
+        }
+    }
+}
+
 __global__ void copy_nodes_kernel(TreeDev t, int nc, int32_t *count, int32_t *first_child, int32_t *next,
                                   int32_t *leaf_start, double *r3, double *fs) {
     const int M = t.max_nodes;
@@ -849,6 +917,21 @@ int dem_tree_nodes(dem_tree *t, int32_t *count, int32_t *first_child, int32_t *n
     copy_nodes_kernel<<<grid_for(t->ctx, nc), 256, 0, counted((cudaStream_t)stream)>>>(view(t), nc, count, first_child, next,
                                                                              leaf_start, r3, fs);
     return dem_check_launch(t->ctx, "tree nodes");
+}
+
+int dem_tree_collision_matrix(dem_tree *t, const int32_t *bins, int nbins, uint32_t *matrix, void *stream) {
+    if (!t || nbins < 1 || !matrix || (t->n > 0 && !bins)) return DEM_E_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    int rc = dem_check_cuda(t->ctx, cudaMemsetAsync(matrix, 0, sizeof(uint32_t) * nbins * nbins, s), "memset");
+    if (rc || t->n == 0) return rc;
+    const int grid = ceil_div(t->n, 128);
+    dem_prof_begin(t->ctx, "tree_collision_walk", s);
+    if (t->periodic)
+        collision_walk_kernel<true><<<grid, 128, 0, counted(s)>>>(view(t), bins, nbins, matrix);
+    else
+        collision_walk_kernel<false><<<grid, 128, 0, counted(s)>>>(view(t), bins, nbins, matrix);
+    dem_prof_end(t->ctx, s);
+    return dem_check_launch(t->ctx, "tree collision walk");
 }
 
 int dem_tree_leaf_indices(dem_tree *t, int32_t *out, void *stream) {

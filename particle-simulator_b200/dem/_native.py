@@ -90,6 +90,9 @@ SIGNATURES = {
     "dem_euler_update_total": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _d, _d, _i, _vp, _vp, _vp, _vp]),
     "dem_hash_detect": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _d, _i, _i, _vp, _i64, _vp, _vp]),
     "dem_hash_detect_noalloc": (_i, [_i, _vp, _vp, _vp, _vp, _d, _i, _i, _vp, _i64, _vp, _vp]),
+    "dem_overlap_pairs": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _d, _i, _i, _vp, _i64, _vp, _vp]),
+    "dem_generate_droplets": (_i, [_vp, _i, C.c_ulonglong, _d, _d, _d, _d, _d, _i, _i, _vp, _vp, _vp, _vp,
+                                   C.POINTER(_i), _vp]),
     "dem_merge": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "dem_tree_create": (_i, [_vp, _i, _i, C.POINTER(_vp)]),
     "dem_tree_destroy": (None, [_vp]),
@@ -99,6 +102,8 @@ SIGNATURES = {
     "dem_tree_velocity": (_i, [_vp, _vp, _vp, _vp, _d, _d, _d, _vp, _vp, _vp, _vp]),
     "dem_tree_stats": (_i, [_vp, C.POINTER(_i64)]),
     "dem_tree_set_correction": (_i, [_vp, _vp]),
+    "dem_tree_collision_matrix": (_i, [_vp, _vp, _i, _vp, _vp]),
+    "dem_pair_bin_matrix": (_i, [_vp, _vp, _vp, _i64, _vp, _i, _vp, _vp]),
     "dem_tree_nodes": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "dem_tree_leaf_indices": (_i, [_vp, _vp, _vp]),
 }
@@ -323,6 +328,29 @@ class Context:
             "hash_detect",
         )
 
+    def overlap_pairs(self, n, pos, r, L, periodic, table_size, pairs, capacity, counts):
+        self._check(
+            lib().dem_overlap_pairs(self.handle, n, ptr(pos[0]), ptr(pos[1]), ptr(pos[2]), ptr(r), float(L),
+                                    int(periodic), int(table_size), ptr(pairs), int(capacity), ptr(counts),
+                                    self.stream()),
+            "overlap_pairs",
+        )
+
+    def generate_droplets(self, n, seed, lo, hi, rmin, rmax, minimum_distance, periodic, max_rounds, pos, r):
+        rounds = _i(0)
+        self._check(
+            lib().dem_generate_droplets(self.handle, int(n), int(seed) & 0xFFFFFFFFFFFFFFFF, float(lo), float(hi),
+                                        float(rmin), float(rmax), float(minimum_distance), int(bool(periodic)),
+                                        int(max_rounds), ptr(pos[0]), ptr(pos[1]), ptr(pos[2]), ptr(r),
+                                        C.byref(rounds), self.stream()),
+            "generate_droplets",
+        )
+        return int(rounds.value)
+
+    def pair_bin_matrix(self, pairs, num_pairs, capacity, bins, nbins, out):
+        self._check(lib().dem_pair_bin_matrix(self.handle, ptr(pairs), ptr(num_pairs), int(capacity), ptr(bins),
+                                              int(nbins), ptr(out), self.stream()), "pair_bin_matrix")
+
     def merge(self, n, pos, r, pairs, num_pairs, out_pos, out_r, n_out, merged=None):
         self._check(
             lib().dem_merge(self.handle, n, ptr(pos[0]), ptr(pos[1]), ptr(pos[2]), ptr(r), ptr(pairs), ptr(num_pairs),
@@ -409,6 +437,10 @@ class Tree:
         self.ctx._check(lib().dem_tree_velocity(self.handle, *a, float(eta_const), float(theta_sq),
                                                 float(stokes_factor), ptr(out[0]), ptr(out[1]), ptr(out[2]),
                                                 self.ctx.stream()), "tree_velocity")
+
+    def collision_matrix(self, bins, nbins, out):
+        self.ctx._check(lib().dem_tree_collision_matrix(self.handle, ptr(bins), int(nbins), ptr(out),
+                                                        self.ctx.stream()), "tree_collision_matrix")
 
     def set_correction(self, corr: Correction | None):
         self._corr = corr  # the tree borrows the grid

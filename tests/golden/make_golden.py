@@ -18,6 +18,8 @@ Cases (reference call in brackets):
   solver_*   Euler loop with merges [EulerDropletSolver.solve]
   tree_*     flat octree            [FlatOctree.build / compute_forces_and_stokeslet /
                                      compute_forces_and_total_velocity]
+  collfreq_* collision matrices     [pbm TreeCollisionFrequency.compute on a FlatOctree,
+                                     DirectCollisionFrequency.compute, VolumeGrid.bin_indices]
   corr_*     periodic-image Oseen correction
                                     [COMSOLLatticeCorrection (shipped data, small grid),
                                      DirectDropletForceCalculator / FlatOctree with
@@ -430,6 +432,36 @@ def gen_correction(R, out):
         print(f"{name}: nodes={t.node_count[None]} |V|max={np.abs(V).max():.3e}")
 
 
+def gen_collfreq(R, out):
+    from pbm.collision_frequency import DirectCollisionFrequency, TreeCollisionFrequency
+    from pbm.volume_grid import VolumeGrid
+
+    rng = np.random.default_rng(17)
+    cases = []
+    # the reference's own test configurations (tests/pbm/collision_frequency/test_tree_collision_freq.py)
+    pos = np.array([[0.10, 0.10, 0.10], [0.12, 0.10, 0.10], [0.50, 0.50, 0.50], [0.80, 0.10, 0.10],
+                    [0.10, 0.80, 0.10], [0.10, 0.10, 0.80]])
+    cases.append(("collfreq_reftest_n6", pos, np.full(6, 0.025), 1.0, False, (0.01, 0.05, 4, "geometric"), 1))
+    pos = np.array([[0.01, 0.5, 0.5], [0.99, 0.5, 0.5]])
+    cases.append(("collfreq_periodic_n2", pos, np.full(2, 0.05), 1.0, True, (0.02, 0.1, 3, "geometric"), 1))
+    # dense boxes with many contacts, mixed sizes (some outside the grid: clamped bins)
+    pos, r = dense_box(rng, 400, 1e-3, 10e-6, 45e-6)
+    cases.append(("collfreq_dense_periodic_n400", pos, r, 1e-3, True, (12e-6, 40e-6, 6, "geometric"), 2))
+    cases.append(("collfreq_dense_open_n400", pos, r, 1e-3, False, (12e-6, 40e-6, 5, "linear"), 4))
+    for name, pos, r, L, periodic, (rmin, rmax, nb, spacing), mpl in cases:
+        n = len(r)
+        g = VolumeGrid.from_radii_range(rmin, rmax, nb, spacing)
+        tree = R["Tree"](theta=0.5, mpl=mpl, num_particles=n)
+        tree.build(pos, r, L, periodic)
+        M_tree = TreeCollisionFrequency(tree, g, max_particles=n).compute(pos, r)
+        M_direct = DirectCollisionFrequency(g).compute(pos, r, L=L, periodic=periodic)
+        bins = g.bin_indices((4.0 / 3.0) * np.pi * r**3)
+        np.savez(out / f"{name}.npz", positions=pos, radii=r, L=L, periodic=int(periodic), mpl=mpl, r_min=rmin,
+                 r_max=rmax, n_bins=nb, spacing=spacing, bins=bins.astype(np.int32), edges=g.edges,
+                 matrix_tree=M_tree, matrix_direct=M_direct)
+        print(f"{name}: pairs={int(M_tree.sum()) // 2} same_as_direct={np.array_equal(M_tree, M_direct)}")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("DEM_REFERENCE", "/root/reference"))
@@ -437,7 +469,7 @@ def main():
     args = ap.parse_args()
     R = _import_reference(Path(args.reference))
     gens = dict(direct=gen_direct, hash=gen_hash, merge=gen_merge, solver=gen_solver, tree=gen_tree,
-                correction=gen_correction)
+                correction=gen_correction, collfreq=gen_collfreq)
     for k, g in gens.items():
         if args.only and k not in args.only.split(","):
             continue

@@ -175,6 +175,13 @@ def loop_config(**kwargs):
     return None
 
 
+def ndrange(*dims):
+    """``for i, j in ti.ndrange(a, b)``: the index tuples in row-major order."""
+    import itertools
+
+    return itertools.product(*(range(d) if isinstance(d, int) else range(*d) for d in dims))
+
+
 def random(dtype=None):
     return float(np.random.random())
 
