@@ -57,10 +57,13 @@ def parse():
     ap.add_argument("--cpu-sample-seconds", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="direct", choices=["direct", "batched", "adjoint", "tree", "correction"],
+    ap.add_argument("--workload", default="direct",
+                    choices=["direct", "batched", "adjoint", "tree", "correction", "trajectory"],
                     help="direct: one box of --n droplets (default); batched: 64 boxes, N ~ U[1024, 32768] (seed 1); "
                          "adjoint: gradients through 200 steps at N = 16,384; tree: Barnes-Hut at N = 2^20; "
-                         "correction: Oseen convection with the periodic-image correction (48^3 grid) at --n")
+                         "correction: Oseen convection with the periodic-image correction (48^3 grid) at --n; "
+                         "trajectory: --traj-steps direct steps in FP64 and mixed from one state, compared")
+    ap.add_argument("--traj-steps", type=int, default=1000)
     ap.add_argument("--accuracy", action="store_true", help="tree: errors on 4,096 droplets against direct FP64 sums")
     ap.add_argument("--fd", type=int, default=0, help="adjoint: central-difference checks on this many coordinates")
     ap.add_argument("--boxes", type=int, default=64)
@@ -140,7 +143,7 @@ class ClockSampler:
 class DeviceStepper:
     """Device-resident direct DEM step through the library's C ABI."""
 
-    def __init__(self, pos, r, L, precision, device):
+    def __init__(self, pos, r, L, precision, device, track=False):
         import torch
 
         from dem.collision_detector import SpatialHashCollisionDetector
@@ -163,14 +166,29 @@ class DeviceStepper:
         self.n_out = torch.zeros(1, dtype=torch.int32, device=self.dev)
         self.merges = 0
         self.launches_per_step = None
+        # track: the detected pair sets per step and the droplets' original ids (merged droplets get new ids)
+        self.track = track
+        self.steps_done = 0
+        self.pair_log = []
+        self.ids = np.arange(n)
+        self.next_id = n
+        self.merged = torch.empty((max(n, 1), 2), dtype=torch.int32, device=self.dev) if track else None
 
     def step(self):
         n, pos, r = self.n, self.pos[self.cur], self.r[self.rc]
         k, pairs, counts = self.det.detect_device(n, pos, r, self.L, True)
         if k > 0:  # coalescence, then detect again at the same time (reference semantics)
             nxt = 1 - self.cur
-            self.ctx.merge(n, pos, r, pairs, counts, self.pos[nxt], self.r[1 - self.rc], self.n_out)
+            self.ctx.merge(n, pos, r, pairs, counts, self.pos[nxt], self.r[1 - self.rc], self.n_out, self.merged)
             self.n = int(self.n_out.item())
+            if self.track:
+                self.pair_log.append((self.steps_done, pairs.cpu().numpy().copy()))
+                m = self.merged[: n - self.n].cpu().numpy()
+                gone = np.zeros(n, dtype=bool)
+                gone[m.ravel()] = True
+                new = np.arange(self.next_id, self.next_id + len(m))
+                self.next_id += len(m)
+                self.ids = np.concatenate([self.ids[~gone], new])
             self.cur, self.rc = nxt, 1 - self.rc
             self.merges += 1
             return self.step()
@@ -178,6 +196,10 @@ class DeviceStepper:
         nxt = 1 - self.cur
         self.ctx.euler_update(n, pos, r, F, V, self.stokes, DT, self.L, True, self.pos[nxt])
         self.cur = nxt
+        self.steps_done += 1
+
+    def positions(self):
+        return self.pos[self.cur][:, : self.n].T.cpu().numpy()
 
 
 def flush_l2(buf):
@@ -840,6 +862,88 @@ def run_correction(args, device):
     return out
 
 
+def run_trajectory(args, device):
+    """Config 1's long run: --traj-steps direct steps (detection, coalescence,
+    forces, convection, Euler) from one seeded state, FP64 and mixed, with the
+    validated FP64 GPU path as the reference (bit-identical to the oracle per
+    step).  Compares the colliding-pair sets of every detection, the merge
+    counts, and the positions of the droplets that never merged."""
+    import torch
+
+    torch.cuda.set_device(device)
+    pos0, r0, L = make_state(args.n, args.seed)
+    K = args.traj_steps
+    runs = {}
+    for prec in ("fp64", "mixed"):
+        st = DeviceStepper(pos0, r0, L, prec, device, track=True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(K):
+            st.step()
+        torch.cuda.synchronize()
+        runs[prec] = dict(seconds=time.perf_counter() - t0, pos=st.positions(), ids=st.ids.copy(), n=st.n,
+                          merges=st.merges, pair_log=st.pair_log)
+    a, b = runs["fp64"], runs["mixed"]
+    same_pairs = len(a["pair_log"]) == len(b["pair_log"]) and all(
+        sa == sb and np.array_equal(pa, pb) for (sa, pa), (sb, pb) in zip(a["pair_log"], b["pair_log"]))
+    first_diff = None
+    for k, ((sa, pa), (sb, pb)) in enumerate(zip(a["pair_log"], b["pair_log"])):
+        if sa != sb or not np.array_equal(pa, pb):
+            first_diff = int(min(sa, sb))
+            break
+    # droplets present from the start in both runs
+    orig = np.intersect1d(a["ids"][a["ids"] < len(r0)], b["ids"][b["ids"] < len(r0)])
+    ia = {v: k for k, v in enumerate(a["ids"])}
+    ib = {v: k for k, v in enumerate(b["ids"])}
+    xa = a["pos"][[ia[v] for v in orig]]
+    xb = b["pos"][[ib[v] for v in orig]]
+    mic = lambda d: d - L * np.rint(d / L)  # noqa: E731
+    disp = mic(xa - pos0[orig])
+    err = mic(xb - xa)
+    return dict(n=len(r0), K=K, L=L, seconds={p: runs[p]["seconds"] for p in runs},
+                merges={p: runs[p]["merges"] for p in runs}, n_final={p: runs[p]["n"] for p in runs},
+                detections_with_pairs={p: len(runs[p]["pair_log"]) for p in runs},
+                pair_sets_identical=bool(same_pairs), first_differing_step=first_diff, compared=int(len(orig)),
+                disp_rms=float(np.sqrt((disp**2).sum(1).mean())),
+                rel_err_norm=float(np.linalg.norm(err) / np.linalg.norm(disp)),
+                max_err_over_rms_disp=float(np.sqrt((err**2).sum(1)).max() / np.sqrt((disp**2).sum(1).mean())))
+
+
+def report_trajectory(args, res):
+    K = res["K"]
+    sec = res["seconds"]
+    line = {
+        "metric": f"DEM direct steps/s over a {K}-step trajectory (N={res['n']}), mixed vs FP64 GPU",
+        "value": K / sec["mixed"],
+        "unit": "steps/s",
+        "n_gpus": 1,
+        "steps": K,
+        "warmup": 0,
+        "ms_per_step": 1000.0 * sec["mixed"] / K,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 pair terms (mixed) against f64",
+        "data": "synthetic (seeded lognormal droplets, 2% volume fraction)",
+        "config": {
+            "workload": "direct step with detection, coalescence and Euler update, wall clock over the whole run "
+                        "(host syncs for the pair count included); FP64 GPU as the reference trajectory",
+            "fp64_steps_per_s": K / sec["fp64"],
+            "speedup_mixed_over_fp64": sec["fp64"] / sec["mixed"],
+            "merges": res["merges"],
+            "detections_with_pairs": res["detections_with_pairs"],
+            "n_final": res["n_final"],
+            "pair_sets_identical_every_detection": res["pair_sets_identical"],
+            "first_differing_step": res["first_differing_step"],
+            "droplets_compared": res["compared"],
+            "rms_displacement_m": res["disp_rms"],
+            "position_error_rel_to_displacement_norm": res["rel_err_norm"],
+            "position_error_max_over_rms_displacement": res["max_err_over_rms_disp"],
+        },
+    }
+    print(json.dumps(line), flush=True)
+
+
 def report_correction(args, res):
     K = args.steps
     n = res["n"]
@@ -916,6 +1020,12 @@ def main():
     if args.workload == "tree":
         if rank == 0:
             report_tree(args, run_tree(args, device))
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+    if args.workload == "trajectory":
+        if rank == 0:
+            report_trajectory(args, run_trajectory(args, device))
         if world > 1:
             torch.distributed.destroy_process_group()
         return
