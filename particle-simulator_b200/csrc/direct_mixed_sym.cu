@@ -15,6 +15,8 @@
 //     component and half), so after 32 steps every sum is back with the lane
 //     owning j;
 //   * I == J: ordered pairs, i side only (every i != j pair seen from both ends);
+//     the j-side sums run there too and are dropped, which keeps the inner
+//     loop free of per-item branches (4 % on the convection pass);
 //   * near-contact pairs, i == j and pairs whose periodic image is ambiguous in
 //     FP32 are recomputed in FP64 with the reference formula; their j-side
 //     terms go to the slot of that j in shared memory (one slot per warp and j);
@@ -292,11 +294,10 @@ __global__ void __launch_bounds__(SYM_T, 4) mixed_sym_kernel(const SymArgs a) {
                                 ax[kp] = p_fma(wj, tx, ax[kp]);
                                 ay[kp] = p_fma(wj, ty, ay[kp]);
                                 az[kp] = p_fma(wj, tz, az[kp]);
-                                if (!diag) {  // force on j: r_i^3 P(-d) / r^7 = r_i^3 t
-                                    sx = p_fma(wi[kp], tx, sx);
-                                    sy = p_fma(wi[kp], ty, sy);
-                                    sz = p_fma(wi[kp], tz, sz);
-                                }
+                                // force on j: r_i^3 P(-d) / r^7 = r_i^3 t (diagonal items discard it)
+                                sx = p_fma(wi[kp], tx, sx);
+                                sy = p_fma(wi[kp], ty, sy);
+                                sz = p_fma(wi[kp], tz, sz);
                             } else {
                                 rinv.x = ea ? 0.f : rinv.x;
                                 rinv.y = eb ? 0.f : rinv.y;
@@ -306,7 +307,7 @@ __global__ void __launch_bounds__(SYM_T, 4) mixed_sym_kernel(const SymArgs a) {
                                 ax[kp] = p_fma(rinv, p_fma(dx, sc, fjx), ax[kp]);
                                 ay[kp] = p_fma(rinv, p_fma(dy, sc, fjy), ay[kp]);
                                 az[kp] = p_fma(rinv, p_fma(dz, sc, fjz), az[kp]);
-                                if (!diag) {  // velocity at j: the same (even) tensor applied to F_i
+                                {  // velocity at j: the same (even) tensor applied to F_i (diagonal: discarded)
                                     const float2 doti = p_fma(dx, fxi[kp], p_fma(dy, fyi[kp], p_mul(dz, fzi[kp])));
                                     const float2 sci = p_mul(doti, rinv2);
                                     sx = p_fma(rinv, p_fma(dx, sci, fxi[kp]), sx);
@@ -355,7 +356,7 @@ __global__ void __launch_bounds__(SYM_T, 4) mixed_sym_kernel(const SymArgs a) {
                                 }
                             }
                         }
-                        if (!diag) {  // pass the running j-side sum to lane - 1
+                        {  // pass the running j-side sum to lane - 1
                             const int src = (lane + 1) & 31;
                             sx.x = __shfl_sync(0xffffffffu, sx.x, src);
                             sx.y = __shfl_sync(0xffffffffu, sx.y, src);
