@@ -210,7 +210,9 @@ def run_ours(args, rank, world, device):
     import torch
 
     torch.cuda.set_device(device)
-    pos, r, L = make_state(args.n, args.seed + rank)
+    from dem.replicas import replica_seed
+
+    pos, r, L = make_state(args.n, replica_seed(args.seed, rank))
     n = len(r)
     st = DeviceStepper(pos, r, L, args.precision, device)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)  # > 126 MB L2
@@ -248,11 +250,12 @@ def run_ours(args, rank, world, device):
     st.ctx.profile(False)
     schedule = st.ctx.plan(n, True) if args.precision == "mixed" else "fp64"
     clocks = sampler.stop() if sampler else None
-    t = torch.tensor([total_ms], device=device)
+    from dem.replicas import job_time_ms
+
+    job_ms = job_time_ms(total_ms, device)
     if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         torch.distributed.barrier()
-    return dict(n=n, n_final=st.n, L=L, total_ms=float(t.item()), step_ms=step_ms, kern=kern, clocks=clocks,
+    return dict(n=n, n_final=st.n, L=L, total_ms=job_ms, step_ms=step_ms, kern=kern, clocks=clocks,
                 merges=st.merges, pos=pos, r=r, launches=launches, schedule=schedule)
 
 
@@ -393,7 +396,9 @@ def run_batched(args, rank, world, device):
     from dem.ensemble import DropletEnsemble
 
     torch.cuda.set_device(device)
-    states, Ls = make_ensemble_states(args.boxes, 1 + rank)
+    from dem.replicas import replica_seed
+
+    states, Ls = make_ensemble_states(args.boxes, replica_seed(1, rank))
     ens = DropletEnsemble(states, Ls, device=device, **PHYS)
     tune = ens.autotune(reps=2)
     K, W = args.steps, args.warmup
@@ -427,11 +432,10 @@ def run_batched(args, rank, world, device):
     s1.record(stream)
     torch.cuda.synchronize()
     seq_ms = s0.elapsed_time(s1) / ks
-    t = torch.tensor([ms], device=device)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    from dem.replicas import job_time_ms
+
     sizes = np.diff(ens.offsets)
-    return dict(ms=float(t.item()), seq_ms=seq_ms, tune=tune, launches=launches, clocks=clocks, sizes=sizes,
+    return dict(ms=job_time_ms(ms, device), seq_ms=seq_ms, tune=tune, launches=launches, clocks=clocks, sizes=sizes,
                 errors=ens.ctx.device_errors())
 
 
@@ -1055,7 +1059,9 @@ def main():
         return
     n = res["n"]
     K = args.steps
-    steps_per_s = K * world / (res["total_ms"] / 1000.0)
+    from dem.replicas import whole_job_rate
+
+    steps_per_s = whole_job_rate(K, world, res["total_ms"])
     pairs = n * (n - 1)
     clocks = res["clocks"] or {}
     # roofline of the dominant kernel
