@@ -77,6 +77,8 @@ struct dem_bh {
     int32_t *hist = nullptr;
     double *ps = nullptr;       // [4][capacity] sorted x, y, z, r
     double *fsort = nullptr;    // [3][capacity] forces in sorted order
+    float4 *loff = nullptr;     // [capacity] (x - c_leaf, y - c_leaf, z - c_leaf, r) / ell per sorted droplet
+    float4 *fs32 = nullptr;     // [capacity] sorted forces scaled by 2^-q (velocity walk)
     int32_t *bounds = nullptr;  // [9][max_nodes] child split points of the current level
     long long *bbox = nullptr;  // [6] min/max of an open box (order-preserving integers)
     double *geom = nullptr;     // [4] root cube origin x, y, z and side
@@ -477,6 +479,8 @@ struct BhWalk {
     const double *geom;                // root cube origin and side
     const unsigned long long *scales;  // [0] max r, [1] max |F|
     const double *fsort;               // forces in sorted order (velocity walk)
+    const float4 *loff;                // per sorted droplet: offset from its leaf's centre and radius, / ell
+    const float4 *fs32;                // per sorted droplet: force * 2^-q (velocity walk)
     float theta2;
     int window_level;
     double L, halfL;
@@ -509,6 +513,7 @@ __global__ void __launch_bounds__(BH_T) bh_walk_kernel(const BhWalk w, double co
     CorrF32 cf = w.corr;
     if (CORR) cf.A = (float)(w.corr_A / inv_ell);  // separations are in units of ell
     const float Ls = (float)(w.L * inv_ell), invLs = (float)(1.0 / (w.L * inv_ell));
+    const float edge = (float)(w.L * inv_ell * (0.5 - 1e-6));  // leaf pairs: FP32 separations err by < 1e-6 L
     const double gox = w.geom[0], goy = w.geom[1], goz = w.geom[2];
     unsigned long long pairs = 0, nodes = 0;
     const int warps = gridDim.x * (BH_T / 32);
@@ -521,6 +526,7 @@ __global__ void __launch_bounds__(BH_T) bh_walk_kernel(const BhWalk w, double co
         // target in the nodes' FP32 frame (node separations: FP32, ~1e-6 relative for any accepted node)
         const float xs = (float)((xi - gox) * inv_ell), ys = (float)((yi - goy) * inv_ell),
                     zs = (float)((zi - goz) * inv_ell);
+        const float ris = (float)(ri * inv_ell);
         float ax = 0.f, ay = 0.f, az = 0.f;
         float cx = 0.f, cy = 0.f, cz = 0.f;  // correction sums (CORR)
         int sp = 1;
@@ -604,27 +610,35 @@ __global__ void __launch_bounds__(BH_T) bh_walk_kernel(const BhWalk w, double co
             if (nch == 0) {  // leaf: exact pair terms (contact cut r^2 >= (r_i + r_j)^2)
                 const int s0 = w.nd.start[node];
                 if (valid) pairs += cnt;
+                // d = x_j - x_i = (x_j - c_leaf) + MIC(c_leaf - x_i): the first part stored per droplet in
+                // FP32, the second taken in FP64 once per leaf, so d carries ~1e-7 of |d|, not of |x|
+                const float lx = (float)(bh_mic<PER>(w.nd.cx[node] - xi, w.L, w.halfL) * inv_ell),
+                            ly = (float)(bh_mic<PER>(w.nd.cy[node] - yi, w.L, w.halfL) * inv_ell),
+                            lz = (float)(bh_mic<PER>(w.nd.cz[node] - zi, w.L, w.halfL) * inv_ell);
                 for (int k = 0; k < cnt; ++k) {
                     const int sj = s0 + k;
-                    const double xj = w.ps[sj], yj = w.ps[cap + sj], zj = w.ps[2 * (size_t)cap + sj],
-                                 rj = w.ps[3 * (size_t)cap + sj];
-                    const double ddx = bh_mic<PER>(xj - xi, w.L, w.halfL), ddy = bh_mic<PER>(yj - yi, w.L, w.halfL),
-                                 ddz = bh_mic<PER>(zj - zi, w.L, w.halfL);
-                    const double r2d = ddx * ddx + ddy * ddy + ddz * ddz, rs = ri + rj;
-                    if (!valid || sj == si || r2d < rs * rs) continue;
-                    const float dx = (float)(ddx * inv_ell), dy = (float)(ddy * inv_ell), dz = (float)(ddz * inv_ell);
-                    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                    const float4 o = w.loff[sj];
+                    float dx = o.x + lx, dy = o.y + ly, dz = o.z + lz;
+                    // within 1e-6 L of the image boundary (or past it: a leaf reaching across L/2 in a
+                    // shallow tree) the image and the separation come from the FP64 positions
+                    if (PER && fmaxf(fabsf(dx), fmaxf(fabsf(dy), fabsf(dz))) > edge) {
+                        dx = (float)(bh_mic<PER>(w.ps[sj] - xi, w.L, w.halfL) * inv_ell);
+                        dy = (float)(bh_mic<PER>(w.ps[cap + sj] - yi, w.L, w.halfL) * inv_ell);
+                        dz = (float)(bh_mic<PER>(w.ps[2 * (size_t)cap + sj] - zi, w.L, w.halfL) * inv_ell);
+                    }
+                    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz)), rs = ris + o.w;
+                    if (!valid || sj == si || r2 < rs * rs) continue;
                     const float rinv = rsqrtf(r2), rinv2 = rinv * rinv;
                     if (FORCE) {
-                        const float rjs = (float)(rj * inv_ell);
+                        const float rjs = o.w;
                         const float b = rjs * rjs * rjs * (rinv2 * rinv2) * (rinv2 * rinv);
                         const float ang = fmaf(4.f * dz, dz, -fmaf(dx, dx, dy * dy));
                         ax = fmaf(b * ang, dx, ax);
                         ay = fmaf(b * ang, dy, ay);
                         az = fmaf(b * fmaf(2.f * dz, dz, -3.f * fmaf(dx, dx, dy * dy)), dz, az);
                     } else {  // e = x_i - x_j = -d
-                        const float fx = (float)(w.fsort[sj] * fsc), fy = (float)(w.fsort[cap + sj] * fsc),
-                                    fz = (float)(w.fsort[2 * (size_t)cap + sj] * fsc);
+                        const float4 fj = w.fs32[sj];
+                        const float fx = fj.x, fy = fj.y, fz = fj.z;
                         const float ex = -dx, ey = -dy, ez = -dz;
                         const float dot = fmaf(ex, fx, fmaf(ey, fy, ez * fz));
                         ax = fmaf(rinv, fmaf(ex, dot * rinv2, fx), ax);
@@ -707,6 +721,30 @@ __global__ void forces_to_sorted_kernel(int n, int cap, const int32_t *__restric
 
 // node aggregates in walk units: centre and side / ell, r3 / ell^3, q / ell^5 (what = 0);
 // fs * 2^-q, dp * 2^-q / ell (what = 1)
+// Per sorted droplet: offset from the centre of its leaf and radius, in units of ell.
+__global__ void leaf_offsets_kernel(BhNodes nd, int nc, const double *__restrict__ ps, int cap,
+                                    const unsigned long long *__restrict__ scales, float4 *__restrict__ loff) {
+    const double inv_ell = pow2_inv_of(scales[0]);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nc; k += gridDim.x * blockDim.x) {
+        if (nd.nchild[k] != 0) continue;
+        const int s0 = nd.start[k], cnt = nd.count[k];
+        const double cx = nd.cx[k], cy = nd.cy[k], cz = nd.cz[k];
+        for (int j = s0; j < s0 + cnt; ++j)
+            loff[j] = make_float4((float)((ps[j] - cx) * inv_ell), (float)((ps[cap + j] - cy) * inv_ell),
+                                  (float)((ps[2 * (size_t)cap + j] - cz) * inv_ell),
+                                  (float)(ps[3 * (size_t)cap + j] * inv_ell));
+    }
+}
+
+// Sorted forces scaled by 2^-q (the velocity walk's unit), FP32.
+__global__ void scale_forces_kernel(int n, int cap, const double *__restrict__ fsort,
+                                    const unsigned long long *__restrict__ scales, float4 *__restrict__ fs32) {
+    const double fsc = pow2_inv_of(scales[1]);
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+        fs32[j] = make_float4((float)(fsort[j] * fsc), (float)(fsort[cap + j] * fsc),
+                              (float)(fsort[2 * (size_t)cap + j] * fsc), 0.f);
+}
+
 __global__ void scale_nodes_kernel(BhNodes nd, int nc, const unsigned long long *scales, const double *geom,
                                    int what) {
     const double inv_ell = pow2_inv_of(scales[0]);
@@ -788,7 +826,7 @@ static int bh_nodes_reserve(dem_bh *b, int m, int keep, cudaStream_t s) {
 static void bh_free(dem_bh *b) {
     cudaSetDevice(b->ctx->device);
     bh_free_nodes(b->nd);
-    void *ptrs[] = {b->keys[0], b->keys[1], b->idx[0],   b->idx[1], b->hist,    b->ps,  b->fsort,
+    void *ptrs[] = {b->keys[0], b->keys[1], b->idx[0],   b->idx[1], b->hist,    b->ps,  b->fsort, b->loff, b->fs32,
                     b->bounds,  b->bbox,    b->geom,     b->counters, b->scales, b->scan_in, b->coff};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -818,6 +856,7 @@ int dem_bh_create(dem_ctx *ctx, int capacity, dem_bh **out) {
         (rc = bh_alloc(ctx, &b->idx[0], n, "bh")) || (rc = bh_alloc(ctx, &b->idx[1], n, "bh")) ||
         (rc = bh_alloc(ctx, &b->hist, 2 * (256 * (size_t)tiles + 1), "bh")) ||
         (rc = bh_alloc(ctx, &b->ps, 4 * n, "bh")) || (rc = bh_alloc(ctx, &b->fsort, 3 * n, "bh")) ||
+        (rc = bh_alloc(ctx, &b->loff, n, "bh")) || (rc = bh_alloc(ctx, &b->fs32, n, "bh")) ||
         (rc = bh_alloc(ctx, &b->bbox, 6, "bh")) || (rc = bh_alloc(ctx, &b->geom, 4, "bh")) ||
         (rc = bh_alloc(ctx, &b->counters, 2, "bh")) || (rc = bh_alloc(ctx, &b->scales, 2, "bh")) ||
         (rc = bh_nodes_reserve(b, std::max(4096, capacity / 4), 0, nullptr))) {
@@ -912,6 +951,8 @@ int dem_bh_build(dem_bh *b, int n, const double *x, const double *y, const doubl
                                                                                        b->capacity, b->geom,
                                                                                        b->keys[0]);
     scale_nodes_kernel<<<grid_of(ctx, le), 256, 0, counted(s)>>>(b->nd, le, b->scales, b->geom, 0);
+    leaf_offsets_kernel<<<grid_of(ctx, le), 256, 0, counted(s)>>>(b->nd, le, b->ps, b->capacity, b->scales,
+                                                                   b->loff);
     dem_prof_end(ctx, s);
     return dem_check_launch(ctx, "bh build");
 }
@@ -927,6 +968,8 @@ static BhWalk walk_args(dem_bh *b, float theta) {
     w.geom = b->geom;
     w.scales = b->scales;
     w.fsort = b->fsort;
+    w.loff = b->loff;
+    w.fs32 = b->fs32;
     w.theta2 = theta * theta;
     w.window_level = b->window_level;
     w.L = b->L;
@@ -985,6 +1028,7 @@ int dem_bh_velocity(dem_bh *b, const double *fx, const double *fy, const double 
         node_force_kernel<false><<<grid_of(ctx, 32LL * (le - top)), 256, 0, counted(s)>>>(b->nd, top, le, b->ps,
                                                                                           b->fsort, b->capacity);
     scale_nodes_kernel<<<grid_of(ctx, le), 256, 0, counted(s)>>>(b->nd, le, b->scales, b->geom, 1);
+    scale_forces_kernel<<<grid_of(ctx, n), 256, 0, counted(s)>>>(n, b->capacity, b->fsort, b->scales, b->fs32);
     if ((rc = dem_check_cuda(ctx, cudaMemsetAsync(b->counters, 0, 2 * sizeof(unsigned long long), s), "memset")))
         return rc;
     const BhWalk w = walk_args(b, (float)theta);
