@@ -73,6 +73,9 @@ DEM_API const char *dem_version(void);
  * contexts and devices; host-side counter, no synchronisation).  The
  * difference across a region is the count of the library's launches in it. */
 DEM_API unsigned long long dem_launch_count(void);
+/* Adds k to that counter: kernels of this library replayed from a CUDA graph
+ * that the caller captured (a replay does not pass through the library). */
+DEM_API void dem_count_replayed_launches(unsigned long long k);
 
 /* Opt-in kernel timing: while enabled, CUDA events are recorded on the launch
  * stream around the main kernels ("mixed_force_pass", "mixed_convection_pass",

@@ -19,6 +19,8 @@ unsigned long long dem_launch_count(void) { return g_launches.load(std::memory_o
 // Kernels launched by a CUDA graph replay (they bypass counted()).
 void dem_count_launches(unsigned long long k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
 
+extern "C" void dem_count_replayed_launches(unsigned long long k) { dem_count_launches(k); }
+
 namespace dem {
 int direct_plan(const dem_ctx *ctx, int n, int periodic, int *schedule, int *i_per_thread, int *threads,
                 long long *ctas, int *j_splits);

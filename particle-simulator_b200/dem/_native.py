@@ -42,6 +42,7 @@ _i, _d, _vp, _i64 = C.c_int, C.c_double, C.c_void_p, C.c_int64
 SIGNATURES = {
     "dem_version": (C.c_char_p, []),
     "dem_launch_count": (C.c_ulonglong, []),
+    "dem_count_replayed_launches": (None, [C.c_ulonglong]),
     "dem_ctx_create": (_i, [_i, _i, C.POINTER(_vp)]),
     "dem_ctx_destroy": (None, [_vp]),
     "dem_ctx_reserve": (_i, [_vp, _i]),
@@ -146,6 +147,11 @@ def version() -> str:
 def launch_count() -> int:
     """Kernels launched by the library in this process so far (host counter)."""
     return int(lib().dem_launch_count())
+
+
+def count_replayed_launches(k: int) -> None:
+    """Credit the counter with k library kernels replayed from a captured CUDA graph."""
+    lib().dem_count_replayed_launches(int(k))
 
 
 def _torch():

@@ -71,6 +71,24 @@ class SpatialHashCollisionDetector(CollisionDetector):
             self._pairs = torch.empty((self._pair_capacity, 2), dtype=torch.int32, device=self._ctx.device)
         return k, self._pairs[:k], self._counts
 
+    def detect_launch(self, n, pos_soa, r, L, periodic):
+        """The detection kernels and an asynchronous copy of the pair count into
+        pinned host memory, without synchronising (capturable in a CUDA graph).
+        Read the result with ``detect_finish`` once the stream has synchronised."""
+        self._reserve(n)
+        self._ctx.hash_detect(n, pos_soa, r, L, periodic, self._hash_table_size, self._pairs, self._pair_capacity,
+                              self._counts)
+        self._counts_host.copy_(self._counts, non_blocking=True)
+
+    def detect_finish(self, n, pos_soa, r, L, periodic):
+        """(K, pairs, counts) of the last ``detect_launch``; on a pair-buffer
+        overflow the detection runs again with room for every pair (the buffer
+        is then a new allocation)."""
+        k = int(self._counts_host[0])
+        if k <= self._pair_capacity:
+            return k, self._pairs[:k], self._counts
+        return self.detect_device(n, pos_soa, r, L, periodic)
+
     def detect(self, positions, radii, *, L: float | None = None, boundary_mode: str | None = None):
         """(is_collision, pairs (K, 2) int32), spatial_hash_collision_detector.py:233-316."""
         use_L = L if L is not None else self._L

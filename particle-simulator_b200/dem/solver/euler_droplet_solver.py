@@ -15,7 +15,12 @@ When the force calculator and the detector are the B200 classes of this
 package, the state stays on the device for the whole run: detection, merge,
 both O(N^2) passes and the Euler update are CUDA kernels, and only the pair
 count (every step), the saved trajectory frames and the merged state cross
-PCIe.  Saved frames are copied on a separate stream into pinned host slots
+PCIe.  With the direct calculator a step runs speculatively: detection, forces,
+convection and the Euler update into the other position buffer are one CUDA
+graph (captured once per droplet count and replayed), followed by one read of
+the pair count; when pairs were found the new positions are dropped and the
+merge proceeds from the unchanged ones, as in the reference.  Saved
+frames are copied on a separate stream into pinned host slots
 (``dem.solution.snapshot.SnapshotWriter``) while the next steps run, and are
 appended to the solution in order.  Any other (duck-typed) calculator or
 detector runs the reference's host loop unchanged.
@@ -33,7 +38,7 @@ from .solver_base import Solver
 
 class EulerDropletSolver(Solver):
     def __init__(self, force_calculator, solution, post_processor, collision_detector=None, save_interval: int = 1,
-                 pbm_coupling=None, verbose: bool = True, snapshot_depth: int = 4):
+                 pbm_coupling=None, verbose: bool = True, snapshot_depth: int = 4, graphs: bool = True):
         self.force_calculator = force_calculator
         self.solution = solution
         self.post_processor = post_processor
@@ -47,6 +52,8 @@ class EulerDropletSolver(Solver):
         self.stokes_factor = 2 * np.pi * eta_oil * (2 * eta_oil + 3 * eta_water) / (eta_oil + eta_water)  # :39-41
         self.steps_taken = 0
         self.snapshot_depth = snapshot_depth  # frames in flight on the device path (0: copy synchronously)
+        self.graphs = graphs  # replay the direct step as a CUDA graph (device path, direct calculator)
+        self.graph_replays = 0
 
     # ------------------------------------------------------------------
     def _device_capable(self) -> bool:
@@ -180,6 +187,47 @@ class EulerDropletSolver(Solver):
 
         writer = SnapshotWriter(ctx, n, self.snapshot_depth) if self.snapshot_depth > 0 else None
 
+        from .. import _native as N
+
+        state = {"graphs": self.graphs and not tree}
+        graphs = {}  # (n, cur, rc, detect) -> (graph, kernels in it); a key is captured on its second use
+        seen = set()
+        speculative = det is not None and hasattr(det, "detect_launch") and hasattr(det, "_pairs")
+        pairs_ptr = [det._pairs.data_ptr() if speculative else 0]
+
+        def advance(n, cur, rc, detect=False):
+            """[detection of pos_bufs[cur] +] forces + convection + Euler from pos_bufs[cur]
+            into pos_bufs[1 - cur]."""
+            def body():
+                if detect:
+                    det.detect_launch(n, pos_bufs[cur], r_bufs[rc], L, periodic)
+                F, V = fc.forces_and_convection_soa(n, pos_bufs[cur], r_bufs[rc])
+                ctx.euler_update(n, pos_bufs[cur], r_bufs[rc], F, V, self.stokes_factor, dt, L, periodic,
+                                 pos_bufs[1 - cur])
+
+            key = (n, cur, rc, detect)
+            if not state["graphs"] or key not in seen:
+                seen.add(key)  # the first call runs eagerly: it sizes every buffer the capture reuses
+                body()
+                return
+            if key not in graphs:
+                g = torch.cuda.CUDAGraph()
+                c0 = N.launch_count()
+                try:
+                    with torch.cuda.graph(g, capture_error_mode="thread_local"):
+                        body()
+                except RuntimeError as e:  # a calculator whose calls cannot be captured: run eagerly
+                    state["graphs"] = False
+                    if self.verbose:
+                        print(f"CUDA graph capture unavailable ({e}); stepping without graphs")
+                    body()
+                    return
+                graphs[key] = (g, N.launch_count() - c0)
+            g, k = graphs[key]
+            g.replay()
+            N.count_replayed_launches(k)
+            self.graph_replays += 1
+
         def save(tt, nn):
             if writer is None:
                 self.solution.save_step(tt, frame(nn))
@@ -196,8 +244,19 @@ class EulerDropletSolver(Solver):
                     is_aborted = True
                     break
                 pos, r = pos_bufs[cur], r_bufs[rc]
+                stepped = False
                 if det is not None and n > 0:
-                    k, pairs, counts = det.detect_device(n, pos, r, L, periodic)
+                    if tree or not speculative:
+                        k, pairs, counts = det.detect_device(n, pos, r, L, periodic)
+                    else:  # detection and the step together; the step is kept when no pair was found
+                        advance(n, cur, rc, detect=True)
+                        torch.cuda.current_stream(dev).synchronize()
+                        k, pairs, counts = det.detect_finish(n, pos, r, L, periodic)
+                        if det._pairs.data_ptr() != pairs_ptr[0]:  # the pair buffer grew: recapture
+                            pairs_ptr[0] = det._pairs.data_ptr()
+                            graphs.clear()
+                            seen.clear()
+                        stepped = k == 0
                     if k > 0:
                         if writer is not None:
                             writer.flush()  # this solution's frames first
@@ -210,6 +269,8 @@ class EulerDropletSolver(Solver):
                         nxt = 1 - cur
                         ctx.merge(n, pos, r, pairs, counts, pos_bufs[nxt], r_bufs[1 - rc], n_out)
                         n = int(n_out.item())
+                        graphs.clear()  # captured for the old droplet count
+                        seen.clear()
                         cur, rc = nxt, 1 - rc
                         new_pos = frame(n).copy()
                         radii_host = r_bufs[rc][:n].cpu().numpy()
@@ -220,13 +281,12 @@ class EulerDropletSolver(Solver):
                             self.post_processor.update_live_plot()
                         break
                 nxt = 1 - cur
-                if n > 0:
+                if n > 0 and not stepped:
                     if tree:
                         V = fc.forces_and_total_velocity_soa(n, pos, r, self.stokes_factor)
                         ctx.euler_update_total(n, pos, V, dt, L, periodic, pos_bufs[nxt])
                     else:
-                        F, V = fc.forces_and_convection_soa(n, pos, r)
-                        ctx.euler_update(n, pos, r, F, V, self.stokes_factor, dt, L, periodic, pos_bufs[nxt])
+                        advance(n, cur, rc)
                 cur = nxt
                 if self.pbm_coupling is not None:
                     self.pbm_coupling.step(t + dt, radii_host, dt)
