@@ -120,8 +120,11 @@ DEM_API int dem_direct_plan(const dem_ctx *ctx, int n, int periodic, int *schedu
  * test s^2 < theta^2 D^2 (flat_tree.py:871), opened per warp of 32 spatially
  * adjacent targets, with monopole forces (:873-884), Stokeslet + dipole
  * velocities (:1215-1265) and exact leaf pairs with the contact cut
- * r^2 >= (r_i + r_j)^2 (:835); leaf separations in FP64, node separations
- * and all terms in FP32.  Results
+ * r^2 >= (r_i + r_j)^2 (:835).  A leaf pair's separation is the FP64
+ * minimum-image vector from the target to the leaf centre (once per leaf
+ * visit) plus the source's FP32 offset from that centre, recomputed in FP64
+ * when a component lies within 1e-6 L of L/2; node separations and all terms
+ * are FP32.  Results
  * approximate the direct sums; the FP64 reference-parity tree is dem_tree_*.
  * dem_bh_build synchronises `stream` once per tree level (level sizes). */
 typedef struct dem_bh dem_bh;

@@ -510,6 +510,9 @@ __global__ void __launch_bounds__(BH_T) bh_walk_kernel(const BhWalk w, double co
     const int n = w.n, cap = w.cap;
     const double inv_ell = pow2_inv_of(w.scales[0]);
     const double fsc = FORCE ? 1.0 : pow2_inv_of(w.scales[1]);
+    // the reference's skip thresholds in the walk's units; ell and 2^-q are powers of two, so
+    // scaling the threshold instead of each node's sum gives the same decisions, without divisions
+    const double r3_skip = 1e-30 * (inv_ell * inv_ell * inv_ell), f2_skip = 1e-60 * (fsc * fsc);
     CorrF32 cf = w.corr;
     if (CORR) cf.A = (float)(w.corr_A / inv_ell);  // separations are in units of ell
     const float Ls = (float)(w.L * inv_ell), invLs = (float)(1.0 / (w.L * inv_ell));
@@ -546,13 +549,13 @@ __global__ void __launch_bounds__(BH_T) bh_walk_kernel(const BhWalk w, double co
             float fnx = 0.f, fny = 0.f, fnz = 0.f, r3n = 0.f;
             if (FORCE) {
                 r3n = w.nd.r3[node];
-                if ((double)r3n / (inv_ell * inv_ell * inv_ell) < 1e-30) continue;  // :861
+                if ((double)r3n < r3_skip) continue;  // :861, R^3 sum < 1e-30 m^3
             } else {
                 fnx = w.nd.fs[3 * (size_t)node];
                 fny = w.nd.fs[3 * (size_t)node + 1];
                 fnz = w.nd.fs[3 * (size_t)node + 2];
-                const double fx = fnx / fsc, fy = fny / fsc, fz = fnz / fsc;
-                if (fx * fx + fy * fy + fz * fz < 1e-60) continue;  // :1155
+                const double fx = fnx, fy = fny, fz = fnz;  // force sums in units of 2^q newtons
+                if (fx * fx + fy * fy + fz * fz < f2_skip) continue;  // :1155, |F sum|^2 < 1e-60 N^2
             }
             const float4 cs = w.nd.cs[node];
             float dx = cs.x - xs, dy = cs.y - ys, dz = cs.z - zs;
