@@ -513,6 +513,9 @@ __global__ void __launch_bounds__(BH_T) bh_walk_kernel(const BhWalk w, double co
     // the reference's skip thresholds in the walk's units; ell and 2^-q are powers of two, so
     // scaling the threshold instead of each node's sum gives the same decisions, without divisions
     const double r3_skip = 1e-30 * (inv_ell * inv_ell * inv_ell), f2_skip = 1e-60 * (fsc * fsc);
+    // A force sum with a component above f_hi has |F|^2 > f2_skip in any rounding (the FP64 sum
+    // of squares is >= the largest square), so only sums below it take the FP64 test.
+    const float f_hi = nextafterf(__double2float_ru(sqrt(f2_skip)), INFINITY);
     CorrF32 cf = w.corr;
     if (CORR) cf.A = (float)(w.corr_A / inv_ell);  // separations are in units of ell
     const float Ls = (float)(w.L * inv_ell), invLs = (float)(1.0 / (w.L * inv_ell));
@@ -554,8 +557,10 @@ __global__ void __launch_bounds__(BH_T) bh_walk_kernel(const BhWalk w, double co
                 fnx = w.nd.fs[3 * (size_t)node];
                 fny = w.nd.fs[3 * (size_t)node + 1];
                 fnz = w.nd.fs[3 * (size_t)node + 2];
-                const double fx = fnx, fy = fny, fz = fnz;  // force sums in units of 2^q newtons
-                if (fx * fx + fy * fy + fz * fz < f2_skip) continue;  // :1155, |F sum|^2 < 1e-60 N^2
+                if (!(fmaxf(fabsf(fnx), fmaxf(fabsf(fny), fabsf(fnz))) > f_hi)) {
+                    const double fx = fnx, fy = fny, fz = fnz;  // force sums in units of 2^q newtons
+                    if (fx * fx + fy * fy + fz * fz < f2_skip) continue;  // :1155, |F sum|^2 < 1e-60 N^2
+                }
             }
             const float4 cs = w.nd.cs[node];
             float dx = cs.x - xs, dy = cs.y - ys, dz = cs.z - zs;
@@ -567,7 +572,7 @@ __global__ void __launch_bounds__(BH_T) bh_walk_kernel(const BhWalk w, double co
             const float D2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
             const float side = cs.w;
             bool accept = side * side < w.theta2 * D2 && D2 > 0.f;
-            if (PER && w.nd.level[node] < w.window_level) {
+            if (PER && w.window_level > 0 && w.nd.level[node] < w.window_level) {
                 // cells larger than L / 2^window_level: the whole cell inside the target's
                 // minimum-image window (else its droplets take different images)
                 const float hw = (float)(w.halfL * inv_ell) - side;
