@@ -56,10 +56,11 @@ struct BhNodes {
     int *start, *count, *first_child, *nchild, *level;
     double *cx, *cy, *cz;  // R^3-weighted centre
     float4 *cs;            // walk copy: centre relative to the root cube origin / ell, and side / ell
-    float *r3;             // R^3 sum
-    float *q;              // [M][6] second moment Q = sum r^3 (x - c)(x - c)^T: xx xy xz yy yz zz
-    float *fs;             // [M][3] sum of forces
-    float *dp;             // [M][9] dipole D_ab = sum (x_a - c_a) F_b
+    // walk records, one 16-byte-aligned group per node so that a visit issues vector loads:
+    float4 *qr;  // [M][2] second moment Q = sum r^3 (x - c)(x - c)^T and R^3 sum:
+                 //        (Qxx, Qxy, Qxz, Qyy), (Qyz, Qzz, R^3, 0)
+    float4 *fd;  // [M][3] force sum and dipole D_ab = sum (x_a - c_a) F_b (row a, column b):
+                 //        (Fx, Fy, Fz, D00), (D01, D02, D10, D11), (D12, D20, D21, D22)
 };
 
 }  // namespace dem
@@ -373,8 +374,7 @@ __global__ void node_r3_kernel(BhNodes nd, int a, int b, const double *__restric
         }
         if (lane == 0) {
             const double w = v[0];
-            nd.r3[k] = (float)w;
-            float *Q = nd.q + 6 * (size_t)k;
+            float Q[6];
             if (w > 0.0) {
                 const double mx = v[1] / w, my = v[2] / w, mz = v[3] / w;
                 nd.cx[k] = rx + mx;
@@ -396,6 +396,8 @@ __global__ void node_r3_kernel(BhNodes nd, int a, int b, const double *__restric
                 nd.cz[k] = oz + compact10(pre) * cell + side * 0.5;
                 for (int q = 0; q < 6; ++q) Q[q] = 0.f;
             }
+            nd.qr[2 * (size_t)k] = make_float4(Q[0], Q[1], Q[2], Q[3]);
+            nd.qr[2 * (size_t)k + 1] = make_float4(Q[4], Q[5], (float)w, 0.f);
         }
     }
 }
@@ -435,8 +437,9 @@ __global__ void node_force_kernel(BhNodes nd, int a, int b, const double *__rest
             __syncthreads();
         }
         if (lane == 0) {  // node-major: one node's aggregates are contiguous for the walk
-            for (int q = 0; q < 3; ++q) nd.fs[3 * (size_t)k + q] = (float)v[q];
-            for (int q = 0; q < 9; ++q) nd.dp[9 * (size_t)k + q] = (float)v[3 + q];
+            for (int q = 0; q < 3; ++q)  // v = (F, D row-major): the record's order
+                nd.fd[3 * (size_t)k + q] = make_float4((float)v[4 * q], (float)v[4 * q + 1], (float)v[4 * q + 2],
+                                                       (float)v[4 * q + 3]);
         }
     }
 }
@@ -446,12 +449,12 @@ __global__ void node_force_kernel(BhNodes nd, int a, int b, const double *__rest
 // ---------------------------------------------------------------------------
 // Scaled units in FP32: lengths / ell (ell = 2^e with 2^(e-1) <= max r), forces
 // * 2^-q (2^(q-1) <= max |F|).  Node aggregates are stored in these units:
-// r3 = R^3 / ell^3, fs = sum F 2^-q, dp = D 2^-q / ell.
+// R^3 / ell^3, Q / ell^5, sum F 2^-q, D 2^-q / ell.
 // (1/6) Q_ab d_a d_b d_c phi at x = D (see the file header); r7 = |x|^-7 etc.
-__device__ __forceinline__ void quad_force(float x, float y, float z, const float *__restrict__ Q, float rinv,
+__device__ __forceinline__ void quad_force(float x, float y, float z, const float4 qa, const float4 qb, float rinv,
                                            float rinv2, float &gx, float &gy, float &gz) {
     const float r7 = (rinv2 * rinv2) * (rinv2 * rinv), r9 = r7 * rinv2, r11 = r9 * rinv2;
-    const float qxx = Q[0], qxy = Q[1], qxz = Q[2], qyy = Q[3], qyz = Q[4], qzz = Q[5];
+    const float qxx = qa.x, qxy = qa.y, qxz = qa.z, qyy = qa.w, qyz = qb.x, qzz = qb.y;
     const float tr = qxx + qyy + qzz;
     const float Qx = fmaf(qxx, x, fmaf(qxy, y, qxz * z));
     const float Qy = fmaf(qxy, x, fmaf(qyy, y, qyz * z));
@@ -550,13 +553,16 @@ __global__ void __launch_bounds__(BH_T) bh_walk_kernel(const BhWalk w, double co
             const int cnt = w.nd.count[node];
             if (cnt == 0) continue;
             float fnx = 0.f, fny = 0.f, fnz = 0.f, r3n = 0.f;
+            float4 rec = make_float4(0.f, 0.f, 0.f, 0.f);  // qr[1] (force) or fd[0] (velocity)
             if (FORCE) {
-                r3n = w.nd.r3[node];
+                rec = w.nd.qr[2 * (size_t)node + 1];
+                r3n = rec.z;
                 if ((double)r3n < r3_skip) continue;  // :861, R^3 sum < 1e-30 m^3
             } else {
-                fnx = w.nd.fs[3 * (size_t)node];
-                fny = w.nd.fs[3 * (size_t)node + 1];
-                fnz = w.nd.fs[3 * (size_t)node + 2];
+                rec = w.nd.fd[3 * (size_t)node];
+                fnx = rec.x;
+                fny = rec.y;
+                fnz = rec.z;
                 if (!(fmaxf(fabsf(fnx), fmaxf(fabsf(fny), fabsf(fnz))) > f_hi)) {
                     const double fx = fnx, fy = fny, fz = fnz;  // force sums in units of 2^q newtons
                     if (fx * fx + fy * fy + fz * fz < f2_skip) continue;  // :1155, |F sum|^2 < 1e-60 N^2
@@ -589,14 +595,15 @@ __global__ void __launch_bounds__(BH_T) bh_walk_kernel(const BhWalk w, double co
                         ax = fmaf(b * ang, dx, ax);
                         ay = fmaf(b * ang, dy, ay);
                         az = fmaf(b * fmaf(2.f * dz, dz, -3.f * fmaf(dx, dx, dy * dy)), dz, az);
-                        quad_force(dx, dy, dz, w.nd.q + 6 * (size_t)node, rinv, rinv2, ax, ay, az);
+                        quad_force(dx, dy, dz, w.nd.qr[2 * (size_t)node], rec, rinv, rinv2, ax, ay, az);
                     } else {  // e = x_i - c = -D
                         const float ex = -dx, ey = -dy, ez = -dz;
                         const float dot = fmaf(ex, fnx, fmaf(ey, fny, ez * fnz));
                         ax = fmaf(rinv, fmaf(ex, dot * rinv2, fnx), ax);
                         ay = fmaf(rinv, fmaf(ey, dot * rinv2, fny), ay);
                         az = fmaf(rinv, fmaf(ez, dot * rinv2, fnz), az);
-                        const float *Dm = w.nd.dp + 9 * (size_t)node;  // D_ab, row a, column b
+                        const float4 d1 = w.nd.fd[3 * (size_t)node + 1], d2 = w.nd.fd[3 * (size_t)node + 2];
+                        const float Dm[9] = {rec.w, d1.x, d1.y, d1.z, d1.w, d2.x, d2.y, d2.z, d2.w};  // D_ab
                         const float Ux = Dm[0] * ex + Dm[3] * ey + Dm[6] * ez;  // D^T e
                         const float Uy = Dm[1] * ex + Dm[4] * ey + Dm[7] * ez;
                         const float Uz = Dm[2] * ex + Dm[5] * ey + Dm[8] * ez;
@@ -762,13 +769,14 @@ __global__ void scale_nodes_kernel(BhNodes nd, int nc, const unsigned long long 
             nd.cs[k] = make_float4((float)((nd.cx[k] - geom[0]) * inv_ell), (float)((nd.cy[k] - geom[1]) * inv_ell),
                                    (float)((nd.cz[k] - geom[2]) * inv_ell),
                                    (float)(ldexp(geom[3], -nd.level[k]) * inv_ell));
-            const double s3 = inv_ell * inv_ell * inv_ell;
-            nd.r3[k] = (float)((double)nd.r3[k] * s3);
-            for (int q = 0; q < 6; ++q) nd.q[6 * (size_t)k + q] = (float)((double)nd.q[6 * (size_t)k + q] * s3 * inv_ell * inv_ell);
+            const double s3 = inv_ell * inv_ell * inv_ell, s5 = s3 * inv_ell * inv_ell;
+            float *qr = reinterpret_cast<float *>(nd.qr + 2 * (size_t)k);  // Q[0..5], R^3
+            for (int q = 0; q < 6; ++q) qr[q] = (float)((double)qr[q] * s5);
+            qr[6] = (float)((double)qr[6] * s3);
         } else {
-            for (int q = 0; q < 3; ++q) nd.fs[3 * (size_t)k + q] = (float)((double)nd.fs[3 * (size_t)k + q] * fsc);
-            for (int q = 0; q < 9; ++q)
-                nd.dp[9 * (size_t)k + q] = (float)((double)nd.dp[9 * (size_t)k + q] * fsc * inv_ell);
+            float *fd = reinterpret_cast<float *>(nd.fd + 3 * (size_t)k);  // F[0..2], D[0..8]
+            for (int q = 0; q < 3; ++q) fd[q] = (float)((double)fd[q] * fsc);
+            for (int q = 3; q < 12; ++q) fd[q] = (float)((double)fd[q] * fsc * inv_ell);
         }
     }
 }
@@ -787,7 +795,7 @@ static int bh_alloc(dem_ctx *ctx, T **p, size_t count, const char *what) {
 
 static void bh_free_nodes(BhNodes &nd) {
     void *ptrs[] = {nd.start, nd.count, nd.first_child, nd.nchild, nd.level, nd.cx,
-                    nd.cy,    nd.cz,    nd.cs,          nd.r3,     nd.q,     nd.fs, nd.dp};
+                    nd.cy,    nd.cz,    nd.cs,          nd.qr,     nd.fd};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     nd = BhNodes{};
@@ -804,9 +812,8 @@ static int bh_nodes_reserve(dem_bh *b, int m, int keep, cudaStream_t s) {
         (rc = bh_alloc(ctx, &nn.level, m, "bh nodes")) || (rc = bh_alloc(ctx, &nn.cx, m, "bh nodes")) ||
         (rc = bh_alloc(ctx, &nn.cy, m, "bh nodes")) || (rc = bh_alloc(ctx, &nn.cz, m, "bh nodes")) ||
         (rc = bh_alloc(ctx, &nn.cs, m, "bh nodes")) ||
-        (rc = bh_alloc(ctx, &nn.r3, m, "bh nodes")) || (rc = bh_alloc(ctx, &nn.q, 6 * (size_t)m, "bh nodes")) ||
-        (rc = bh_alloc(ctx, &nn.fs, 3 * (size_t)m, "bh nodes")) ||
-        (rc = bh_alloc(ctx, &nn.dp, 9 * (size_t)m, "bh nodes"))) {
+        (rc = bh_alloc(ctx, &nn.qr, 2 * (size_t)m, "bh nodes")) ||
+        (rc = bh_alloc(ctx, &nn.fd, 3 * (size_t)m, "bh nodes"))) {
         bh_free_nodes(nn);
         return rc;
     }
