@@ -504,8 +504,11 @@ __device__ __forceinline__ double bh_mic(double d, double L, double halfL) {
 // else:  u_i = [F_i / (stokes r_i)] + eta (sum_leaf G(e) F_j + sum_nodes G(e) F_node + dipole), e = x_i - x_j
 // CORR (velocity): + the periodic-image correction of every leaf pair and
 // accepted node (FP32, summed apart) and, when stokes <= 0, the self term.
+// Resident CTAs per SM asked of the register allocator (72 / 78-80 / 96 registers, none
+// spilled): the force walk runs fastest at 6, the velocity walk at 7; the correction's extra
+// live values fit at 5.
 template <bool PER, bool FORCE, bool CORR = false>
-__global__ void __launch_bounds__(BH_T) bh_walk_kernel(const BhWalk w, double coeff, double stokes,
+__global__ void __launch_bounds__(BH_T, FORCE ? 6 : (CORR ? 5 : 7)) bh_walk_kernel(const BhWalk w, double coeff, double stokes,
                                                        double *__restrict__ ox, double *__restrict__ oy,
                                                        double *__restrict__ oz, double *__restrict__ fsort_out) {
     __shared__ int stack[BH_T / 32][BH_STACK];
