@@ -10,7 +10,8 @@
 //   2. bucket of every droplet, bucket counts (atomics)
 //   3. exclusive scan of the counts (bucket starts), scatter into buckets
 //   4. per droplet i: the distinct hash buckets of its 27 neighbour cells; count
-//      the j > i in them with MIC distance <= r_i + r_j
+//      the j > i in them with MIC distance <= r_i + r_j (threads take the
+//      droplets in bucket order, so the lanes of a warp share candidate lists)
 //   5. exclusive scan of the per-i counts -> pair offsets (lexicographic order)
 //   6. per droplet i: write its pairs, sort its j's ascending
 // The candidate set of a droplet is exactly the reference's (the same buckets,
@@ -112,6 +113,20 @@ __global__ void scatter_kernel(int n, const int32_t *__restrict__ cell_hash, con
     }
 }
 
+// The reference's contact test sqrt(d2) <= s (s = r_i + r_j, the root correctly
+// rounded), decided from d2 alone unless d2 lies within a relative 2^-45 of s^2.
+// With s2 = RN(s * s): d2 > s2 (1 + 2^-45) implies sqrt(d2) > s (1 + 2^-47), above
+// s + ulp(s) / 2, so the rounded root exceeds s; d2 <= s2 (1 - 2^-45) implies
+// d2 < s^2, so the rounded root is <= s.  Both need s > 0 and s2 normal and
+// finite (the relative bounds), else, and inside the band, the square root decides.
+__device__ __forceinline__ bool contact_rn(double d2, double s) {
+    const double s2 = s * s;
+    const bool normal = s > 0.0 && s2 >= 0x1p-960 && s2 <= 0x1p+960;
+    if (normal && d2 > s2 * (1.0 + 0x1p-45)) return false;
+    if (normal && d2 <= s2 * (1.0 - 0x1p-45)) return true;
+    return sqrt(d2) <= s;
+}
+
 // Visits every candidate j > i of droplet i (the distinct buckets of its 27
 // neighbour cells) and calls f(j, multiplicity) for those in contact.
 template <typename F>
@@ -131,8 +146,7 @@ __device__ __forceinline__ void for_each_contact(int i, const double *__restrict
             dy = mic64(dy, L, halfL);
             dz = mic64(dz, L, halfL);
         }
-        const double dist = sqrt(dx * dx + dy * dy + dz * dz);
-        if (dist <= ri + rj) f(j, m);
+        if (contact_rn(dx * dx + dy * dy + dz * dz, ri + rj)) f(j, m);  // dist <= r_i + r_j
     };
     // Neighbour cell c = 9 (di + 1) + 3 (dj + 1) + (dk + 1): its bucket, or -1 outside an open box.
     auto cell_hash = [&](int c) -> int32_t {
@@ -218,7 +232,8 @@ __global__ void count_pairs_kernel(int n, const double *__restrict__ x, const do
                                    int32_t *__restrict__ pair_count, unsigned long long *__restrict__ raw) {
     const HashParams p = *hp;
     unsigned long long local_raw = 0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const int i = p.valid ? sorted_idx[t] : t;  // bucket order (the buckets are filled when valid)
         int32_t c = 0;
         if (p.valid) {
             for_each_contact(i, x, y, z, r, p, periodic, L, 0.5 * L, mask, n, bstart, sorted_idx, [&](int32_t, int m) {
@@ -243,7 +258,8 @@ __global__ void write_pairs_kernel(int n, const double *__restrict__ x, const do
         if (p.valid && offset[n] > cap) raise_device_error(err, DEM_DEVERR_PAIR_OVERFLOW);
     }
     if (!p.valid) return;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const int i = sorted_idx[t];  // bucket order, as in count_pairs_kernel
         const int64_t o0 = offset[i], o1 = offset[i + 1];
         if (o1 == o0) continue;
         int64_t w = o0;
