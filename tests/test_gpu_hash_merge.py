@@ -65,6 +65,57 @@ def test_reference_detector_cases():
     assert hit is True and len(pairs) == len({tuple(sorted(p)) for p in pairs}) == 3
 
 
+def _boundary_pairs(periodic, seed):
+    """Pairs set a few ulps either side of contact: droplet 2k on a coarse
+    lattice (no contact between lattice sites), droplet 2k+1 at distance
+    (r_a + r_b)(1 + delta) along a random direction, |delta| <= 2^-44.  Sites
+    are L / 8 = 122 um apart (periodic images included) and a partner lies at
+    most 2 r_max = 31 um from its anchor, so only the constructed pairs can
+    touch.  L = 2^-10 m and r_max = 2^-16 m make the hash grid 32 whole cells,
+    so pairs across the periodic faces are compared too; the first lattice
+    layer of every axis sits within 1 um of the face, so about half of those
+    partners lie across it."""
+    rng = np.random.default_rng(seed)
+    L, m, rmax = 2.0**-10, 8, 2.0**-16
+    g = (np.arange(m) + (0.0 if periodic else 0.5)) * (L / m)
+    anchors = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    k = len(anchors)
+    if periodic:
+        anchors += rng.uniform(0, 1e-6, anchors.shape)
+    ra = rng.uniform(5e-6, rmax, k)
+    rb = rng.uniform(5e-6, rmax, k)
+    ra[0] = rmax
+    u = rng.normal(size=(k, 3))
+    u /= np.linalg.norm(u, axis=1)[:, None]
+    axis = rng.random(k) < 0.25  # some pairs along a coordinate axis
+    u[axis] = np.eye(3)[rng.integers(0, 3, axis.sum())] * rng.choice([-1.0, 1.0], (axis.sum(), 1))
+    # half within a few ulps (the square root decides), half near the edges of the
+    # 2^-45 band on d^2 (decided from d^2 alone)
+    delta = np.where(rng.random(k) < 0.5, rng.integers(-6, 7, k) * 2.0**-52,
+                     rng.choice([-1.0, 1.0], k) * 2.0 ** rng.uniform(-48, -44, k))
+    partners = anchors + u * ((ra + rb) * (1.0 + delta))[:, None]
+    pos = np.empty((2 * k, 3))
+    pos[0::2], pos[1::2] = anchors, partners
+    if periodic:
+        pos = np.mod(pos, L)
+    r = np.empty(2 * k)
+    r[0::2], r[1::2] = ra, rb
+    return pos, r, L, k
+
+
+@pytest.mark.parametrize("periodic", [True, False])
+def test_contact_boundary_pairs_bit_exact(periodic):
+    # the contact test sqrt(d2) <= r_i + r_j decided within a few ulps of equality
+    for seed in range(3):
+        pos, r, L, k = _boundary_pairs(periodic, seed)
+        det = _det(len(r), L, "periodic" if periodic else "open")
+        hit, pairs = det.detect(pos, r)
+        hit_ref, pairs_ref = O.hash_detect(pos, r, L, periodic, table_size=det._hash_table_size)
+        assert hit == hit_ref
+        np.testing.assert_array_equal(pairs, pairs_ref)
+        assert 0 < len(pairs_ref) < k  # both outcomes occur among the near-contact pairs
+
+
 def test_pair_buffer_grows_beyond_capacity():
     rng = np.random.default_rng(9)
     pos = rng.uniform(0, 1e-4, (300, 3))
