@@ -53,12 +53,18 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=65536)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--schedule", default="auto", choices=["auto", "split", "symmetric", "symmetric_plain"],
+                    help="mixed passes: auto (default), or force a schedule (symmetric_plain: blocks in the caller's "
+                         "droplet order)")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--cpu-sample-seconds", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true", help="direct: skip the FP64 GPU step and the error report")
+    ap.add_argument("--advance", type=int, default=500,
+                    help="direct: untimed steps before the warm-up, so that the timed steps include coalescence")
     ap.add_argument("--workload", default="direct",
-                    choices=["direct", "batched", "adjoint", "tree", "correction", "trajectory"],
+                    choices=["direct", "batched", "adjoint", "tree", "parity_tree", "correction", "trajectory"],
                     help="direct: one box of --n droplets (default); batched: 64 boxes, N ~ U[1024, 32768] (seed 1); "
                          "adjoint: gradients through 200 steps at N = 16,384; tree: Barnes-Hut at N = 2^20; "
                          "correction: Oseen convection with the periodic-image correction (48^3 grid) at --n; "
@@ -67,15 +73,40 @@ def parse():
     ap.add_argument("--accuracy", action="store_true", help="tree: errors on 4,096 droplets against direct FP64 sums")
     ap.add_argument("--fd", type=int, default=0, help="adjoint: central-difference checks on this many coordinates")
     ap.add_argument("--boxes", type=int, default=64)
+    ap.add_argument("--parity-n", default="", help="parity_tree: comma-separated droplet counts (default 100k,250k,500k)")
     return ap.parse_args()
 
 
-def make_state(n, seed):
+def make_state(n, seed, device="auto"):
+    """The seeded lognormal state.  ``device="host"`` runs the overlap search
+    with scipy and never loads the CUDA library (the reference arm); the GPU
+    search gives the same state."""
     from dem.particle_generator import LognormalDropletGenerator
 
-    g = LognormalDropletGenerator(n, seed=seed)
+    g = LognormalDropletGenerator(n, seed=seed, device=device)
     s = g.generate()
     return s.positions, s.radii, g.L
+
+
+def direct_workload(n):
+    """The workload string both arms print for the direct step."""
+    return (f"direct DEM step (hash detection + merge + dipole force + Oseen convection + Euler), N={n}, "
+            f"periodic, 2% volume fraction, dt=1e-4")
+
+
+def mapped_libraries():
+    """Shared objects under this repository that the process has mapped."""
+    root = str(ROOT)
+    seen = []
+    try:
+        with open("/proc/self/maps") as f:
+            for ln in f:
+                path = ln.split()[-1] if ln.strip() else ""
+                if path.startswith(root) and path.endswith(".so") and path not in seen:
+                    seen.append(path)
+    except OSError:
+        return None
+    return [str(Path(p).relative_to(ROOT)) for p in seen]
 
 
 # ---------------------------------------------------------------------------
@@ -143,7 +174,7 @@ class ClockSampler:
 class DeviceStepper:
     """Device-resident direct DEM step through the library's C ABI."""
 
-    def __init__(self, pos, r, L, precision, device, track=False):
+    def __init__(self, pos, r, L, precision, device, track=False, schedule="auto"):
         import torch
 
         from dem.collision_detector import SpatialHashCollisionDetector
@@ -155,6 +186,8 @@ class DeviceStepper:
                                                device=device, **PHYS)
         self.det = SpatialHashCollisionDetector(num_particles=n, L=L, boundary_mode="periodic", device=device)
         self.ctx = self.fc._ctx
+        if precision == "mixed" and schedule != "auto":
+            self.fc.set_tuning(schedule=schedule)
         self.L = L
         eta_o, eta_w = PHYS["eta_oil"], PHYS["eta_water"]
         self.stokes = 2 * np.pi * eta_o * (2 * eta_o + 3 * eta_w) / (eta_o + eta_w)
@@ -206,6 +239,52 @@ def flush_l2(buf):
     buf.fill_(1)
 
 
+def time_steps(st, steps, flush, stream):
+    """CUDA-event time of each of ``steps`` steps, L2 flushed before each one
+    (outside the events); returns (per-step ms, merges inside the window)."""
+    import torch
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    m0 = st.merges
+    torch.cuda.synchronize()
+    for k in range(steps):
+        flush_l2(flush)  # every step starts with a cold L2
+        ev[k][0].record(stream)
+        st.step()
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in ev], st.merges - m0
+
+
+def mixed_vs_fp64(st, device):
+    """Forces and convection of the mixed and the FP64 GPU passes on the
+    stepper's current state: norm-wise relative error and the reference's
+    per-droplet metric |d|/(|ref| + 0.01 mean|ref|) (benchmarks/test.py:63-77)."""
+    import torch
+
+    from dem.force_calculator import DirectDropletForceCalculator
+
+    n = st.n
+    pos, r = st.pos[st.cur], st.r[st.rc]
+    out = {}
+    for prec in ("fp64", "mixed"):
+        fc = DirectDropletForceCalculator(num_particles=n, L=st.L, boundary_mode="periodic", precision=prec,
+                                          device=device, **PHYS)
+        F, V = fc.forces_and_convection_soa(n, pos, r)
+        out[prec] = (F[:, :n].T.cpu().numpy().copy(), V[:, :n].T.cpu().numpy().copy())
+    torch.cuda.synchronize()
+
+    def errs(a, b):
+        d = np.linalg.norm(a - b, axis=1)
+        nb = np.linalg.norm(b, axis=1)
+        e = d / (nb + 0.01 * nb.mean())
+        return {"rel_norm": float(np.linalg.norm(a - b) / np.linalg.norm(b)), "ref_metric_mean": float(e.mean()),
+                "ref_metric_max": float(e.max())}
+
+    return {"forces": errs(out["mixed"][0], out["fp64"][0]), "convection": errs(out["mixed"][1], out["fp64"][1]),
+            "state": f"the state after the timed steps ({n} droplets)"}
+
+
 def run_ours(args, rank, world, device):
     import torch
 
@@ -214,8 +293,11 @@ def run_ours(args, rank, world, device):
 
     pos, r, L = make_state(args.n, replica_seed(args.seed, rank))
     n = len(r)
-    st = DeviceStepper(pos, r, L, args.precision, device)
+    st = DeviceStepper(pos, r, L, args.precision, device, schedule=args.schedule)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)  # > 126 MB L2
+    for _ in range(args.advance):  # untimed: the timed window lies where droplets have begun to coalesce
+        st.step()
+    merges_advance = st.merges
     for _ in range(args.warmup):
         st.step()
     torch.cuda.synchronize()
@@ -229,17 +311,10 @@ def run_ours(args, rank, world, device):
     from dem._native import launch_count
 
     stream = torch.cuda.current_stream()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     torch.cuda.synchronize()
     launches0 = launch_count()
-    for k in range(args.steps):
-        flush_l2(flush)  # outside the timed events: every step starts with a cold L2
-        ev[k][0].record(stream)
-        st.step()
-        ev[k][1].record(stream)
-    torch.cuda.synchronize()
+    step_ms, merges_timed = time_steps(st, args.steps, flush, stream)
     launches = launch_count() - launches0
-    step_ms = [a.elapsed_time(b) for a, b in ev]
     total_ms = float(sum(step_ms))
     kern = {}
     for name in ("mixed_force_pass", "mixed_convection_pass", "fp64_force_pass", "fp64_convection_pass",
@@ -248,15 +323,27 @@ def run_ours(args, rank, world, device):
         if cnt:
             kern[name] = (ms, cnt)
     st.ctx.profile(False)
-    schedule = st.ctx.plan(n, True) if args.precision == "mixed" else "fp64"
+    schedule = st.ctx.plan(st.n, True) if args.precision == "mixed" else "fp64"
     clocks = sampler.stop() if sampler else None
     from dem.replicas import job_time_ms
 
     job_ms = job_time_ms(total_ms, device)
     if world > 1:
         torch.distributed.barrier()
-    return dict(n=n, n_final=st.n, L=L, total_ms=job_ms, step_ms=step_ms, kern=kern, clocks=clocks,
-                merges=st.merges, pos=pos, r=r, launches=launches, schedule=schedule)
+    res = dict(n=n, n_final=st.n, L=L, total_ms=job_ms, step_ms=step_ms, kern=kern, clocks=clocks,
+               merges=st.merges, merges_advance=merges_advance, merges_timed=merges_timed, pos=pos, r=r,
+               launches=launches, schedule=schedule)
+    if args.precision == "mixed" and not args.no_fp64 and rank == 0:
+        # the second half of the metric: the plain FP64 GPU step from the same state, timed the same way,
+        # and the mixed passes' error against it on that state
+        res["accuracy"] = mixed_vs_fp64(st, device)
+        st64 = DeviceStepper(st.positions(), st.r[st.rc][: st.n].cpu().numpy(), L, "fp64", device)
+        for _ in range(2):
+            st64.step()
+        k64 = max(3, min(args.steps, 10))
+        ms64, m64 = time_steps(st64, k64, flush, stream)
+        res["fp64"] = dict(steps=k64, ms_per_step=float(np.mean(ms64)), merges=m64)
+    return res
 
 
 def run_e2e(args, device, steps, warmup):
@@ -339,35 +426,70 @@ def cpu_step_rate(pos, r, L, budget_s, threads=0):
                 pairs_per_s=n * (n - 1) / t_step)
 
 
+def cpu_full_step(pos, r, L, O, consts, table):
+    """One whole step of the reference's loop (euler_droplet_solver.py:97-139)
+    on the oracle kernels: detect, merge and detect again while pairs exist,
+    then forces, convection and the Euler update with the periodic wrap."""
+    m, eta, stokes = consts
+    merges = 0
+    while True:
+        hit, pairs = O.hash_detect(pos, r, L, True, table_size=table)
+        if not hit:
+            break
+        pos, r, _ = O.merge(pos, r, pairs)
+        merges += 1
+    F = O.direct_forces(pos, r, m, L, True)
+    V = O.direct_convection(pos, F, eta, L, True)
+    return O.euler_direct(pos, r, F, V, stokes, DT, L, True), r, merges
+
+
 def run_reference(args, rank, world):
+    """The reference's algorithm on the host cores: the C restatement of its
+    kernels (oracle/dem_oracle.c, all host threads), whole steps of the direct
+    loop on the same seeded state, timed one by one.  It loads no CUDA code of
+    this repository (the state comes from the host overlap search)."""
     if rank != 0:
         return
-    pos, r, L = make_state(args.n, args.seed)
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    pos, r, L = make_state(args.n, args.seed, device="host")
     n = len(r)
-    budget = max(1.0, min(args.cpu_sample_seconds, 120.0 / max(args.steps + args.warmup, 1)))
+    consts = O.physics_constants(**PHYS)
+    table = O.next_power_of_2(2 * n)
+    merges = 0
     for _ in range(args.warmup):
-        cpu_step_rate(pos, r, L, budget)
-    rates = [cpu_step_rate(pos, r, L, budget) for _ in range(args.steps)]
-    sps = float(np.median([x["steps_per_s"] for x in rates]))
+        pos, r, k = cpu_full_step(pos, r, L, O, consts, table)
+        merges += k
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        pos, r, k = cpu_full_step(pos, r, L, O, consts, table)
+        times.append(time.perf_counter() - t0)
+        merges += k
+    total = float(sum(times))
+    sps = args.steps / total
+    cores = O.max_threads()
     line = {
         "impl": "reference",
-        "metric": "DEM steps/s (direct, N=%d)" % n,
+        "metric": f"DEM steps/s (direct, N={n})",
         "value": sps,
         "unit": "steps/s",
         "n_gpus": args.gpus,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": 1000.0 / sps,
+        "ms_per_step": 1000.0 * total / args.steps,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
-        "data": "synthetic (seeded lognormal droplets)",
-        "config": {"workload": f"direct DEM step, N={n}, periodic, 2% volume fraction, dt=1e-4",
-                   "pairs_per_s": sps * n * (n - 1)},
-        "cpu_baseline": {"value": sps, "unit": "steps/s", "cores": rates[0]["cores"], "kind": "port",
-                         "sample": f"hash detection + Euler on all {n} droplets, both O(N^2) passes on "
-                                   f"{rates[0]['rows']} rows x {n} columns per step, extrapolated"},
+        "data": "synthetic (seeded lognormal droplets, 2% volume fraction)",
+        "config": {"workload": direct_workload(n), "precision": "fp64 (the reference's arithmetic)",
+                   "pairs_per_s": sps * n * (n - 1), "merges_in_timed_and_warmup": merges, "n_final": len(r),
+                   "in_tree_libraries_mapped": mapped_libraries()},
+        "cpu_baseline": {"value": sps, "unit": "steps/s", "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} whole steps (detection, merges, both O(N^2) passes over all {n} "
+                                   f"droplets, Euler) of the C restatement of the reference kernels"},
         "e2e": {"value": sps, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -749,6 +871,111 @@ def report_tree(args, res):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# the main_tree.py drop-in: the reference-parity FP64 octree, timed as the
+# reference's own benchmark times it (benchmarks/test.py)
+# ---------------------------------------------------------------------------
+PARITY_N = (100_000, 250_000, 500_000)
+PARITY_MPL = (1, 2, 4, 8, 16)
+PARITY_RADII = (2.5e-6, 7.5e-6)  # benchmarks/test.py:26
+PARITY_PHYS = dict(eps_oil=2.85, eta_oil=0.065, eta_water=0.001, E=3e5)  # benchmarks/test.py:29
+
+
+def parity_box_side(n, radii=PARITY_RADII, wvc=0.02):
+    """box_size_from_volume, benchmarks/test.py:79-88."""
+    return float(np.cbrt(np.pi * n * np.sum(radii) * np.sum(np.square(radii)) / (3 * wvc)))
+
+
+def run_parity_tree(args, device):
+    """TreeDropletForceCalculator (the reference-parity FP64 octree, the class
+    main_tree.py builds) at N = 100k / 250k / 500k, theta = 0.5, mpl 1 / 2 / 4 /
+    8 / 16.  One step = calculate(pos, r) + calculate_convection(pos, r, F)
+    through the numpy API with host arrays, each call building the tree, as
+    benchmarks/test.py:127-164 times it (mean of --steps calls after --warmup).
+    The state: uniform radii in [2.5, 7.5] um, box side from the volume
+    formula, open box, overlaps rejected with a 1 um gap (benchmarks/test.py:
+    104-118), seeded.  Velocity error: the reference's metric (:63-77) of the
+    total velocity F / (gamma r) + V against the FP64 direct sums."""
+    import torch
+
+    from dem.force_calculator import DirectDropletForceCalculator
+    from dem.octree import TreeDropletForceCalculator
+    from dem.particle_generator import UniformDropletGenerator
+
+    torch.cuda.set_device(device)
+    eta_o, eta_w = PARITY_PHYS["eta_oil"], PARITY_PHYS["eta_water"]
+    sf = 2 * np.pi * eta_o * (2 * eta_o + 3 * eta_w) / (eta_o + eta_w)
+    ns = [int(x) for x in args.parity_n.split(",")] if args.parity_n else list(PARITY_N)
+    rows = []
+    for n in ns:
+        L = parity_box_side(n)
+        st = UniformDropletGenerator(coord_range=(0, L), radii_range=PARITY_RADII, num_particles=n,
+                                     minimum_distance=1e-6, seed=args.seed, device=device).generate()
+        pos, rad = st.positions, st.radii
+        fd = DirectDropletForceCalculator(num_particles=n, L=L, boundary_mode="open", device=device, **PARITY_PHYS)
+        F_d, V_d = fd.calculate_forces_and_convection(pos, rad)
+        vt_d = V_d + F_d / (sf * rad[:, None])
+        tc = TreeDropletForceCalculator(num_particles=n, theta=0.5, mpl=1, periodic=False, **PARITY_PHYS)
+        for mpl in PARITY_MPL:
+            tc.update_params(0.5, mpl)
+
+            def step():
+                f = tc.calculate(pos, rad)
+                return f, tc.calculate_convection(pos, rad, f)
+
+            for _ in range(max(args.warmup, 1)):
+                step()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                f, v = step()
+            torch.cuda.synchronize()
+            ms = 1000.0 * (time.perf_counter() - t0) / args.steps
+            vt = v + f / (sf * rad[:, None])
+            dn = np.linalg.norm(vt - vt_d, axis=1)
+            nr = np.linalg.norm(vt_d, axis=1)
+            rel = dn / (nr + 0.01 * nr.mean())
+            stats = tc.octree.get_tree_stats() if hasattr(tc.octree, "get_tree_stats") else {}
+            rows.append(dict(n=n, theta=0.5, mpl=mpl, tree_ms=ms, mean_err_pct=100 * float(rel.mean()),
+                             max_err_pct=100 * float(rel.max()), nodes=stats.get("node_count")))
+    return rows
+
+
+# benchmarks/data.txt:116-119, 344-347, 572-575: the reference's Taichi CPU tree step (ms), i7-11800H, 16 threads
+PARITY_PUBLISHED_MS = {
+    (100_000, 1): 570.3, (100_000, 2): 460.8, (100_000, 4): 444.0, (100_000, 8): 566.6, (100_000, 16): 662.4,
+    (250_000, 1): 1702.7, (250_000, 2): 1597.4, (250_000, 4): 1571.4, (250_000, 8): 1984.0, (250_000, 16): 1944.8,
+    (500_000, 1): 5055.6, (500_000, 2): 4625.8, (500_000, 4): 4839.6, (500_000, 8): 7610.1, (500_000, 16): 8316.9,
+}
+
+
+def report_parity_tree(args, rows):
+    for row in rows:
+        pub = PARITY_PUBLISHED_MS.get((row["n"], row["mpl"]))
+        row["reference_published_ms"] = pub
+        row["vs_published"] = pub / row["tree_ms"] if pub else None
+    head = rows[0]
+    line = {
+        "metric": "DEM tree step ms (TreeDropletForceCalculator, theta=0.5)",
+        "value": head["tree_ms"],
+        "unit": "ms/step",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": head["tree_ms"],
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": head["vs_published"],
+        "dtype": "f64",
+        "data": "synthetic (seeded uniform radii 2.5-7.5 um, 2% water volume fraction, open box)",
+        "config": {"workload": "main_tree.py drop-in: calculate + calculate_convection of the reference-parity FP64 "
+                               "octree through the numpy API (host arrays, tree built per call), as "
+                               "benchmarks/test.py times it",
+                   "rows": rows},
+    }
+    print(json.dumps(line), flush=True)
+
+
 CORR_GRID = 48  # points per axis of the periodic-image correction grid (the shipped COMSOL grid's size)
 
 
@@ -1027,6 +1254,12 @@ def main():
         if world > 1:
             torch.distributed.destroy_process_group()
         return
+    if args.workload == "parity_tree":
+        if rank == 0:
+            report_parity_tree(args, run_parity_tree(args, device))
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
     if args.workload == "trajectory":
         if rank == 0:
             report_trajectory(args, run_trajectory(args, device))
@@ -1101,12 +1334,14 @@ def main():
         "dtype": "f32 pair terms + f64 near pairs/sums" if prec == "mixed" else "f64",
         "data": "synthetic (seeded lognormal droplets, 2% volume fraction)",
         "config": {
-            "workload": f"direct DEM step (hash detection + merge + dipole force + Oseen convection + Euler), "
-                        f"N={n}, periodic, dt=1e-4",
+            "workload": direct_workload(n),
             "precision": prec,
             "pairs_per_s": steps_per_s * pairs,
             "l2": "flushed between steps (256 MiB write outside the timed events)",
-            "merges_in_timed_and_warmup": res["merges"],
+            "timed_window": f"steps {args.advance + args.warmup}..{args.advance + args.warmup + K - 1} of the "
+                            f"trajectory from the seeded state ({args.advance} untimed steps, then the warm-up)",
+            "merges_before_timed": res["merges_advance"],
+            "merges_in_timed": res["merges_timed"],
             "n_final": res["n_final"],
             "kernel_ms_per_launch": {k: v[0] / v[1] for k, v in kern.items()},
             "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
@@ -1138,6 +1373,19 @@ def main():
         line["cpu_baseline"] = {"value": c["steps_per_s"], "unit": "steps/s", "cores": c["cores"], "kind": "port",
                                 "sample": f"hash + Euler on all {n} droplets; both O(N^2) passes on {c['rows']} rows "
                                           f"x {n} columns, extrapolated ({c['sample_s']:.1f} s of CPU work)"}
+    if "fp64" in res:
+        f64 = res["fp64"]
+        fp64_sps = 1000.0 / f64["ms_per_step"]
+        line["fp64_gpu"] = {
+            "steps_per_s": fp64_sps,
+            "ms_per_step": f64["ms_per_step"],
+            "steps_timed": f64["steps"],
+            "merges_in_timed": f64["merges"],
+            "speedup_mixed_vs_fp64": steps_per_s / fp64_sps,
+            "how": "the FP64 drop-in step (bit-exact with the oracle) on the state after the mixed timed steps, "
+                   "same CUDA events and L2 flush",
+        }
+        line["accuracy_mixed_vs_fp64"] = res["accuracy"]
     # kernels of the library launched inside the timed region (its own launch counter); a step without a merge
     # is hash detection (12) + forces (4) + convection (6) + Euler (1)
     line["gpu_launches"] = res["launches"]

@@ -69,6 +69,10 @@ DEM_API const char *dem_last_error(const dem_ctx *ctx);
 DEM_API int dem_device_errors(dem_ctx *ctx, uint32_t *flags_host, void *stream);
 /* Library version string (host). */
 DEM_API const char *dem_version(void);
+/* The binary version (major * 10 + minor, 100 for sm_100a) of the device code
+ * the CUDA runtime loads for this library's kernels on `device`, from
+ * cudaFuncGetAttributes.  Needs a CUDA device.  No reference counterpart. */
+DEM_API int dem_kernel_binary_version(int device, int *version);
 /* Number of kernels this library has launched in the process so far (all
  * contexts and devices; host-side counter, no synchronisation).  The
  * difference across a region is the count of the library's launches in it. */
@@ -89,7 +93,11 @@ DEM_API int dem_profile_reset(dem_ctx *ctx);
 /* schedules of the mixed-precision direct passes */
 #define DEM_SCHED_AUTO 0      /* symmetric when its partial sums fit, else split */
 #define DEM_SCHED_SPLIT 1     /* every ordered pair; the j range split in chunks */
-#define DEM_SCHED_SYMMETRIC 2 /* every unordered pair once (F_ji = -F_ij, Oseen tensor even) */
+#define DEM_SCHED_SYMMETRIC 2 /* every unordered pair once (F_ji = -F_ij, Oseen tensor even); one box:
+                                 blocks of droplets in Morton order, far j's without the per-pair
+                                 minimum image and tests */
+#define DEM_SCHED_SYMMETRIC_PLAIN 3 /* symmetric, blocks in the caller's droplet order (every pair takes the
+                                       minimum image and the tests) */
 
 /* Tuning of the mixed-precision direct kernels (0 keeps the current value).
  *   i_per_thread  i-particles register-blocked per thread (1, 2, 4 or 8;
@@ -104,8 +112,9 @@ DEM_API int dem_direct_set_tuning(dem_ctx *ctx, int i_per_thread, int threads, i
 DEM_API int dem_direct_get_tuning(const dem_ctx *ctx, int *i_per_thread, int *threads, int *j_splits,
                                   double *near_force, double *near_oseen, int *schedule);
 /* The plan the mixed-precision passes run for n droplets under the current
- * tuning (no launch): the resolved schedule (DEM_SCHED_SPLIT or
- * DEM_SCHED_SYMMETRIC), i-per-thread blocking, threads per CTA, CTAs per pass
+ * tuning (no launch): the resolved schedule (DEM_SCHED_SPLIT,
+ * DEM_SCHED_SYMMETRIC or DEM_SCHED_SYMMETRIC_PLAIN), i-per-thread blocking,
+ * threads per CTA, CTAs per pass
  * and, for the split schedule, the number of j-chunks. */
 DEM_API int dem_direct_plan(const dem_ctx *ctx, int n, int periodic, int *schedule, int *i_per_thread,
                             int *threads, long long *ctas, int *j_splits);
@@ -315,9 +324,10 @@ DEM_API int dem_euler_update_total(dem_ctx *ctx, int n, const double *x, const d
  * (ix*73856093 ^ iy*19349663 ^ iz*83492791) & (table_size - 1), 27 neighbour
  * cells, MIC distance <= r_i + r_j.
  * pairs: int32[pair_capacity][2] (device).  counts: int64[2] (device):
- * counts[0] = number of unique pairs (may exceed pair_capacity: then only the
- * first pair_capacity pairs are written and DEM_DEVERR_PAIR_OVERFLOW is
- * raised), counts[1] = raw hits before de-duplication.
+ * counts[0] = number of unique pairs (may exceed pair_capacity: then the
+ * buffer holds the lexicographically first pair_capacity pairs of the sorted
+ * set and DEM_DEVERR_PAIR_OVERFLOW is raised), counts[1] = raw hits before
+ * de-duplication.
  * Replaces SpatialHashCollisionDetector.detect,
  * dem/collision_detector/spatial_hash_collision_detector.py:233-316
  * (kernels :74-229, np.unique :312). */
@@ -342,10 +352,12 @@ DEM_API int dem_overlap_pairs(dem_ctx *ctx, int n, const double *x, const double
  * cudaMalloc when they detect collisions (a fixed device-memory budget handed
  * over up front, a control loop that must not take cudaMalloc's device-wide
  * synchronisation between steps, or an allocator owned by another
- * component).  Same arguments, semantics and pair output as dem_hash_detect,
- * without a context: the workspace is a fixed device array inside the
- * library (about 2.9 MB, held on every GPU that loads the library until the
- * process exits).  Limits: n <= 65536 droplets and table_size <= 131072
+ * component).  Same arguments and pair output as dem_hash_detect, without a
+ * context: the workspace is a fixed device array inside the library (about
+ * 2.9 MB, held on every GPU that loads the library until the process exits).
+ * Overflow: with no context there is no error flag to read, so a caller sees
+ * a short pair buffer only as counts[0] > pair_capacity (the buffer then holds
+ * the lexicographically first pair_capacity pairs).  Limits: n <= 65536 droplets and table_size <= 131072
  * buckets; larger sizes return DEM_E_CAPACITY; bad pointers DEM_E_INVALID;
  * CUDA failures DEM_E_CUDA (no message: there is no context).  The first call
  * on a device looks up the array's device address (cudaGetSymbolAddress) with

@@ -43,6 +43,7 @@
 
 #include "corr.cuh"
 #include "mixed_common.cuh"
+#include "morton.cuh"
 #include "scan.cuh"
 
 namespace dem {
@@ -88,6 +89,7 @@ struct dem_bh {
     int32_t *scan_in = nullptr, *coff = nullptr;  // [max_nodes + 1] children per node of a level, offsets
     BhNodes nd{};
     std::vector<int> level_off;
+    double *top_part = nullptr;  // [TOP_PARTIALS][12] chunk partials of the top levels' moments
     const dem_corr *corr = nullptr;  // periodic-image correction of the velocity walk (borrowed), or none
 };
 
@@ -328,6 +330,41 @@ __global__ void level_write_kernel(BhNodes nd, int ls, int le, const int32_t *__
     }
 }
 
+// Node k's R^3-weighted centre and second moment from its sums v (weight, first and
+// second moments relative to (rx, ry, rz), the node's first droplet).
+__device__ void r3_finish(BhNodes nd, int k, const double *v, double rx, double ry, double rz, int s0, int c, double ox,
+                          double oy, double oz, double box, const uint32_t *__restrict__ keys) {
+    {
+        {  // (kept as one block: the body of node_r3_kernel's final step)
+            const double w = v[0];
+            float Q[6];
+            if (w > 0.0) {
+                const double mx = v[1] / w, my = v[2] / w, mz = v[3] / w;
+                nd.cx[k] = rx + mx;
+                nd.cy[k] = ry + my;
+                nd.cz[k] = rz + mz;
+                Q[0] = (float)(v[4] - w * mx * mx);
+                Q[1] = (float)(v[5] - w * mx * my);
+                Q[2] = (float)(v[6] - w * mx * mz);
+                Q[3] = (float)(v[7] - w * my * my);
+                Q[4] = (float)(v[8] - w * my * mz);
+                Q[5] = (float)(v[9] - w * mz * mz);
+            } else {  // geometric centre of the cell (octree_node.py:98-114)
+                const int lv = nd.level[k];
+                const uint32_t key = c > 0 ? keys[s0] : 0u;
+                const uint32_t pre = lv > 0 ? key >> (30 - 3 * lv) << (30 - 3 * lv) : 0u;
+                const double side = ldexp(box, -lv), cell = ldexp(box, -10);
+                nd.cx[k] = ox + compact10(pre >> 2) * cell + side * 0.5;
+                nd.cy[k] = oy + compact10(pre >> 1) * cell + side * 0.5;
+                nd.cz[k] = oz + compact10(pre) * cell + side * 0.5;
+                for (int q = 0; q < 6; ++q) Q[q] = 0.f;
+            }
+            nd.qr[2 * (size_t)k] = make_float4(Q[0], Q[1], Q[2], Q[3]);
+            nd.qr[2 * (size_t)k + 1] = make_float4(Q[4], Q[5], (float)w, 0.f);
+        }
+    }
+}
+
 // R^3 and R^3-weighted centre of nodes [a, b), one CTA (big nodes) or one warp per node
 template <bool BLOCK>
 __global__ void node_r3_kernel(BhNodes nd, int a, int b, const double *__restrict__ ps, int cap,
@@ -372,34 +409,143 @@ __global__ void node_r3_kernel(BhNodes nd, int a, int b, const double *__restric
                 }
             __syncthreads();
         }
-        if (lane == 0) {
-            const double w = v[0];
-            float Q[6];
-            if (w > 0.0) {
-                const double mx = v[1] / w, my = v[2] / w, mz = v[3] / w;
-                nd.cx[k] = rx + mx;
-                nd.cy[k] = ry + my;
-                nd.cz[k] = rz + mz;
-                Q[0] = (float)(v[4] - w * mx * mx);
-                Q[1] = (float)(v[5] - w * mx * my);
-                Q[2] = (float)(v[6] - w * mx * mz);
-                Q[3] = (float)(v[7] - w * my * my);
-                Q[4] = (float)(v[8] - w * my * mz);
-                Q[5] = (float)(v[9] - w * mz * mz);
-            } else {  // geometric centre of the cell (octree_node.py:98-114)
-                const int lv = nd.level[k];
-                const uint32_t key = c > 0 ? keys[s0] : 0u;
-                const uint32_t pre = lv > 0 ? key >> (30 - 3 * lv) << (30 - 3 * lv) : 0u;
-                const double side = ldexp(box, -lv), cell = ldexp(box, -10);
-                nd.cx[k] = ox + compact10(pre >> 2) * cell + side * 0.5;
-                nd.cy[k] = oy + compact10(pre >> 1) * cell + side * 0.5;
-                nd.cz[k] = oz + compact10(pre) * cell + side * 0.5;
-                for (int q = 0; q < 6; ++q) Q[q] = 0.f;
-            }
-            nd.qr[2 * (size_t)k] = make_float4(Q[0], Q[1], Q[2], Q[3]);
-            nd.qr[2 * (size_t)k + 1] = make_float4(Q[4], Q[5], (float)w, 0.f);
-        }
+        if (lane == 0) r3_finish(nd, k, v, rx, ry, rz, s0, c, ox, oy, oz, box, keys);
     }
+}
+
+// ---------------------------------------------------------------------------
+// The top three levels (the root, its children and grandchildren) cover every
+// droplet once per level, in a few huge nodes: one CTA per node would leave the
+// root's 2^20 droplets to one SM.  Their moments are summed in chunks instead,
+// TOP_CHUNKS >> (3 level) CTAs per node, each writing one partial, and a second
+// kernel adds a node's partials in chunk order (deterministic).  The sums are
+// the same as node_r3_kernel's / node_force_kernel's (relative to the node's
+// first droplet / to its centre), in another order.
+// ---------------------------------------------------------------------------
+constexpr int TOP_LEVELS = 3;
+constexpr int TOP_CHUNKS = 512;  // chunks of the root; a level-l node gets TOP_CHUNKS >> (3 l)
+constexpr int TOP_T = 256;
+constexpr int TOP_PARTIALS = 3 * TOP_CHUNKS;  // each full level of the top three holds TOP_CHUNKS chunks in all
+
+struct TopPlan {
+    int levels;
+    int node0[TOP_LEVELS], nodes[TOP_LEVELS], chunks[TOP_LEVELS];
+    int cta0[TOP_LEVELS + 1];  // first CTA (partial) of each level; cta0[levels] = total
+};
+
+__device__ __forceinline__ void top_locate(const TopPlan &tp, int q, int &node, int &chunk, int &nchunk) {
+    int l = 0;
+    while (l + 1 < tp.levels && q >= tp.cta0[l + 1]) ++l;
+    const int local = q - tp.cta0[l];
+    nchunk = tp.chunks[l];
+    node = tp.node0[l] + local / nchunk;
+    chunk = local % nchunk;
+}
+
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double (*red)[TOP_T / 32]) {
+    for (int q = 0; q < NV; ++q)
+        for (int o = 16; o; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+    const int wp = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0)
+        for (int q = 0; q < NV; ++q) red[q][wp] = v[q];
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int q = 0; q < NV; ++q) {
+            v[q] = 0;
+            for (int u = 0; u < TOP_T / 32; ++u) v[q] += red[q][u];
+        }
+}
+
+__global__ void __launch_bounds__(TOP_T) top_r3_partial_kernel(BhNodes nd, TopPlan tp, const double *__restrict__ ps,
+                                                               int cap, double *__restrict__ part) {
+    __shared__ double red[10][TOP_T / 32];
+    int k, c, nc;
+    top_locate(tp, blockIdx.x, k, c, nc);
+    const int s0 = nd.start[k], cnt = nd.count[k];
+    const double rx = cnt > 0 ? ps[s0] : 0.0, ry = cnt > 0 ? ps[cap + s0] : 0.0,
+                 rz = cnt > 0 ? ps[2 * (size_t)cap + s0] : 0.0;
+    const int t0 = (int)((long long)cnt * c / nc), t1 = (int)((long long)cnt * (c + 1) / nc);
+    double v[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int t = t0 + threadIdx.x; t < t1; t += TOP_T) {
+        const double r = ps[3 * (size_t)cap + s0 + t];
+        const double w = r * r * r;
+        const double dx = ps[s0 + t] - rx, dy = ps[cap + s0 + t] - ry, dz = ps[2 * (size_t)cap + s0 + t] - rz;
+        v[0] += w;
+        v[1] += w * dx;
+        v[2] += w * dy;
+        v[3] += w * dz;
+        v[4] += w * dx * dx;
+        v[5] += w * dx * dy;
+        v[6] += w * dx * dz;
+        v[7] += w * dy * dy;
+        v[8] += w * dy * dz;
+        v[9] += w * dz * dz;
+    }
+    block_sum<10>(v, red);
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 10; ++q) part[(size_t)blockIdx.x * 12 + q] = v[q];
+}
+
+__global__ void top_force_partial_kernel(BhNodes nd, TopPlan tp, const double *__restrict__ ps,
+                                         const double *__restrict__ fsort, int cap, double *__restrict__ part) {
+    __shared__ double red[12][TOP_T / 32];
+    int k, c, nc;
+    top_locate(tp, blockIdx.x, k, c, nc);
+    const int s0 = nd.start[k], cnt = nd.count[k];
+    const double cx = nd.cx[k], cy = nd.cy[k], cz = nd.cz[k];
+    const int t0 = (int)((long long)cnt * c / nc), t1 = (int)((long long)cnt * (c + 1) / nc);
+    double v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int t = t0 + threadIdx.x; t < t1; t += TOP_T) {
+        const int si = s0 + t;
+        const double F[3] = {fsort[si], fsort[cap + si], fsort[2 * (size_t)cap + si]};
+        const double d[3] = {ps[si] - cx, ps[cap + si] - cy, ps[2 * (size_t)cap + si] - cz};
+        for (int q = 0; q < 3; ++q) v[q] += F[q];
+        for (int pp = 0; pp < 3; ++pp)
+            for (int q = 0; q < 3; ++q) v[3 + 3 * pp + q] += d[pp] * F[q];
+    }
+    block_sum<12>(v, red);
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 12; ++q) part[(size_t)blockIdx.x * 12 + q] = v[q];
+}
+
+// One thread per top node: its chunk partials added in chunk order, then node_r3_kernel's final step.
+__global__ void top_r3_finish_kernel(BhNodes nd, TopPlan tp, const double *__restrict__ part,
+                                     const double *__restrict__ ps, int cap, const double *__restrict__ geom,
+                                     const uint32_t *__restrict__ keys) {
+    const int total = tp.node0[tp.levels - 1] + tp.nodes[tp.levels - 1] - tp.node0[0];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const int k = tp.node0[0] + t;
+    int l = 0;
+    while (l + 1 < tp.levels && k >= tp.node0[l + 1]) ++l;
+    const int nc = tp.chunks[l];
+    const size_t q0 = (size_t)tp.cta0[l] + (size_t)(k - tp.node0[l]) * nc;
+    double v[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int c = 0; c < nc; ++c)
+        for (int q = 0; q < 10; ++q) v[q] += part[(q0 + c) * 12 + q];
+    const int s0 = nd.start[k], cnt = nd.count[k];
+    const double rx = cnt > 0 ? ps[s0] : 0.0, ry = cnt > 0 ? ps[cap + s0] : 0.0,
+                 rz = cnt > 0 ? ps[2 * (size_t)cap + s0] : 0.0;
+    r3_finish(nd, k, v, rx, ry, rz, s0, cnt, geom[0], geom[1], geom[2], geom[3], keys);
+}
+
+// One thread per top node: force sum and dipole from its chunk partials, in chunk order.
+__global__ void top_force_finish_kernel(BhNodes nd, TopPlan tp, const double *__restrict__ part) {
+    const int total = tp.node0[tp.levels - 1] + tp.nodes[tp.levels - 1] - tp.node0[0];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const int k = tp.node0[0] + t;
+    int l = 0;
+    while (l + 1 < tp.levels && k >= tp.node0[l + 1]) ++l;
+    const int nc = tp.chunks[l];
+    const size_t q0 = (size_t)tp.cta0[l] + (size_t)(k - tp.node0[l]) * nc;
+    double v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int c = 0; c < nc; ++c)
+        for (int q = 0; q < 12; ++q) v[q] += part[(q0 + c) * 12 + q];
+    for (int q = 0; q < 3; ++q)  // v = (F, D row-major): the record's order
+        nd.fd[3 * (size_t)k + q] = make_float4((float)v[4 * q], (float)v[4 * q + 1], (float)v[4 * q + 2],
+                                               (float)v[4 * q + 3]);
 }
 
 // sum F and dipole D = sum (x - c) F^T of nodes [a, b)
@@ -786,6 +932,60 @@ __global__ void scale_nodes_kernel(BhNodes nd, int nc, const unsigned long long 
 
 }  // namespace
 
+namespace dem {
+
+static size_t ws_align(size_t b) { return (b + 255) & ~size_t(255); }
+
+size_t morton_ws_bytes(int n) {
+    const size_t tiles = (size_t)((n + RS_TILE - 1) / RS_TILE);
+    return 4 * ws_align(4 * (size_t)n) + ws_align(4 * 2 * (256 * tiles + 1)) + ws_align(6 * 8) + ws_align(4 * 8);
+}
+
+MortonWs morton_ws_carve(void *base, int n) {
+    const size_t tiles = (size_t)((n + RS_TILE - 1) / RS_TILE);
+    char *p = static_cast<char *>(base);
+    MortonWs w;
+    w.keys[0] = reinterpret_cast<uint32_t *>(p);
+    p += ws_align(4 * (size_t)n);
+    w.keys[1] = reinterpret_cast<uint32_t *>(p);
+    p += ws_align(4 * (size_t)n);
+    w.idx[0] = reinterpret_cast<int32_t *>(p);
+    p += ws_align(4 * (size_t)n);
+    w.idx[1] = reinterpret_cast<int32_t *>(p);
+    p += ws_align(4 * (size_t)n);
+    w.hist = reinterpret_cast<int32_t *>(p);
+    p += ws_align(4 * 2 * (256 * tiles + 1));
+    w.bbox = reinterpret_cast<long long *>(p);
+    p += ws_align(6 * 8);
+    w.geom = reinterpret_cast<double *>(p);
+    return w;
+}
+
+int morton_order(dem_ctx *ctx, int n, const double *x, const double *y, const double *z, int periodic, double L,
+                 const MortonWs &w, cudaStream_t s) {
+    const int g = std::max(1, std::min((n + 255) / 256, 8 * ctx->sm_count));
+    if (!periodic) {
+        bbox_init_kernel<<<1, 32, 0, counted(s)>>>(w.bbox);
+        bbox_kernel<<<g, 256, 0, counted(s)>>>(n, x, y, z, w.bbox);
+    }
+    geom_kernel<<<1, 32, 0, counted(s)>>>(periodic ? 1 : 0, L, w.bbox, w.geom);
+    keys_kernel<<<g, 256, 0, counted(s)>>>(n, x, y, z, w.geom, w.keys[0], w.idx[0]);
+    const int tiles = (n + RS_TILE - 1) / RS_TILE;
+    int32_t *hist = w.hist, *off = w.hist + 256 * (size_t)tiles + 1;
+    int cur = 0, rc;
+    for (int pass = 0; pass < 4; ++pass) {
+        const int shift = 8 * pass;
+        rs_hist_kernel<<<tiles, RS_T, 0, counted(s)>>>(n, w.keys[cur], shift, tiles, hist);
+        if ((rc = exclusive_scan<int32_t, int32_t>(ctx, hist, off, 256LL * tiles, s))) return rc;
+        rs_scatter_kernel<<<tiles, RS_T, 0, counted(s)>>>(n, w.keys[cur], w.idx[cur], w.keys[1 - cur],
+                                                          w.idx[1 - cur], shift, tiles, off);
+        cur = 1 - cur;
+    }
+    return dem_check_launch(ctx, "morton order");  // four passes: the result is back in buffer 0
+}
+
+}  // namespace dem
+
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
@@ -844,7 +1044,7 @@ static int bh_nodes_reserve(dem_bh *b, int m, int keep, cudaStream_t s) {
 static void bh_free(dem_bh *b) {
     cudaSetDevice(b->ctx->device);
     bh_free_nodes(b->nd);
-    void *ptrs[] = {b->keys[0], b->keys[1], b->idx[0],   b->idx[1], b->hist,    b->ps,  b->fsort, b->loff, b->fs32,
+    void *ptrs[] = {b->top_part, b->keys[0], b->keys[1], b->idx[0],   b->idx[1], b->hist,    b->ps,  b->fsort, b->loff, b->fs32,
                     b->bounds,  b->bbox,    b->geom,     b->counters, b->scales, b->scan_in, b->coff};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -856,6 +1056,20 @@ static inline int grid_of(dem_ctx *ctx, long long work, int threads = 256) {
     if (g < 1) g = 1;
     if (g > 8LL * ctx->sm_count) g = 8LL * ctx->sm_count;
     return (int)g;
+}
+
+// The chunked sums of the top levels (levels 0 .. min(3, nlevels) - 1).
+static TopPlan top_plan(const dem_bh *b) {
+    TopPlan tp{};
+    tp.levels = std::min(TOP_LEVELS, b->nlevels);
+    tp.cta0[0] = 0;
+    for (int l = 0; l < tp.levels; ++l) {
+        tp.node0[l] = b->level_off[l];
+        tp.nodes[l] = (l + 1 < b->nlevels ? b->level_off[l + 1] : b->node_count) - b->level_off[l];
+        tp.chunks[l] = TOP_CHUNKS >> (3 * l);
+        tp.cta0[l + 1] = tp.cta0[l] + tp.nodes[l] * tp.chunks[l];
+    }
+    return tp;
 }
 
 extern "C" {
@@ -877,6 +1091,7 @@ int dem_bh_create(dem_ctx *ctx, int capacity, dem_bh **out) {
         (rc = bh_alloc(ctx, &b->loff, n, "bh")) || (rc = bh_alloc(ctx, &b->fs32, n, "bh")) ||
         (rc = bh_alloc(ctx, &b->bbox, 6, "bh")) || (rc = bh_alloc(ctx, &b->geom, 4, "bh")) ||
         (rc = bh_alloc(ctx, &b->counters, 2, "bh")) || (rc = bh_alloc(ctx, &b->scales, 2, "bh")) ||
+        (rc = bh_alloc(ctx, &b->top_part, (size_t)TOP_PARTIALS * 12, "bh")) ||
         (rc = bh_nodes_reserve(b, std::max(4096, capacity / 4), 0, nullptr))) {
         bh_free(b);
         return rc;
@@ -960,10 +1175,12 @@ int dem_bh_build(dem_bh *b, int n, const double *x, const double *y, const doubl
     }
     b->node_count = le;
     b->nlevels = (int)b->level_off.size();
-    // node R^3 and centres: one CTA per node on the top three levels, one warp per node below
-    const int top = b->nlevels > 3 ? b->level_off[3] : le;
-    node_r3_kernel<true><<<std::max(top, 1), 256, 0, counted(s)>>>(b->nd, 0, top, b->ps, b->capacity, b->geom,
-                                                                   b->keys[0]);
+    // node R^3 and centres: chunked sums on the top three levels, one warp per node below
+    const TopPlan tp = top_plan(b);
+    const int top = tp.node0[tp.levels - 1] + tp.nodes[tp.levels - 1];
+    top_r3_partial_kernel<<<tp.cta0[tp.levels], TOP_T, 0, counted(s)>>>(b->nd, tp, b->ps, b->capacity, b->top_part);
+    top_r3_finish_kernel<<<(top + 127) / 128, 128, 0, counted(s)>>>(b->nd, tp, b->top_part, b->ps, b->capacity,
+                                                                    b->geom, b->keys[0]);
     if (le > top)
         node_r3_kernel<false><<<grid_of(ctx, 32LL * (le - top)), 256, 0, counted(s)>>>(b->nd, top, le, b->ps,
                                                                                        b->capacity, b->geom,
@@ -1040,8 +1257,11 @@ int dem_bh_velocity(dem_bh *b, const double *fx, const double *fy, const double 
         return rc;
     maxabs_kernel<<<grid_of(ctx, n), 256, 0, counted(s)>>>(n, fs, fs + b->capacity, fs + 2 * (size_t)b->capacity,
                                                            b->scales + 1);
-    const int top = b->nlevels > 3 ? b->level_off[3] : le;
-    node_force_kernel<true><<<std::max(top, 1), 256, 0, counted(s)>>>(b->nd, 0, top, b->ps, b->fsort, b->capacity);
+    const TopPlan tp = top_plan(b);
+    const int top = tp.node0[tp.levels - 1] + tp.nodes[tp.levels - 1];
+    top_force_partial_kernel<<<tp.cta0[tp.levels], TOP_T, 0, counted(s)>>>(b->nd, tp, b->ps, b->fsort, b->capacity,
+                                                                            b->top_part);
+    top_force_finish_kernel<<<(top + 127) / 128, 128, 0, counted(s)>>>(b->nd, tp, b->top_part);
     if (le > top)
         node_force_kernel<false><<<grid_of(ctx, 32LL * (le - top)), 256, 0, counted(s)>>>(b->nd, top, le, b->ps,
                                                                                           b->fsort, b->capacity);

@@ -103,9 +103,31 @@ static void prof_clear(dem_ctx *ctx) {
     ctx->prof.clear();
 }
 
+namespace {
+// An empty kernel of this library: the runtime reports the binary version of
+// the code it would load for it, i.e. the architecture the library was built for.
+__global__ void binary_version_probe_kernel() {}
+}  // namespace
+
 extern "C" {
 
 const char *dem_version(void) { return DEM_VERSION; }
+
+int dem_kernel_binary_version(int device, int *version) {
+    if (!version) return DEM_E_INVALID;
+    int prev = 0;
+    if (cudaGetDevice(&prev) != cudaSuccess) return DEM_E_CUDA;
+    if (cudaSetDevice(device) != cudaSuccess) return DEM_E_CUDA;
+    cudaFuncAttributes a;
+    cudaError_t e = cudaFuncGetAttributes(&a, binary_version_probe_kernel);
+    cudaSetDevice(prev);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return DEM_E_CUDA;
+    }
+    *version = a.binaryVersion;
+    return DEM_OK;
+}
 
 int dem_profile_enable(dem_ctx *ctx, int enable) {
     if (!ctx) return DEM_E_INVALID;
@@ -151,6 +173,7 @@ int dem_ctx_reserve(dem_ctx *ctx, int capacity) {
     if ((rc = grow(ctx, &ctx->pack_b, n, "workspace"))) return rc;
     if ((rc = grow(ctx, &ctx->cell_hash, n, "workspace"))) return rc;
     if ((rc = grow(ctx, &ctx->sorted_idx, n, "workspace"))) return rc;
+    if ((rc = grow(ctx, &ctx->hash_pos, 2 * n, "workspace"))) return rc;
     if ((rc = grow(ctx, &ctx->pair_count, n + 1, "workspace"))) return rc;
     if ((rc = grow(ctx, &ctx->pair_offset, n + 1, "workspace"))) return rc;
     if ((rc = grow(ctx, &ctx->flags, n + 1, "workspace"))) return rc;
@@ -190,7 +213,7 @@ void dem_ctx_destroy(dem_ctx *ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     void *ptrs[] = {ctx->d_err,         ctx->pack_a,      ctx->pack_b,     ctx->partial,    ctx->dscratch,
-                    ctx->cell_hash,     ctx->bucket_count, ctx->bucket_start, ctx->bucket_cursor, ctx->sorted_idx,
+                    ctx->cell_hash,     ctx->bucket_count, ctx->bucket_start, ctx->bucket_cursor, ctx->sorted_idx, ctx->hash_pos,
                     ctx->pair_count,    ctx->pair_offset, ctx->flags,      ctx->keep_off,   ctx->merged_buf,
                     ctx->merged_cnt,    ctx->scan_tmp,    ctx->sym_partial};
     for (void *p : ptrs)
@@ -231,7 +254,7 @@ int dem_direct_set_tuning(dem_ctx *ctx, int i_per_thread, int threads, int j_spl
     ctx->tuning.j_splits = j_splits;
     if (near_force > 0) ctx->tuning.near_force = near_force;
     if (near_oseen > 0) ctx->tuning.near_oseen = near_oseen;
-    if (schedule < DEM_SCHED_AUTO || schedule > DEM_SCHED_SYMMETRIC)
+    if (schedule < DEM_SCHED_AUTO || schedule > DEM_SCHED_SYMMETRIC_PLAIN)
         return dem_set_error(ctx, DEM_E_INVALID, "unknown schedule");
     ctx->tuning.schedule = schedule;
     return DEM_OK;

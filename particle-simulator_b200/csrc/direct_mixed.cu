@@ -301,7 +301,7 @@ static int symmetric_ipt(const dem_ctx *ctx, int n) {
     const int sched = ctx->tuning.schedule;
     if (sched == DEM_SCHED_SPLIT) return 0;
     const int max_ipt = ctx->tuning.i_per_thread >= 4 ? 4 : 2;  // two i's per packed FP32x2 operation
-    if (sched == DEM_SCHED_SYMMETRIC) return max_ipt;
+    if (sched == DEM_SCHED_SYMMETRIC || sched == DEM_SCHED_SYMMETRIC_PLAIN) return max_ipt;
     const long long enough = (long long)(3.5 * ctx->sm_count);
     for (int ipt = max_ipt; ipt >= 2; ipt /= 2)
         if (sym_block_pairs(n, ipt) >= enough && sym_partial_bytes(n, ipt) <= SYM_BUDGET) return ipt;
@@ -315,7 +315,7 @@ int direct_plan(const dem_ctx *ctx, int n, int periodic, int *schedule, int *i_p
     if (sym) {
         const long long B = (long long)128 * sym;
         const long long nb = (n + B - 1) / B;
-        *schedule = DEM_SCHED_SYMMETRIC;
+        *schedule = ctx->tuning.schedule == DEM_SCHED_SYMMETRIC_PLAIN ? DEM_SCHED_SYMMETRIC_PLAIN : DEM_SCHED_SYMMETRIC;
         *i_per_thread = sym;
         *threads = 128;
         *ctas = nb * (nb + 1) / 2;

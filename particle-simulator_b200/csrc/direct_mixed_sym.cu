@@ -37,6 +37,7 @@
 // when gridDim.x < items).  j-tiles come in by 1-D TMA bulk copies (no
 // multicast) into a double buffer on mbarriers with bounded waits; the copy of
 // the next tile, possibly of the next item, is in flight while a tile is used.
+#include "morton.cuh"
 #include "sym.cuh"
 
 namespace dem {
@@ -414,13 +415,571 @@ __global__ void __launch_bounds__(SYM_T, 4) mixed_sym_kernel(const SymArgs a) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// One box with its droplets in Morton order: lists of far j's without the
+// per-pair tests.
+//
+// The packed layout holds the droplets in Morton order (perm maps a packed
+// position to its droplet), so a block of B consecutive positions is compact
+// in space (about L/4 per side at N = 65,536).  For a work item (I, J), I < J,
+// every j of block J is classified against block I:
+//
+//   * far: the minimum-image distance from j to the bounding box of block I
+//     exceeds k (max r_I + r_j) (0.1 % margin), so no pair of j with block I
+//     is near contact;
+//   * unambiguous: no droplet of block I lies within 2^-17 L (twice the
+//     ambiguity margin of the pair test) of the point where its separation
+//     from j would be L/2 on some axis.  Checked against a per-block bitmap of
+//     occupied 1/65,536 L bins per axis;
+//   * fixed image: on every axis one periodic image serves every i of the
+//     block, with the whole separation interval inside the ambiguity margin
+//     (fixed implies unambiguous).
+//
+// Classes and their sub-tile loops:
+//   fast   (far, fixed image): stored with that image applied; the loop takes
+//          d = x_j - x_i and the pair terms, nothing else;
+//   medium (far, unambiguous): the loop takes the FP32 minimum image and the
+//          pair terms, without the near and ambiguity tests and the FP64 branch;
+//   slow   (the rest, and every j of a diagonal item): the loop of
+//          mixed_sym_kernel.
+// A far, unambiguous pair is one the slow loop would evaluate in FP32 too, so
+// every pair takes the same FP32 / FP64 decision as in mixed_sym_kernel.
+//
+// The lists are filled in j order, fast, medium and slow runs one after the
+// other, each padded to whole 32-entry sub-tiles with zero-weight entries.  All
+// warps walk the same lists, so every warp does the same work between the CTA
+// barriers.  The j block is classified as it is loaded (coalesced vector loads
+// from the L2-resident packed arrays), so it is not staged by TMA.  Results are
+// deterministic: lists, sums and their order depend only on the inputs.
+// ---------------------------------------------------------------------------
+struct SortedArgs {
+    SymArgs s;               // one box; packed layout in Morton order
+    const int32_t *perm;     // packed position -> droplet (first n positions)
+    const float4 *bounds;    // [nb][2]: (min s_x, min s_y, min s_z, max k r), (max s_x, max s_y, max s_z, 0)
+    const uint32_t *occ;     // [nb][3][AMB_BINS / 32]: occupied bins of the stored coordinates per block
+};
+
+constexpr int SORTED_PAD = 96;      // list slots beyond B: the padding of the three runs (<= 31 each)
+constexpr int AMB_BINS = 65536;     // bins per axis of the occupancy bitmaps (a power of two)
+constexpr int AMB_WORDS = AMB_BINS / 32;
+
+template <bool FORCE>
+constexpr int sorted_entry_bytes() {
+    return FORCE ? 16 + 16 + 8 + 4 : 16 + 16 + 16 + 8 + 4;
+}
+template <int IPT, bool FORCE>
+constexpr int sorted_smem_bytes() {
+    return (SYM_T * IPT + SORTED_PAD) * sorted_entry_bytes<FORCE>();
+}
+
+// far entry of the fast run's padding: zero weight, ~10^6 ell from every droplet
+constexpr float SORTED_FAR = 1.0e6f;
+
+enum { CLS_FAST = 0, CLS_MEDIUM = 1, CLS_SLOW = 2 };
+
+__device__ __forceinline__ int amb_bin(float v, float Ls, float invLs) {
+    return ((int)floorf(fmaf(v, invLs, 0.5f) * (float)AMB_BINS)) & (AMB_BINS - 1);
+}
+
+// Class of the stored j entry (sc: coordinates, kj: k r_j) against block I; for
+// CLS_FAST sc comes back with the fixed image applied.
+template <bool PER>
+__device__ __forceinline__ int classify_j(float sc[3], float kj, const float4 &blo, const float4 &bhi,
+                                          const uint32_t *__restrict__ occ, float Ls, float invLs, float hm_fast,
+                                          float m_amb) {
+    const float lo3[3] = {blo.x, blo.y, blo.z}, hi3[3] = {bhi.x, bhi.y, bhi.z};
+    bool fixed = true;
+    float g2 = 0.f;
+    float u3[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        float dlo = sc[c] - hi3[c], dhi = sc[c] - lo3[c];
+        float gap;
+        if (PER) {
+            const float u = rintf(0.5f * (dlo + dhi) * invLs);
+            u3[c] = u;
+            dlo = fmaf(-u, Ls, dlo);
+            dhi = fmaf(-u, Ls, dhi);
+            fixed = fixed && dlo >= -hm_fast && dhi <= hm_fast;
+            // minimum-image distance of the interval from 0: the nearest of its three images
+            gap = fmaxf(0.f, fmaxf(dlo, -dhi));
+            gap = fminf(gap, fmaxf(0.f, fmaxf(dlo + Ls, -(dhi + Ls))));
+            gap = fminf(gap, fmaxf(0.f, fmaxf(dlo - Ls, -(dhi - Ls))));
+        } else {
+            gap = fmaxf(0.f, fmaxf(dlo, -dhi));
+        }
+        g2 = fmaf(gap, gap, g2);
+    }
+    const float kk = blo.w + kj;
+    if (!(g2 > 1.001f * kk * kk)) return CLS_SLOW;
+    if (!PER) return CLS_FAST;
+    if (fixed) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) sc[c] = fmaf(-u3[c], Ls, sc[c]);
+        return CLS_FAST;
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {  // a droplet of block I near s_j - L/2 on this axis: ambiguous
+        const float a = sc[c] - 0.5f * Ls;
+        const int b0 = amb_bin(a - m_amb, Ls, invLs), b1 = amb_bin(a + m_amb, Ls, invLs);
+        const uint32_t *w = occ + c * AMB_WORDS;
+        if ((w[b0 >> 5] >> (b0 & 31)) & 1u) return CLS_SLOW;
+        if ((w[b1 >> 5] >> (b1 & 31)) & 1u) return CLS_SLOW;
+    }
+    return CLS_MEDIUM;
+}
+
+template <int IPT, bool PER, bool FORCE, int MODE>
+__device__ __forceinline__ void sorted_subtile(const SortedArgs &a, const float4 *C0, const float4 *C1,
+                                               const float4 *C2, const float2 *C3, const int *CI, int e0, int lane,
+                                               int tid, int warp, int I, int J, bool diag, const BoxView &v,
+                                               double inv_ell, double fscale_inv, float2 invL2, float2 magic2,
+                                               float2 nmagic2, float2 nL2, float hm, const float2 *xi,
+                                               const float2 *yi, const float2 *zi, const float2 *ki,
+                                               const float2 *wi, const float2 *fxi, const float2 *fyi,
+                                               const float2 *fzi, float2 *ax, float2 *ay, float2 *az, float *hx,
+                                               float *hy, float *hz, float *lx, float *ly, float *lz,
+                                               double (*jnear)[3][32], float2 &sx, float2 &sy, float2 &sz,
+                                               bool &had_exact) {
+    constexpr int B = SYM_T * IPT;
+    constexpr int KP = IPT / 2;
+    constexpr bool TESTS = MODE == CLS_SLOW;
+    constexpr bool IMAGE = MODE != CLS_FAST;
+#pragma unroll 1
+    for (int st = 0; st < 32; ++st) {
+        const int u = (lane + st) & 31;
+        const int jj = e0 + u;
+        const float4 A = C0[jj], Bv = C1[jj];
+        const float2 pjx = make_float2(A.x, A.y), pjy = make_float2(A.z, A.w);
+        const float2 pjz = make_float2(Bv.x, Bv.y);
+        float2 wj, kj, fjx, fjy, fjz;
+        if (FORCE) {
+            wj = make_float2(Bv.z, Bv.w);
+            kj = C3[jj];
+        } else {
+            kj = make_float2(Bv.z, Bv.w);
+            const float4 Q = C2[jj];
+            fjx = make_float2(Q.x, Q.y);
+            fjy = make_float2(Q.z, Q.w);
+            fjz = C3[jj];
+        }
+        bool ex[IPT];
+#pragma unroll
+        for (int kp = 0; kp < KP; ++kp) {
+            float2 dx = p_add(pjx, xi[kp]), dy = p_add(pjy, yi[kp]), dz = p_add(pjz, zi[kp]);
+            if (IMAGE) {
+                dx = p_mic<PER>(dx, invL2, magic2, nmagic2, nL2);
+                dy = p_mic<PER>(dy, invL2, magic2, nmagic2, nL2);
+                dz = p_mic<PER>(dz, invL2, magic2, nmagic2, nL2);
+            }
+            const float2 r2 = p_fma(dx, dx, p_fma(dy, dy, p_mul(dz, dz)));
+            bool ea = false, eb = false;
+            if (TESTS) {
+                const float2 sr = p_add(ki[kp], kj);
+                const float2 sr2 = p_mul(sr, sr);
+                ea = needs_exact<PER>(r2.x, sr2.x, dx.x, dy.x, dz.x, hm);
+                eb = needs_exact<PER>(r2.y, sr2.y, dx.y, dy.y, dz.y, hm);
+            }
+            ex[2 * kp] = ea;
+            ex[2 * kp + 1] = eb;
+            float2 rinv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+            if (FORCE) {
+                const float2 rinv2 = p_mul(rinv, rinv);
+                const float2 rinv4 = p_mul(rinv2, rinv2);
+                float2 base = p_mul(rinv4, p_mul(rinv2, rinv));  // r^-7
+                if (TESTS) {
+                    base.x = ea ? 0.f : base.x;
+                    base.y = eb ? 0.f : base.y;
+                }
+                const float2 angp = p_fma(p_mul(dup2(-5.f), dz), dz, r2);
+                const float2 angzp = p_fma(dup2(2.f), r2, angp);
+                const float2 gp = p_mul(base, angp);
+                const float2 tx = p_mul(gp, dx), ty = p_mul(gp, dy);
+                const float2 tz = p_mul(p_mul(base, angzp), dz);
+                ax[kp] = p_fma(wj, tx, ax[kp]);
+                ay[kp] = p_fma(wj, ty, ay[kp]);
+                az[kp] = p_fma(wj, tz, az[kp]);
+                sx = p_fma(wi[kp], tx, sx);
+                sy = p_fma(wi[kp], ty, sy);
+                sz = p_fma(wi[kp], tz, sz);
+            } else {
+                if (TESTS) {
+                    rinv.x = ea ? 0.f : rinv.x;
+                    rinv.y = eb ? 0.f : rinv.y;
+                }
+                const float2 rinv2 = p_mul(rinv, rinv);
+                const float2 dot = p_fma(dx, fjx, p_fma(dy, fjy, p_mul(dz, fjz)));
+                const float2 sc = p_mul(dot, rinv2);
+                ax[kp] = p_fma(rinv, p_fma(dx, sc, fjx), ax[kp]);
+                ay[kp] = p_fma(rinv, p_fma(dy, sc, fjy), ay[kp]);
+                az[kp] = p_fma(rinv, p_fma(dz, sc, fjz), az[kp]);
+                const float2 doti = p_fma(dx, fxi[kp], p_fma(dy, fyi[kp], p_mul(dz, fzi[kp])));
+                const float2 sci = p_mul(doti, rinv2);
+                sx = p_fma(rinv, p_fma(dx, sci, fxi[kp]), sx);
+                sy = p_fma(rinv, p_fma(dy, sci, fyi[kp]), sy);
+                sz = p_fma(rinv, p_fma(dz, sci, fzi[kp]), sz);
+            }
+        }
+        if (TESTS) {
+            bool any = false;
+#pragma unroll
+            for (int k = 0; k < IPT; ++k) any |= ex[k];
+            if (__any_sync(0xffffffffu, any)) {  // rare: exact FP64 terms
+                had_exact = true;
+                const int jo = CI[jj];
+                const int jl = J * B + jo;  // packed position of j
+                if (any && jo >= 0 && jl < v.n) {
+                    const int j = a.perm[jl];
+                    double ex_ = 0.0, ey_ = 0.0, ez_ = 0.0;
+#pragma unroll
+                    for (int k = 0; k < IPT; ++k) {
+                        const int il = I * B + k * SYM_T + tid;
+                        if (ex[k] && il < v.n) {
+                            const int i = a.perm[il];
+                            const double3 w1 = FORCE ? near_force_fp64(i, j, a.s.m, PER ? 1 : 0, inv_ell, v.L)
+                                                     : near_oseen_fp64(i, j, a.s.m, PER ? 1 : 0, inv_ell,
+                                                                       fscale_inv, v.L);
+                            const double sg = FORCE ? -1.0 : 1.0;  // the force i side is held negated
+                            fold_double(hx[k], lx[k], sg * w1.x);
+                            fold_double(hy[k], ly[k], sg * w1.y);
+                            fold_double(hz[k], lz[k], sg * w1.z);
+                            if (!diag) {
+                                const double3 w2 = FORCE ? near_force_fp64(j, i, a.s.m, PER ? 1 : 0, inv_ell, v.L)
+                                                         : near_oseen_fp64(j, i, a.s.m, PER ? 1 : 0, inv_ell,
+                                                                           fscale_inv, v.L);
+                                ex_ += w2.x;
+                                ey_ += w2.y;
+                                ez_ += w2.z;
+                            }
+                        }
+                    }
+                    if (!diag) {
+                        jnear[warp][0][u] += ex_;
+                        jnear[warp][1][u] += ey_;
+                        jnear[warp][2][u] += ez_;
+                    }
+                }
+            }
+        }
+        {  // pass the running j-side sum to lane - 1
+            const int src = (lane + 1) & 31;
+            sx.x = __shfl_sync(0xffffffffu, sx.x, src);
+            sx.y = __shfl_sync(0xffffffffu, sx.y, src);
+            sy.x = __shfl_sync(0xffffffffu, sy.x, src);
+            sy.y = __shfl_sync(0xffffffffu, sy.y, src);
+            sz.x = __shfl_sync(0xffffffffu, sz.x, src);
+            sz.y = __shfl_sync(0xffffffffu, sz.y, src);
+        }
+    }
+}
+
+template <int IPT, bool PER, bool FORCE>
+__global__ void __launch_bounds__(SYM_T, 4) mixed_sym_sorted_kernel(const SortedArgs a) {
+    static_assert(IPT % 2 == 0, "two i's per packed operation");
+    constexpr int B = SYM_T * IPT;
+    constexpr int KP = IPT / 2;
+    constexpr int CAP = B + SORTED_PAD;
+    constexpr int NW = SYM_T / 32;
+    extern __shared__ __align__(128) unsigned char sorted_smem[];
+    float4 *C0 = reinterpret_cast<float4 *>(sorted_smem);
+    float4 *C1 = C0 + CAP;
+    float4 *C2 = C1 + CAP;  // convection only
+    float2 *C3 = reinterpret_cast<float2 *>(C2 + (FORCE ? 0 : CAP));
+    int *CI = reinterpret_cast<int *>(C3 + CAP);  // list entry -> j within block J (-1: padding entry)
+    __shared__ double jsum[NW][3][TJ];            // j-side sums of the chunk's list slots, per warp
+    __shared__ double jnear[NW][3][32];           // exact j-side terms of the current sub-tile, per warp
+    __shared__ int wcnt[IPT][NW][3];              // entries per round, warp and class
+
+    const int nitems = a.s.t.items_total;
+    if ((int)blockIdx.x >= nitems) return;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int c = tid; c < NW * 3 * 32; c += SYM_T) (&jnear[0][0][0])[c] = 0.0;
+    const size_t plane = (size_t)B;
+    const unsigned lt = (1u << lane) - 1u;
+
+    for (int q = blockIdx.x; q < nitems; q += gridDim.x) {
+        int ql, I, J;
+        const BoxView v = item_box(a.s.t, B, q, ql);
+        decode_item(ql, v.nbk, I, J);
+        const bool diag = (I == J);
+        const double inv_ell = pow2_inv_of(v.sc[0]);
+        const double fscale_inv = FORCE ? 1.0 : pow2_inv_of(v.sc[1]);
+        const float Ls = (float)(v.L * inv_ell);
+        const float invLs = (float)(1.0 / (v.L * inv_ell));
+        const float2 invL2 = dup2(invLs);
+        const float2 nL2 = dup2(-Ls);
+        const float2 magic2 = dup2(RINT_MAGIC), nmagic2 = dup2(-RINT_MAGIC);
+        const float hm = (float)(v.L * inv_ell * (0.5 - MIC_MARGIN));
+        // fast intervals and the bitmap check keep another MIC_MARGIN from the pair test's margin
+        // (FP32 rounding of the bounds and bins is ~2^-22 L)
+        const float hm_fast = (float)(v.L * inv_ell * (0.5 - 2.0 * MIC_MARGIN));
+        const float m_amb = (float)(v.L * inv_ell * 2.0 * MIC_MARGIN);
+
+        // ---- the lists of block J against block I: count per class, then write ----
+        const float4 blo = a.bounds[2 * I], bhi = a.bounds[2 * I + 1];
+        const uint32_t *occ = a.occ + (size_t)I * 3 * AMB_WORDS;
+        auto load_entry = [&](int p, float4 &A, float4 &Bv, float4 &Q, float2 &S3) {
+            A = a.s.p0[p];
+            Bv = a.s.p1[p];
+            Q = FORCE ? make_float4(0.f, 0.f, 0.f, 0.f) : a.s.q0[p];
+            S3 = FORCE ? a.s.k2[p] : a.s.q1[p];
+        };
+        auto class_of = [&](const float4 &A, const float4 &Bv, const float2 &S3, float sc[3]) {
+            sc[0] = A.x;
+            sc[1] = A.z;
+            sc[2] = Bv.x;
+            if (diag) return (int)CLS_SLOW;
+            return classify_j<PER>(sc, FORCE ? S3.x : Bv.z, blo, bhi, occ, Ls, invLs, hm_fast, m_amb);
+        };
+#pragma unroll 1
+        for (int k = 0; k < IPT; ++k) {
+            float4 A, Bv, Q;
+            float2 S3;
+            float sc[3];
+            load_entry(v.p0 + J * B + k * SYM_T + tid, A, Bv, Q, S3);
+            const int cls = class_of(A, Bv, S3, sc);
+            const unsigned bf = __ballot_sync(0xffffffffu, cls == CLS_FAST);
+            const unsigned bm = __ballot_sync(0xffffffffu, cls == CLS_MEDIUM);
+            if (lane == 0) {
+                wcnt[k][warp][0] = __popc(bf);
+                wcnt[k][warp][1] = __popc(bm);
+                wcnt[k][warp][2] = 32 - __popc(bf) - __popc(bm);
+            }
+        }
+        __syncthreads();
+        int tot[3] = {0, 0, 0};
+        for (int k = 0; k < IPT; ++k)
+            for (int w = 0; w < NW; ++w)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) tot[c] += wcnt[k][w][c];
+        const int nf_pad = (tot[0] + 31) & ~31, nm_pad = (tot[1] + 31) & ~31, ns_pad = (tot[2] + 31) & ~31;
+        int run[3] = {0, 0, 0};  // entries of each class in the rounds before k
+#pragma unroll 1
+        for (int k = 0; k < IPT; ++k) {
+            float4 A, Bv, Q;
+            float2 S3;
+            float sc[3];
+            const int jb = k * SYM_T + tid;
+            load_entry(v.p0 + J * B + jb, A, Bv, Q, S3);
+            const int cls = class_of(A, Bv, S3, sc);
+            const unsigned bf = __ballot_sync(0xffffffffu, cls == CLS_FAST);
+            const unsigned bm = __ballot_sync(0xffffffffu, cls == CLS_MEDIUM);
+            const unsigned bs = ~(bf | bm);
+            // this thread's run: base of its class's region + entries of its class before it
+            const bool isf = cls == CLS_FAST, ism = cls == CLS_MEDIUM;
+            int e = isf ? run[0] : (ism ? nf_pad + run[1] : nf_pad + nm_pad + run[2]);
+            const int cc = isf ? 0 : (ism ? 1 : 2);
+            for (int w = 0; w < warp; ++w) e += wcnt[k][w][cc];
+            e += __popc((isf ? bf : (ism ? bm : bs)) & lt);
+            if (cls == CLS_FAST) {
+                A = make_float4(sc[0], sc[0], sc[1], sc[1]);
+                Bv.x = Bv.y = sc[2];
+            }
+            C0[e] = A;
+            C1[e] = Bv;
+            if (!FORCE) C2[e] = Q;
+            C3[e] = S3;
+            CI[e] = jb;
+            for (int w = 0; w < NW; ++w)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) run[c] += wcnt[k][w][c];
+        }
+        // padding of the three runs: zero weight; the fast run's padding lies far from every droplet
+        if (tid < 96) {
+            const int c = tid >> 5, o = tid & 31;
+            const int start = (c == 0 ? tot[0] : (c == 1 ? nf_pad + tot[1] : nf_pad + nm_pad + tot[2])) + o;
+            const int end = c == 0 ? nf_pad : (c == 1 ? nf_pad + nm_pad : nf_pad + nm_pad + ns_pad);
+            if (start < end) {
+                const float f = c == 0 ? SORTED_FAR : 0.f;
+                C0[start] = make_float4(f, f, f, f);
+                C1[start] = make_float4(f, f, 0.f, 0.f);
+                if (!FORCE) C2[start] = make_float4(0.f, 0.f, 0.f, 0.f);
+                C3[start] = make_float2(0.f, 0.f);
+                CI[start] = -1;
+            }
+        }
+
+        // ---- i state, two i's per packed register: k = 2 kp (.x) and 2 kp + 1 (.y) ----
+        float2 xi[KP], yi[KP], zi[KP], ki[KP], wi[KP];
+        float2 fxi[KP], fyi[KP], fzi[KP];
+        float2 ax[KP], ay[KP], az[KP];
+        float hx[IPT], hy[IPT], hz[IPT], lx[IPT], ly[IPT], lz[IPT];
+#pragma unroll
+        for (int kp = 0; kp < KP; ++kp) {
+            const int ia = v.p0 + I * B + (2 * kp) * SYM_T + tid, ib = ia + SYM_T;
+            const float4 a0 = a.s.p0[ia], b0 = a.s.p0[ib], a1 = a.s.p1[ia], b1 = a.s.p1[ib];
+            xi[kp] = make_float2(-a0.x, -b0.x);
+            yi[kp] = make_float2(-a0.z, -b0.z);
+            zi[kp] = make_float2(-a1.x, -b1.x);
+            if (FORCE) {
+                wi[kp] = make_float2(a1.z, b1.z);
+                ki[kp] = make_float2(a.s.k2[ia].x, a.s.k2[ib].x);
+            } else {
+                ki[kp] = make_float2(a1.z, b1.z);
+                const float4 fa = a.s.q0[ia], fb = a.s.q0[ib];
+                fxi[kp] = make_float2(fa.x, fb.x);
+                fyi[kp] = make_float2(fa.z, fb.z);
+                fzi[kp] = make_float2(a.s.q1[ia].x, a.s.q1[ib].x);
+            }
+            ax[kp] = ay[kp] = az[kp] = make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) hx[k] = hy[k] = hz[k] = lx[k] = ly[k] = lz[k] = 0.f;
+        __syncthreads();  // the lists are complete (and wcnt may be rewritten by the next item)
+
+        const int nfs = nf_pad >> 5, nms = nm_pad >> 5, nsub = nfs + nms + (ns_pad >> 5);
+        double *PJ = a.s.pj + (size_t)q * 3 * plane;
+        for (int c0 = 0; c0 < nsub; c0 += TJ / 32) {
+            const int c1 = min(c0 + TJ / 32, nsub);
+            for (int sub = c0; sub < c1; ++sub) {
+                float2 sx = make_float2(0.f, 0.f), sy = sx, sz = sx;
+                bool had_exact = false;
+#define DEM_SORTED_SUBTILE(MODE)                                                                                    \
+    sorted_subtile<IPT, PER, FORCE, MODE>(a, C0, C1, C2, C3, CI, 32 * sub, lane, tid, warp, I, J, diag, v, inv_ell, \
+                                          fscale_inv, invL2, magic2, nmagic2, nL2, hm, xi, yi, zi, ki, wi, fxi, fyi, \
+                                          fzi, ax, ay, az, hx, hy, hz, lx, ly, lz, jnear, sx, sy, sz, had_exact)
+                if (sub < nfs)
+                    DEM_SORTED_SUBTILE(CLS_FAST);
+                else if (sub < nfs + nms)
+                    DEM_SORTED_SUBTILE(CLS_MEDIUM);
+                else
+                    DEM_SORTED_SUBTILE(CLS_SLOW);
+#undef DEM_SORTED_SUBTILE
+                if (!diag) {  // the sums are back with the lanes owning their list entries
+                    double vx = (double)(sx.x + sx.y), vy = (double)(sy.x + sy.y), vz = (double)(sz.x + sz.y);
+                    if (had_exact) {  // warp-uniform: this sub-tile left exact j-side terms in jnear
+                        __syncwarp();
+                        vx += jnear[warp][0][lane];
+                        vy += jnear[warp][1][lane];
+                        vz += jnear[warp][2][lane];
+                        jnear[warp][0][lane] = jnear[warp][1][lane] = jnear[warp][2][lane] = 0.0;
+                        __syncwarp();
+                    }
+                    const int slot = (sub - c0) * 32 + lane;
+                    jsum[warp][0][slot] = vx;
+                    jsum[warp][1][slot] = vy;
+                    jsum[warp][2][slot] = vz;
+                }
+                if ((sub & 1) || sub == nsub - 1) {  // fold the FP32 i-side runs every 64 j and at the end
+#pragma unroll
+                    for (int kp = 0; kp < KP; ++kp) {
+                        two_sum_fold(hx[2 * kp], lx[2 * kp], ax[kp].x);
+                        two_sum_fold(hx[2 * kp + 1], lx[2 * kp + 1], ax[kp].y);
+                        two_sum_fold(hy[2 * kp], ly[2 * kp], ay[kp].x);
+                        two_sum_fold(hy[2 * kp + 1], ly[2 * kp + 1], ay[kp].y);
+                        two_sum_fold(hz[2 * kp], lz[2 * kp], az[kp].x);
+                        two_sum_fold(hz[2 * kp + 1], lz[2 * kp + 1], az[kp].y);
+                        ax[kp] = ay[kp] = az[kp] = make_float2(0.f, 0.f);
+                    }
+                }
+            }
+            __syncthreads();
+            if (!diag) {  // combine the warps in a fixed order, per list slot, into the j's partial
+                const int sub = c0 + (tid >> 5);
+                if (sub < c1) {
+                    const int jo = CI[32 * sub + (tid & 31)];
+                    if (jo >= 0) {
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            double w = 0.0;
+#pragma unroll
+                            for (int wp = 0; wp < NW; ++wp) w += jsum[wp][c][tid];
+                            PJ[c * plane + jo] = w;
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        double *PI = a.s.pi + (size_t)q * 3 * plane;
+        const double sg = FORCE ? -1.0 : 1.0;
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) {
+            const int li = k * SYM_T + tid;
+            PI[li] = sg * ((double)hx[k] + (double)lx[k]);
+            PI[plane + li] = sg * ((double)hy[k] + (double)ly[k]);
+            PI[2 * plane + li] = sg * ((double)hz[k] + (double)lz[k]);
+        }
+    }
+}
+
+// Per block of the packed layout: the bins of its stored coordinates that hold a droplet, per axis.
+__global__ void sorted_occupancy_kernel(int B, double L, const unsigned long long *__restrict__ scales,
+                                        const float4 *__restrict__ p0, const float4 *__restrict__ p1,
+                                        uint32_t *__restrict__ occ) {
+    const double inv_ell = pow2_inv_of(scales[0]);
+    const float Ls = (float)(L * inv_ell), invLs = (float)(1.0 / (L * inv_ell));
+    uint32_t *o = occ + (size_t)blockIdx.x * 3 * AMB_WORDS;
+    for (int l = threadIdx.x; l < B; l += blockDim.x) {
+        const int p = blockIdx.x * B + l;
+        const float4 A = p0[p], Bv = p1[p];
+        const float v[3] = {A.x, A.z, Bv.x};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const int b = amb_bin(v[c], Ls, invLs);
+            atomicOr(&o[c * AMB_WORDS + (b >> 5)], 1u << (b & 31));
+        }
+    }
+}
+
+// Per block of the packed layout: bounds of the stored coordinates and the largest k r.
+template <bool FORCE>
+__global__ void __launch_bounds__(SYM_T) sorted_bounds_kernel(int B, const float4 *__restrict__ p0,
+                                                              const float4 *__restrict__ p1,
+                                                              const float2 *__restrict__ k2,
+                                                              float4 *__restrict__ bounds) {
+    __shared__ float red[7][SYM_T / 32];
+    float mn[3] = {3.0e38f, 3.0e38f, 3.0e38f}, mx[3] = {-3.0e38f, -3.0e38f, -3.0e38f}, km = 0.f;
+    for (int l = threadIdx.x; l < B; l += SYM_T) {
+        const int p = blockIdx.x * B + l;
+        const float4 A = p0[p], Bv = p1[p];
+        const float v[3] = {A.x, A.z, Bv.x};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            mn[c] = fminf(mn[c], v[c]);
+            mx[c] = fmaxf(mx[c], v[c]);
+        }
+        km = fmaxf(km, FORCE ? k2[p].x : Bv.z);
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            mn[c] = fminf(mn[c], __shfl_xor_sync(0xffffffffu, mn[c], o));
+            mx[c] = fmaxf(mx[c], __shfl_xor_sync(0xffffffffu, mx[c], o));
+        }
+        km = fmaxf(km, __shfl_xor_sync(0xffffffffu, km, o));
+    }
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        for (int c = 0; c < 3; ++c) {
+            red[c][w] = mn[c];
+            red[3 + c][w] = mx[c];
+        }
+        red[6][w] = km;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int ww = 1; ww < SYM_T / 32; ++ww) {
+            for (int c = 0; c < 3; ++c) {
+                red[c][0] = fminf(red[c][0], red[c][ww]);
+                red[3 + c][0] = fmaxf(red[3 + c][0], red[3 + c][ww]);
+            }
+            red[6][0] = fmaxf(red[6][0], red[6][ww]);
+        }
+        bounds[2 * blockIdx.x] = make_float4(red[0][0], red[1][0], red[2][0], red[6][0]);
+        bounds[2 * blockIdx.x + 1] = make_float4(red[3][0], red[4][0], red[5][0], 0.f);
+    }
+}
+
 // Packed, zero-padded layout of the symmetric passes (see SymArgs).
 template <bool FORCE>
 __global__ void prep_sym_kernel(const SymBoxes t, const double *__restrict__ x, const double *__restrict__ y,
                                 const double *__restrict__ z, const double *__restrict__ r,
                                 const double *__restrict__ fx, const double *__restrict__ fy,
-                                const double *__restrict__ fz, double k_near, float4 *__restrict__ p0,
-                                float4 *__restrict__ p1, float4 *__restrict__ q0, float2 *__restrict__ k2q1) {
+                                const double *__restrict__ fz, double k_near, const int32_t *__restrict__ perm,
+                                float4 *__restrict__ p0, float4 *__restrict__ p1, float4 *__restrict__ q0,
+                                float2 *__restrict__ k2q1) {
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < t.npad_total; p += gridDim.x * blockDim.x) {
         int o0 = 0, nb = t.n1, pb = 0;
         double L = t.L1;
@@ -436,7 +995,7 @@ __global__ void prep_sym_kernel(const SymBoxes t, const double *__restrict__ x, 
         const int l = p - pb;
         float X = 0.f, Y = 0.f, Z = 0.f, W = 0.f, K = 0.f, Fx = 0.f, Fy = 0.f, Fz = 0.f;
         if (l < nb) {
-            const int i = o0 + l;
+            const int i = perm ? perm[l] : o0 + l;  // perm: one box in Morton order
             const double s = pow2_inv_of(sc[0]);
             const double center = 0.5 * L;
             const double rs = r[i] * s;
@@ -469,8 +1028,10 @@ __global__ void prep_sym_kernel(const SymBoxes t, const double *__restrict__ x, 
 template <bool FORCE>
 __global__ void reduce_sym_kernel(const SymBoxes t, int B, const double *__restrict__ pi, const double *__restrict__ pj,
                                   const double *__restrict__ r, double coeff, double *__restrict__ ox,
-                                  double *__restrict__ oy, double *__restrict__ oz, uint32_t *err) {
+                                  double *__restrict__ oy, double *__restrict__ oz, uint32_t *err,
+                                  const int32_t *__restrict__ perm) {
     const size_t plane = (size_t)B;
+    // d: position in the packed layout; with perm (one box in Morton order) its droplet is perm[d]
     for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < t.n_total; d += gridDim.x * blockDim.x) {
         int o0 = 0, nbk = t.npad1 / B, ib = 0;
         const unsigned long long *sc = t.scales1;
@@ -511,19 +1072,20 @@ __global__ void reduce_sym_kernel(const SymBoxes t, int B, const double *__restr
             }
         }
         const double s = pow2_inv_of(sc[0]);
+        const int od = perm ? perm[d] : d;
         double f;
         if (FORCE) {
             const double ell = 1.0 / s;
-            const double rs = r[d] * s;
+            const double rs = r[od] * s;
             f = coeff * ipow3(rs) * ell * ell;
         } else {
             f = coeff * s / pow2_inv_of(sc[1]);
         }
         const double vx = f * sx, vy = f * sy, vz = f * sz;
         if (!(isfinite(vx) && isfinite(vy) && isfinite(vz))) raise_device_error(err, DEM_DEVERR_NONFINITE);
-        ox[d] = vx;
-        oy[d] = vy;
-        oz[d] = vz;
+        ox[od] = vx;
+        oy[od] = vy;
+        oz[od] = vz;
     }
 }
 
@@ -586,11 +1148,97 @@ size_t sym_workspace_bytes(long long npad_total, long long items_total, int B) {
     return align256((size_t)npad_total * 64) + (size_t)(2 * items_total * 3 * (long long)B) * sizeof(double);
 }
 
-// Workspace bytes of the symmetric schedule for one box of n droplets.
+// Workspace bytes of the symmetric schedule for one box of n droplets: the
+// packed layout and partial sums, plus the Morton order and the per-block
+// bounds of the sorted kernel.
 size_t sym_partial_bytes(int n, int ipt) {
     const long long B = (long long)SYM_T * ipt;
     const long long nb = (n + B - 1) / B;
-    return sym_workspace_bytes(nb * B, nb * (nb + 1) / 2, (int)B);
+    return sym_workspace_bytes(nb * B, nb * (nb + 1) / 2, (int)B) + align256(morton_ws_bytes(n > 0 ? n : 1)) +
+           align256((size_t)nb * 2 * sizeof(float4)) + (size_t)nb * 3 * AMB_WORDS * sizeof(uint32_t);
+}
+
+template <int IPT, bool PER, bool FORCE>
+static int launch_sorted(dem_ctx *ctx, const SortedArgs &a, int grid, cudaStream_t s) {
+    constexpr int smem = sorted_smem_bytes<IPT, FORCE>();
+    // the dynamic shared memory limit is raised once per device, on the first (eager) call
+    static bool attr_set[64] = {};
+    const int dev = ctx->device >= 0 && ctx->device < 64 ? ctx->device : 0;
+    if (!attr_set[dev]) {
+        int rc = dem_check_cuda(ctx, cudaFuncSetAttribute(mixed_sym_sorted_kernel<IPT, PER, FORCE>,
+                                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                                "sorted pass: shared memory attribute");
+        if (rc) return rc;
+        attr_set[dev] = true;
+    }
+    mixed_sym_sorted_kernel<IPT, PER, FORCE><<<grid, SYM_T, smem, counted(s)>>>(a);
+    return DEM_OK;
+}
+
+// One box, droplets in Morton order: sort, pack, per-block bounds, the pair
+// kernel with fast and slow lists, then the fixed-order reduction through the
+// permutation.
+template <bool FORCE>
+static int run_sym_sorted(dem_ctx *ctx, const SymBoxes &t, int ipt, bool per, const MixedArgs &m, double *work,
+                          double coeff, double *ox, double *oy, double *oz, cudaStream_t s) {
+    const int B = SYM_T * ipt;
+    const int n = t.n_total;
+    const int nb = t.npad_total / B;
+    if (n == 0) return DEM_OK;
+    char *base = reinterpret_cast<char *>(work);
+    const size_t np = (size_t)t.npad_total;
+    float4 *p0 = reinterpret_cast<float4 *>(base);
+    float4 *p1 = p0 + np;
+    float4 *q0 = p1 + np;
+    float2 *k2q1 = reinterpret_cast<float2 *>(q0 + np);
+    double *pi = reinterpret_cast<double *>(base + align256(np * 64));
+    double *pj = pi + (size_t)t.items_total * 3 * B;
+    char *extra = base + sym_workspace_bytes(t.npad_total, t.items_total, B);
+    const MortonWs mw = morton_ws_carve(extra, n);
+    float4 *bounds = reinterpret_cast<float4 *>(extra + align256(morton_ws_bytes(n)));
+    uint32_t *occ = reinterpret_cast<uint32_t *>(extra + align256(morton_ws_bytes(n)) +
+                                                 align256((size_t)nb * 2 * sizeof(float4)));
+    int rc = morton_order(ctx, n, m.x, m.y, m.z, per ? 1 : 0, m.L, mw, s);
+    if (rc) return rc;
+    const int32_t *perm = mw.idx[0];
+    const int pgrid = max(1, min(ceil_div(t.npad_total, 256), 4 * ctx->sm_count));
+    prep_sym_kernel<FORCE><<<pgrid, 256, 0, counted(s)>>>(t, m.x, m.y, m.z, m.r, m.fx, m.fy, m.fz,
+                                                          FORCE ? ctx->tuning.near_force : ctx->tuning.near_oseen,
+                                                          perm, p0, p1, q0, k2q1);
+    sorted_bounds_kernel<FORCE><<<nb, SYM_T, 0, counted(s)>>>(B, p0, p1, k2q1, bounds);
+    if (per) {
+        rc = dem_check_cuda(ctx, cudaMemsetAsync(occ, 0, (size_t)nb * 3 * AMB_WORDS * sizeof(uint32_t), s), "memset");
+        if (rc) return rc;
+        sorted_occupancy_kernel<<<nb, SYM_T, 0, counted(s)>>>(B, m.L, m.scales, p0, p1, occ);
+    }
+    rc = dem_check_launch(ctx, "sorted pass prep");
+    if (rc) return rc;
+    SortedArgs a;
+    a.s.t = t;
+    a.s.p0 = p0;
+    a.s.p1 = p1;
+    a.s.q0 = q0;
+    a.s.k2 = k2q1;
+    a.s.q1 = k2q1;
+    a.s.m = m;
+    a.s.pi = pi;
+    a.s.pj = pj;
+    a.perm = perm;
+    a.bounds = bounds;
+    a.occ = occ;
+    const int grid = t.items_total;
+    dem_prof_begin(ctx, FORCE ? "mixed_force_pass" : "mixed_convection_pass", s);
+    if (ipt == 4)
+        rc = per ? launch_sorted<4, true, FORCE>(ctx, a, grid, s) : launch_sorted<4, false, FORCE>(ctx, a, grid, s);
+    else
+        rc = per ? launch_sorted<2, true, FORCE>(ctx, a, grid, s) : launch_sorted<2, false, FORCE>(ctx, a, grid, s);
+    dem_prof_end(ctx, s);
+    if (rc) return rc;
+    rc = dem_check_launch(ctx, FORCE ? "mixed force (symmetric, Morton order)" : "mixed convection (symmetric, Morton order)");
+    if (rc) return rc;
+    const int rgrid = max(1, min(ceil_div(n, 256), 4 * ctx->sm_count));
+    reduce_sym_kernel<FORCE><<<rgrid, 256, 0, counted(s)>>>(t, B, pi, pj, m.r, coeff, ox, oy, oz, m.err, perm);
+    return dem_check_launch(ctx, "mixed reduce (symmetric, Morton order)");
 }
 
 template <bool FORCE>
@@ -608,7 +1256,7 @@ int run_sym_boxes(dem_ctx *ctx, const SymBoxes &t, int ipt, int ctas, bool per, 
     const int pgrid = max(1, min(ceil_div(t.npad_total, 256), 4 * ctx->sm_count));
     prep_sym_kernel<FORCE><<<pgrid, 256, 0, counted(s)>>>(t, m.x, m.y, m.z, m.r, m.fx, m.fy, m.fz,
                                                           FORCE ? ctx->tuning.near_force : ctx->tuning.near_oseen,
-                                                          p0, p1, q0, k2q1);
+                                                          nullptr, p0, p1, q0, k2q1);
     SymArgs a;
     a.t = t;
     a.p0 = p0;
@@ -629,7 +1277,8 @@ int run_sym_boxes(dem_ctx *ctx, const SymBoxes &t, int ipt, int ctas, bool per, 
     int rc = dem_check_launch(ctx, FORCE ? "mixed force (symmetric)" : "mixed convection (symmetric)");
     if (rc) return rc;
     const int rgrid = max(1, min(ceil_div(t.n_total, 256), 4 * ctx->sm_count));
-    reduce_sym_kernel<FORCE><<<rgrid, 256, 0, counted(s)>>>(t, B, a.pi, a.pj, m.r, coeff, ox, oy, oz, m.err);
+    reduce_sym_kernel<FORCE><<<rgrid, 256, 0, counted(s)>>>(t, B, a.pi, a.pj, m.r, coeff, ox, oy, oz, m.err,
+                                                            nullptr);
     return dem_check_launch(ctx, "mixed reduce (symmetric)");
 }
 
@@ -657,7 +1306,9 @@ int run_sym_pass(dem_ctx *ctx, int n, int ipt, bool per, const MixedArgs &m, dou
     t.scales1 = m.scales;
     MixedArgs mm = m;
     mm.r = r;
-    return run_sym_boxes<FORCE>(ctx, t, ipt, 0, per, mm, work, coeff, ox, oy, oz, s);
+    if (ctx->tuning.schedule == DEM_SCHED_SYMMETRIC_PLAIN)
+        return run_sym_boxes<FORCE>(ctx, t, ipt, 0, per, mm, work, coeff, ox, oy, oz, s);
+    return run_sym_sorted<FORCE>(ctx, t, ipt, per, mm, work, coeff, ox, oy, oz, s);
 }
 
 template int run_sym_pass<true>(dem_ctx *, int, int, bool, const MixedArgs &, double *, const double *, double,

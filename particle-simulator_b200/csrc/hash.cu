@@ -129,13 +129,29 @@ __device__ __forceinline__ bool contact_rn(double d2, double s) {
 
 // Visits every candidate j > i of droplet i (the distinct buckets of its 27
 // neighbour cells) and calls f(j, multiplicity) for those in contact.
-template <typename F>
-__device__ __forceinline__ void for_each_contact(int i, const double *__restrict__ x, const double *__restrict__ y,
-                                                 const double *__restrict__ z, const double *__restrict__ r,
+// PACKED: the droplets' (x, y), (z, r) in bucket order are in P (two double2
+// per bucket slot, slot ti holding droplet i), so a bucket's candidates are
+// read as contiguous 32-byte records instead of four scattered gathers.
+template <bool PACKED, typename F>
+__device__ __forceinline__ void for_each_contact(int i, int ti, const double *__restrict__ x,
+                                                 const double *__restrict__ y, const double *__restrict__ z,
+                                                 const double *__restrict__ r, const double2 *__restrict__ P,
                                                  const HashParams &p, int periodic, double L, double halfL,
                                                  int32_t mask, int n, const int32_t *__restrict__ bstart,
                                                  const int32_t *__restrict__ sorted_idx, F &&f) {
-    const double xi = x[i], yi = y[i], zi = z[i], ri = r[i];
+    double xi, yi, zi, ri;
+    if (PACKED) {
+        const double2 a = P[2 * ti], b = P[2 * ti + 1];
+        xi = a.x;
+        yi = a.y;
+        zi = b.x;
+        ri = b.y;
+    } else {
+        xi = x[i];
+        yi = y[i];
+        zi = z[i];
+        ri = r[i];
+    }
     const int32_t cx = cell_coord(xi, p.cell, p.grid, periodic);
     const int32_t cy = cell_coord(yi, p.cell, p.grid, periodic);
     const int32_t cz = cell_coord(zi, p.cell, p.grid, periodic);
@@ -147,6 +163,16 @@ __device__ __forceinline__ void for_each_contact(int i, const double *__restrict
             dz = mic64(dz, L, halfL);
         }
         if (contact_rn(dx * dx + dy * dy + dz * dz, ri + rj)) f(j, m);  // dist <= r_i + r_j
+    };
+    auto candidate = [&](int32_t s, int m) {
+        const int32_t j = sorted_idx[s];
+        if (!(i < j)) return;
+        if (PACKED) {
+            const double2 a = P[2 * s], b = P[2 * s + 1];
+            bucket(a.x, a.y, b.x, b.y, j, m);
+        } else {
+            bucket(x[j], y[j], z[j], r[j], j, m);
+        }
     };
     // Neighbour cell c = 9 (di + 1) + 3 (dj + 1) + (dk + 1): its bucket, or -1 outside an open box.
     auto cell_hash = [&](int c) -> int32_t {
@@ -177,11 +203,7 @@ __device__ __forceinline__ void for_each_contact(int i, const double *__restrict
                 const int32_t start = bstart[hc];
                 int32_t end = bstart[hc + 1];
                 if (end > n) end = n;  // :199-201
-                for (int32_t s = start; s < end; ++s) {
-                    const int32_t j = sorted_idx[s];
-                    if (!(i < j)) continue;
-                    bucket(x[j], y[j], z[j], r[j], j, 1);
-                }
+                for (int32_t s = start; s < end; ++s) candidate(s, 1);
             }
             return;
         }
@@ -217,38 +239,52 @@ __device__ __forceinline__ void for_each_contact(int i, const double *__restrict
         const int32_t start = bstart[hs[q]];
         int32_t end = bstart[hs[q] + 1];
         if (end > n) end = n;  // :199-201
-        for (int32_t s = start; s < end; ++s) {
-            const int32_t j = sorted_idx[s];
-            if (!(i < j)) continue;
-            bucket(x[j], y[j], z[j], r[j], j, mult[q]);
-        }
+        for (int32_t s = start; s < end; ++s) candidate(s, mult[q]);
     }
 }
 
+// The droplets' positions and radii in bucket order: P[2 s] = (x, y), P[2 s + 1] = (z, r) of sorted_idx[s].
+__global__ void bucket_positions_kernel(int n, const double *__restrict__ x, const double *__restrict__ y,
+                                        const double *__restrict__ z, const double *__restrict__ r,
+                                        const HashParams *__restrict__ hp, const int32_t *__restrict__ sorted_idx,
+                                        double2 *__restrict__ P) {
+    if (!hp->valid) return;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        const int j = sorted_idx[s];
+        P[2 * s] = make_double2(x[j], y[j]);
+        P[2 * s + 1] = make_double2(z[j], r[j]);
+    }
+}
+
+template <bool PACKED>
 __global__ void count_pairs_kernel(int n, const double *__restrict__ x, const double *__restrict__ y,
                                    const double *__restrict__ z, const double *__restrict__ r,
-                                   const HashParams *__restrict__ hp, int periodic, double L, int32_t mask,
-                                   const int32_t *__restrict__ bstart, const int32_t *__restrict__ sorted_idx,
-                                   int32_t *__restrict__ pair_count, unsigned long long *__restrict__ raw) {
+                                   const double2 *__restrict__ P, const HashParams *__restrict__ hp, int periodic,
+                                   double L, int32_t mask, const int32_t *__restrict__ bstart,
+                                   const int32_t *__restrict__ sorted_idx, int32_t *__restrict__ pair_count,
+                                   unsigned long long *__restrict__ raw) {
     const HashParams p = *hp;
     unsigned long long local_raw = 0;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
         const int i = p.valid ? sorted_idx[t] : t;  // bucket order (the buckets are filled when valid)
         int32_t c = 0;
         if (p.valid) {
-            for_each_contact(i, x, y, z, r, p, periodic, L, 0.5 * L, mask, n, bstart, sorted_idx, [&](int32_t, int m) {
-                ++c;
-                local_raw += (unsigned long long)m;
-            });
+            for_each_contact<PACKED>(i, t, x, y, z, r, P, p, periodic, L, 0.5 * L, mask, n, bstart, sorted_idx,
+                                     [&](int32_t, int m) {
+                                         ++c;
+                                         local_raw += (unsigned long long)m;
+                                     });
         }
         pair_count[i] = c;
     }
     if (local_raw) atomicAdd(raw, local_raw);
 }
 
+template <bool PACKED>
 __global__ void write_pairs_kernel(int n, const double *__restrict__ x, const double *__restrict__ y,
                                    const double *__restrict__ z, const double *__restrict__ r,
-                                   const HashParams *__restrict__ hp, int periodic, double L, int32_t mask,
+                                   const double2 *__restrict__ P, const HashParams *__restrict__ hp, int periodic,
+                                   double L, int32_t mask,
                                    const int32_t *__restrict__ bstart, const int32_t *__restrict__ sorted_idx,
                                    const int64_t *__restrict__ offset, int32_t *__restrict__ pairs, int64_t cap,
                                    int64_t *__restrict__ counts, uint32_t *err) {
@@ -261,26 +297,30 @@ __global__ void write_pairs_kernel(int n, const double *__restrict__ x, const do
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
         const int i = sorted_idx[t];  // bucket order, as in count_pairs_kernel
         const int64_t o0 = offset[i], o1 = offset[i + 1];
-        if (o1 == o0) continue;
-        int64_t w = o0;
-        for_each_contact(i, x, y, z, r, p, periodic, L, 0.5 * L, mask, n, bstart, sorted_idx, [&](int32_t j, int) {
-            if (w < cap) {
-                pairs[2 * w] = i;
-                pairs[2 * w + 1] = j;
+        // the row's slots that fit in the buffer: all of them, except in the one row that the
+        // capacity cuts (o0 < cap < o1), and none in the rows after it
+        const int64_t m = (o1 < cap ? o1 : cap) - o0;
+        if (m <= 0) continue;
+        // ascending j within the row of droplet i: each j found is inserted into the sorted run
+        // pairs[o0 .. o0 + len); once the run holds m entries the largest drops out, so a cut row
+        // keeps its m smallest j and the buffer holds the lexicographically first cap pairs
+        int64_t len = 0;
+        for_each_contact<PACKED>(i, t, x, y, z, r, P, p, periodic, L, 0.5 * L, mask, n, bstart, sorted_idx,
+                                 [&](int32_t j, int) {
+            int64_t q;
+            if (len < m) {
+                pairs[2 * (o0 + len)] = i;
+                q = len++;
+            } else {
+                if (j >= pairs[2 * (o0 + m - 1) + 1]) return;
+                q = m - 1;
             }
-            ++w;
+            while (q > 0 && pairs[2 * (o0 + q - 1) + 1] > j) {
+                pairs[2 * (o0 + q) + 1] = pairs[2 * (o0 + q - 1) + 1];
+                --q;
+            }
+            pairs[2 * (o0 + q) + 1] = j;
         });
-        // ascending j within the row of droplet i (insertion sort of a short run)
-        const int64_t e = o1 < cap ? o1 : cap;
-        for (int64_t a = o0 + 1; a < e; ++a) {
-            const int32_t v = pairs[2 * a + 1];
-            int64_t b = a - 1;
-            while (b >= o0 && pairs[2 * b + 1] > v) {
-                pairs[2 * (b + 1) + 1] = pairs[2 * b + 1];
-                --b;
-            }
-            pairs[2 * (b + 1) + 1] = v;
-        }
     }
 }
 
@@ -324,15 +364,18 @@ int launch_hash_detect(dem_ctx *ctx, int n, const double *x, const double *y, co
                         "cursor copy");
     if (rc) return rc;
     scatter_kernel<<<grid, 256, 0, counted(s)>>>(n, ctx->cell_hash, hp, ctx->bucket_cursor, ctx->sorted_idx);
+    bucket_positions_kernel<<<grid, 256, 0, counted(s)>>>(n, x, y, z, r, hp, ctx->sorted_idx, ctx->hash_pos);
     const int dgrid = ceil_div(n, 128);
-    count_pairs_kernel<<<dgrid, 128, 0, counted(s)>>>(n, x, y, z, r, hp, periodic, L, mask, ctx->bucket_start, ctx->sorted_idx,
-                                             ctx->pair_count, reinterpret_cast<unsigned long long *>(counts + 1));
+    count_pairs_kernel<true><<<dgrid, 128, 0, counted(s)>>>(n, x, y, z, r, ctx->hash_pos, hp, periodic, L, mask,
+                                                            ctx->bucket_start, ctx->sorted_idx, ctx->pair_count,
+                                                            reinterpret_cast<unsigned long long *>(counts + 1));
     rc = dem_check_launch(ctx, "hash count");
     if (rc) return rc;
     rc = exclusive_scan<int32_t, int64_t>(ctx, ctx->pair_count, ctx->pair_offset, n, s);
     if (rc) return rc;
-    write_pairs_kernel<<<dgrid, 128, 0, counted(s)>>>(n, x, y, z, r, hp, periodic, L, mask, ctx->bucket_start, ctx->sorted_idx,
-                                             ctx->pair_offset, pairs, cap, counts, ctx->d_err);
+    write_pairs_kernel<true><<<dgrid, 128, 0, counted(s)>>>(n, x, y, z, r, ctx->hash_pos, hp, periodic, L, mask,
+                                                            ctx->bucket_start, ctx->sorted_idx, ctx->pair_offset,
+                                                            pairs, cap, counts, ctx->d_err);
     dem_prof_end(ctx, s);
     return dem_check_launch(ctx, "hash write");
 }
@@ -448,14 +491,16 @@ extern "C" int dem_hash_detect_noalloc(int n, const double *x, const double *y, 
         return DEM_E_CUDA;
     scatter_kernel<<<grid, 256, 0, counted(s)>>>(n, cell_hash, hp, bucket_cursor, sorted_idx);
     const int dgrid = ceil_div(n, 128);
-    count_pairs_kernel<<<dgrid, 128, 0, counted(s)>>>(n, x, y, z, r, hp, periodic, L, mask, bucket_start, sorted_idx,
-                                             pair_count, reinterpret_cast<unsigned long long *>(counts + 1));
+    count_pairs_kernel<false><<<dgrid, 128, 0, counted(s)>>>(n, x, y, z, r, nullptr, hp, periodic, L, mask,
+                                                             bucket_start, sorted_idx, pair_count,
+                                                             reinterpret_cast<unsigned long long *>(counts + 1));
     if (cudaGetLastError() != cudaSuccess) return DEM_E_CUDA;
     if (exclusive_scan_into<int32_t, int64_t>(pair_count, pair_offset, n, static_cast<int64_t *>(sums), s) !=
         cudaSuccess)
         return DEM_E_CUDA;
-    write_pairs_kernel<<<dgrid, 128, 0, counted(s)>>>(n, x, y, z, r, hp, periodic, L, mask, bucket_start, sorted_idx,
-                                             pair_offset, pairs, pair_capacity, counts, err);
+    write_pairs_kernel<false><<<dgrid, 128, 0, counted(s)>>>(n, x, y, z, r, nullptr, hp, periodic, L, mask,
+                                                             bucket_start, sorted_idx, pair_offset, pairs,
+                                                             pair_capacity, counts, err);
     return cudaGetLastError() == cudaSuccess ? DEM_OK : DEM_E_CUDA;
 }
 

@@ -30,7 +30,9 @@ PRECISIONS = {"fp64": PREC_FP64, "mixed": PREC_MIXED}
 SCHED_AUTO = 0
 SCHED_SPLIT = 1
 SCHED_SYMMETRIC = 2
-SCHEDULES = {"auto": SCHED_AUTO, "split": SCHED_SPLIT, "symmetric": SCHED_SYMMETRIC}
+SCHED_SYMMETRIC_PLAIN = 3
+SCHEDULES = {"auto": SCHED_AUTO, "split": SCHED_SPLIT, "symmetric": SCHED_SYMMETRIC,
+             "symmetric_plain": SCHED_SYMMETRIC_PLAIN}
 
 DEVERR_WAIT_TIMEOUT = 1
 DEVERR_PAIR_OVERFLOW = 2
@@ -41,6 +43,7 @@ DEVERR_NONFINITE = 8
 _i, _d, _vp, _i64 = C.c_int, C.c_double, C.c_void_p, C.c_int64
 SIGNATURES = {
     "dem_version": (C.c_char_p, []),
+    "dem_kernel_binary_version": (_i, [_i, C.POINTER(_i)]),
     "dem_launch_count": (C.c_ulonglong, []),
     "dem_count_replayed_launches": (None, [C.c_ulonglong]),
     "dem_ctx_create": (_i, [_i, _i, C.POINTER(_vp)]),
@@ -142,6 +145,16 @@ def exported_symbols():
 
 def version() -> str:
     return lib().dem_version().decode()
+
+
+def kernel_binary_version(device: int = 0) -> int:
+    """Binary version of the device code the runtime loads for this library's
+    kernels (100 for sm_100a); needs a CUDA device."""
+    v = _i()
+    rc = lib().dem_kernel_binary_version(int(device), C.byref(v))
+    if rc != DEM_OK:
+        raise RuntimeError(f"dem_kernel_binary_version failed ({rc})")
+    return v.value
 
 
 def launch_count() -> int:

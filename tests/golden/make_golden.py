@@ -4,7 +4,7 @@ classes (ddkx21/particle-simulator) through the Taichi stand-in in
 
 Run from the repository root, in a checkout where the reference is present:
 
-    python tests/golden/make_golden.py [--reference PATH]
+    python tests/golden/make_golden.py --reference PATH   (or DEM_REFERENCE=PATH)
 
 Every ``*.npz`` written next to this file holds the inputs, the parameters and
 the reference's outputs for one case.  Tests compare the C oracle and the CUDA
@@ -464,9 +464,12 @@ def gen_collfreq(R, out):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("DEM_REFERENCE", "/root/reference"))
+    ap.add_argument("--reference", default=os.environ.get("DEM_REFERENCE"),
+                    help="the reference checkout (default: $DEM_REFERENCE)")
     ap.add_argument("--only", default="")
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("name the reference checkout with --reference or DEM_REFERENCE")
     R = _import_reference(Path(args.reference))
     gens = dict(direct=gen_direct, hash=gen_hash, merge=gen_merge, solver=gen_solver, tree=gen_tree,
                 correction=gen_correction, collfreq=gen_collfreq)

@@ -16,8 +16,10 @@ import pytest
 from dem.periodic_correction import COMSOLLatticeCorrection
 from dem.periodic_correction.comsol_lattice_correction import DATA_ENV
 
-# the reference checkout (as for tests/golden/make_golden.py); absent on most machines
-REF_DATA = Path(os.environ.get("DEM_REFERENCE", "/root/reference")) / "dem" / "periodic_correction" / "data"
+# the reference checkout, named by DEM_REFERENCE (as for tests/golden/make_golden.py); the
+# test that reads its COMSOL data is skipped when the variable is unset
+_REF = os.environ.get("DEM_REFERENCE")
+REF_DATA = Path(_REF) / "dem" / "periodic_correction" / "data" if _REF else None
 
 
 @pytest.fixture(scope="module")
@@ -74,7 +76,8 @@ def test_load_default_needs_the_data(monkeypatch, tmp_path):
         COMSOLLatticeCorrection.load_default()
 
 
-@pytest.mark.skipif(not REF_DATA.exists(), reason="the reference's COMSOL data are not on this machine")
+@pytest.mark.skipif(REF_DATA is None or not REF_DATA.exists(),
+                    reason="DEM_REFERENCE does not name a reference checkout with its COMSOL data")
 def test_loader_reproduces_reference_grid(golden, monkeypatch):
     g = golden("corr_grid_comsol_r12.npz")
     import json

@@ -81,6 +81,7 @@ def test_mixed_against_fp64_oracle(n, seed):
 @pytest.mark.parametrize("ipt,threads,splits,schedule", [
     (1, 128, 0, "split"), (2, 256, 3, "split"), (4, 64, 1, "split"), (8, 128, 0, "split"), (4, 512, 7, "split"),
     (1, 0, 0, "symmetric"), (2, 0, 0, "symmetric"), (4, 0, 0, "symmetric"),
+    (2, 0, 0, "symmetric_plain"), (4, 0, 0, "symmetric_plain"),
 ])
 def test_mixed_tunings_agree_and_are_deterministic(ipt, threads, splits, schedule):
     pos, r, L = lognormal_state(3000, seed=2)
@@ -94,6 +95,36 @@ def test_mixed_tunings_agree_and_are_deterministic(ipt, threads, splits, schedul
     F_ref = O.direct_forces(pos, r, m, L, True)
     assert rel_norm(F1, F_ref) <= MIXED_NORM_TOL
     assert rel_norm(V1, O.direct_convection(pos, F_ref, eta, L, True)) <= MIXED_V_NORM_TOL
+
+
+@pytest.mark.parametrize("periodic,n", [(True, 20000), (False, 16384)])
+def test_symmetric_morton_blocks_against_oracle_and_plain_blocks(periodic, n):
+    """The symmetric schedule on Morton-ordered blocks (fast, medium and slow
+    j lists) against the oracle, and against the same schedule on blocks in
+    the caller's order: the same pairs go to FP64 in both, only the FP32
+    summation order differs."""
+    pos, r, L = lognormal_state(n, seed=11, periodic=periodic)
+    m, eta, _ = consts()
+    fc = _calc(n, L, periodic, precision="mixed")
+    fc.set_tuning(schedule="symmetric")
+    assert fc._ctx.plan(n, periodic)["schedule"] == "symmetric"
+    F, V = fc.calculate_forces_and_convection(pos, r)
+    F2, V2 = fc.calculate_forces_and_convection(pos, r)
+    np.testing.assert_array_equal(F, F2)  # deterministic
+    np.testing.assert_array_equal(V, V2)
+    rows = (0, 2048)
+    F_ref = O.direct_forces(pos, r, m, L, periodic)
+    V_ref = O.direct_convection(pos, F_ref, eta, L, periodic, rows=rows)[: rows[1]]
+    assert rel_norm(F, F_ref) <= MIXED_NORM_TOL
+    assert ref_metric(F, F_ref)[1] <= MIXED_PER_DROPLET_TOL
+    assert rel_norm(V[: rows[1]], V_ref) <= MIXED_V_NORM_TOL
+    assert ref_metric(V[: rows[1]], V_ref)[1] <= MIXED_V_PER_DROPLET_TOL
+    fc.set_tuning(schedule="symmetric_plain")
+    assert fc._ctx.plan(n, periodic)["schedule"] == "symmetric_plain"
+    Fp, Vp = fc.calculate_forces_and_convection(pos, r)
+    assert rel_norm(F, Fp) <= MIXED_NORM_TOL
+    assert rel_norm(V, Vp) <= MIXED_V_NORM_TOL
+    assert fc._ctx.device_errors() == 0
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])

@@ -127,6 +127,37 @@ def test_pair_buffer_grows_beyond_capacity():
     np.testing.assert_array_equal(pairs, pairs_ref)
 
 
+def test_short_pair_buffer_holds_the_lexicographically_first_pairs():
+    """dem_hash_detect with a buffer shorter than the pair set: counts[0] is the
+    whole count, the overflow flag is raised, and the buffer holds the first
+    `capacity` pairs of the sorted set, the row that the capacity cuts
+    included (its smallest j)."""
+    import torch
+
+    import dem._native as N
+
+    rng = np.random.default_rng(12)
+    pos = rng.uniform(0, 2e-4, (400, 3))
+    r = rng.uniform(5e-6, 2e-5, 400)
+    _, pairs_ref = O.hash_detect(pos, r, 2e-4, True, table_size=1024)
+    k = len(pairs_ref)
+    rows = np.bincount(pairs_ref[:, 0], minlength=400)
+    assert k > 100 and rows.max() >= 4
+    ctx = N.Context(400)
+    soa = torch.as_tensor(np.ascontiguousarray(pos.T), device="cuda")
+    rr = torch.as_tensor(r, device="cuda")
+    starts = np.concatenate([[0], np.cumsum(rows)])
+    big = int(np.argmax(rows))
+    for cap in (1, k // 2, int(starts[big]) + 2, k - 1):  # the third cuts the longest row after two pairs
+        pairs = torch.full((cap, 2), -1, dtype=torch.int32, device="cuda")
+        counts = torch.zeros(2, dtype=torch.int64, device="cuda")
+        ctx.hash_detect(400, soa, rr, 2e-4, True, 1024, pairs, cap, counts)
+        torch.cuda.synchronize()
+        assert int(counts[0]) == k
+        np.testing.assert_array_equal(pairs.cpu().numpy(), pairs_ref[:cap])
+        assert ctx.device_errors() & N.DEVERR_PAIR_OVERFLOW
+
+
 @pytest.mark.parametrize("name", sorted(p.name for p in GOLDEN.glob("merge_*.npz")))
 def test_merge_bit_exact_against_golden(golden, name):
     from dem.particle_state import DropletState

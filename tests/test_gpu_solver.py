@@ -29,7 +29,7 @@ class _Post:
 
 
 def _run(pos, r, L, dt, total_time, precision="fp64", eta_oil=ETA_OIL, eps_oil=2.85, eta_water=0.001, E=3e5,
-         snapshot_depth=4, save_interval=1, correction=None, host_loop=False, graphs=True):
+         snapshot_depth=4, save_interval=1, correction=None, host_loop=False, graphs=True, pbm_coupling=None):
     from dem.collision_detector import SpatialHashCollisionDetector
     from dem.force_calculator import DirectDropletForceCalculator
     from dem.particle_state import DropletState
@@ -45,7 +45,7 @@ def _run(pos, r, L, dt, total_time, precision="fp64", eta_oil=ETA_OIL, eps_oil=2
     det = SpatialHashCollisionDetector(num_particles=n, L=L, boundary_mode="periodic")
     sol = DropletSolution(initial_droplet_state=DropletState(pos.copy(), r.copy(), time=0.0), length=4)
     solver = EulerDropletSolver(fc, sol, _Post(), collision_detector=det, verbose=False, save_interval=save_interval,
-                                snapshot_depth=snapshot_depth, graphs=graphs)
+                                snapshot_depth=snapshot_depth, graphs=graphs, pbm_coupling=pbm_coupling)
     if host_loop:
         solver._solve_host(dt, total_time)  # the reference's loop through the numpy API
     else:
@@ -160,3 +160,48 @@ def test_graph_replayed_steps_equal_eager_steps(golden, precision):
     _same_chain(graphed, eager)
     assert solver.graph_replays >= 30
     assert launch_count() - c0 > 40 * 3  # replayed kernels are counted too
+
+
+class _RecordingCoupling:
+    """Stands in for the DEM->PBM coupling (pbm/coupling.py:51-68 upstream):
+    records every on_collision(pairs, radii) and step(t, radii, dt) call with
+    copies of its arguments."""
+
+    def __init__(self):
+        self.calls = []
+
+    def on_collision(self, collided_pairs, radii):
+        self.calls.append(("on_collision", np.array(collided_pairs, dtype=np.int64).copy(),
+                           np.array(radii, dtype=np.float64).copy()))
+
+    def step(self, current_time, radii, dt):
+        self.calls.append(("step", float(current_time), np.array(radii, dtype=np.float64).copy(), float(dt)))
+
+
+@pytest.mark.parametrize("graphs", [True, False])
+def test_pbm_coupling_hooks_device_loop_equals_host_loop(golden, graphs):
+    """The device-resident loop makes the same coupling calls, in the same
+    order and with equal arguments, as the reference's host loop
+    (euler_droplet_solver.py:100-101 on_collision before each merge,
+    :135-136 step(t + dt, radii, dt) after each Euler update), across the six
+    merges of the golden run."""
+    g = golden("solver_direct_periodic_n48.npz")
+    args = (g["positions"], g["radii"], float(g["L"]), float(g["dt"]), float(g["total_time"]))
+    kw = dict(eta_oil=float(g["eta_oil"]), eps_oil=float(g["eps_oil"]), eta_water=float(g["eta_water"]),
+              E=float(g["E"]))
+    host, dev = _RecordingCoupling(), _RecordingCoupling()
+    _, chain_h = _run(*args, host_loop=True, pbm_coupling=host, **kw)
+    _, chain_d = _run(*args, graphs=graphs, pbm_coupling=dev, **kw)
+    _same_chain(chain_d, chain_h)
+    kinds = [c[0] for c in host.calls]
+    assert kinds.count("on_collision") == int(g["n_solutions"]) - 1 >= 6
+    assert kinds.count("step") >= 10
+    assert len(dev.calls) == len(host.calls)
+    for a, b in zip(dev.calls, host.calls):
+        assert a[0] == b[0]
+        if a[0] == "on_collision":
+            np.testing.assert_array_equal(a[1], b[1])
+            np.testing.assert_array_equal(a[2], b[2])
+        else:
+            assert a[1] == b[1] and a[3] == b[3]
+            np.testing.assert_array_equal(a[2], b[2])

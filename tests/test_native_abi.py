@@ -6,6 +6,8 @@ from __future__ import annotations
 import ctypes
 import re
 
+import pytest
+
 from conftest import ROOT
 
 import dem._native as N
@@ -36,7 +38,14 @@ def test_binding_matches_header():
     assert N.version().startswith("dem_b200")
 
 
-def test_library_is_built_for_sm100a():
-    # the fat binary of an sm_100a build names the architecture in its ELF notes
-    data = N.LIB_PATH.read_bytes()
-    assert b"sm_100a" in data
+def test_build_targets_sm100a_only():
+    # every object of the library is compiled with exactly this architecture flag
+    import build_native
+
+    assert build_native.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+@pytest.mark.gpu
+def test_runtime_loads_sm100_code():
+    # the runtime's own answer for a kernel of the library: the code it loads is sm_100
+    assert N.kernel_binary_version(0) == 100
