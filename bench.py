@@ -239,6 +239,47 @@ def flush_l2(buf):
     buf.fill_(1)
 
 
+HBM_FALLBACK_GBS = 6650.0  # an earlier STREAM-style copy on this pool's B200s, used when no measured file exists
+
+
+def hbm_peak():
+    """(GB/s, source): the measured copy bandwidth of MEASURED_PEAKS.json when
+    present, else the fallback figure."""
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        d = json.loads(p.read_text())
+        for k in ("hbm_gbs", "hbm_GBs", "hbm"):
+            if k in d and d[k]:
+                return float(d[k]), "measured (MEASURED_PEAKS.json)"
+    except Exception:
+        pass
+    return HBM_FALLBACK_GBS, "fallback (no MEASURED_PEAKS.json)"
+
+
+# Algorithmic bytes of the memory-bound kernels (what a kernel that touches
+# every input and output once would move):
+#   hash detection (csrc/hash.cu): per droplet its position and radius (32 B
+#     read), its bucket id (4 B written, 4 B read) and bucket slot (4 B written,
+#     4 B read); per table slot its start (4 B written, 4 B read); 8 B per pair.
+#   Morton build (csrc/bh.cu): per droplet positions (24 B read), key (4 B
+#     written), 4 radix passes over (key, index) (16 B each), the gather of
+#     position and radius into key order (32 B read, 32 B written); per node its
+#     records (~140 B written).
+def hash_bytes(n, table, pairs):
+    return 48 * n + 8 * table + 8 * pairs
+
+
+def morton_build_bytes(n, nodes):
+    return (24 + 4 + 4 * 16 + 64) * n + 140 * nodes
+
+
+def hbm_entry(name, ms, nbytes, peak, src, formula):
+    gbs = nbytes / (ms * 1e-3) / 1e9 if ms else None
+    return {"kernel": name, "ms_per_launch": ms, "algorithmic_bytes": nbytes, "formula": formula,
+            "achieved_gbs": gbs, "peak_gbs": peak, "peak_source": src,
+            "frac": gbs / peak if gbs else None}
+
+
 def time_steps(st, steps, flush, stream):
     """CUDA-event time of each of ``steps`` steps, L2 flushed before each one
     (outside the events); returns (per-step ms, merges inside the window)."""
@@ -868,6 +909,17 @@ def report_tree(args, res):
         "clocks": clocks,
         "gpu_launches": res["launches"],
     }
+    peak_b, src_b = hbm_peak()
+    mb = []
+    if "hash_detect" in res["kern"]:
+        table = 1 << max(int(2 * n - 1).bit_length(), 0)
+        mb.append(hbm_entry("hash detection", res["kern"]["hash_detect"], hash_bytes(n, table, 0), peak_b, src_b,
+                            "48 N + 8 table + 8 pairs"))
+    if "bh_build" in res["kern"]:
+        mb.append(hbm_entry("Morton octree build (keys, radix sort, gather, levels, node moments)",
+                            res["kern"]["bh_build"], morton_build_bytes(n, st["node_count"]), peak_b, src_b,
+                            "156 N + 140 nodes"))
+    line["memory_bound"] = mb
     print(json.dumps(line), flush=True)
 
 
@@ -1373,6 +1425,12 @@ def main():
         line["cpu_baseline"] = {"value": c["steps_per_s"], "unit": "steps/s", "cores": c["cores"], "kind": "port",
                                 "sample": f"hash + Euler on all {n} droplets; both O(N^2) passes on {c['rows']} rows "
                                           f"x {n} columns, extrapolated ({c['sample_s']:.1f} s of CPU work)"}
+    if "hash_detect" in kern:
+        peak_b, src_b = hbm_peak()
+        table = 1 << max(int(2 * n - 1).bit_length(), 0)
+        line["memory_bound"] = [hbm_entry("hash detection (assign, scans, scatter, bucket records, count, write)",
+                                          kern["hash_detect"][0] / kern["hash_detect"][1], hash_bytes(n, table, 0),
+                                          peak_b, src_b, "48 N + 8 table + 8 pairs")]
     if "fp64" in res:
         f64 = res["fp64"]
         fp64_sps = 1000.0 / f64["ms_per_step"]

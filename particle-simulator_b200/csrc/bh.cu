@@ -11,6 +11,10 @@
 //           bits, split into its non-empty octants while it holds more than
 //           `leaf_size` droplets (and level < 10); nodes are contiguous runs
 //           of the sorted arrays, children stored consecutively.
+//           Algorithmic bytes of the build: 156 N + 140 M (N droplets, M nodes):
+//           positions read and key written (28 B), four radix passes over
+//           (key, index) (64 B), position and radius gathered into key order
+//           (64 B), the node records written.
 //   nodes   R^3 sum and R^3-weighted centre (flat_tree.py:544-554,
 //           octree_node.py:98-114), side = root side / 2^level, and the
 //           R^3-weighted second moment Q of the node about that centre; after the force

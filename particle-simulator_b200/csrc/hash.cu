@@ -14,6 +14,11 @@
 //      droplets in bucket order, so the lanes of a warp share candidate lists)
 //   5. exclusive scan of the per-i counts -> pair offsets (lexicographic order)
 //   6. per droplet i: write its pairs, sort its j's ascending
+// Memory roofline: the chain is bounded by HBM and latency, not arithmetic.  Its
+// algorithmic bytes per detection are 48 N + 8 T + 8 K (N droplets, T table
+// slots, K pairs): position and radius read once (32 B), bucket id and bucket
+// slot written and read (16 B), bucket starts written and read (8 B per slot),
+// 8 B per pair written.
 // The candidate set of a droplet is exactly the reference's (the same buckets,
 // including buckets shared by aliased cells), and the distance test is the
 // same IEEE expression (this file is compiled with -fmad=false), so the pair
