@@ -74,6 +74,7 @@ def parse():
     ap.add_argument("--fd", type=int, default=0, help="adjoint: central-difference checks on this many coordinates")
     ap.add_argument("--boxes", type=int, default=64)
     ap.add_argument("--parity-n", default="", help="parity_tree: comma-separated droplet counts (default 100k,250k,500k)")
+    ap.add_argument("--parity-mpl", default="", help="parity_tree: comma-separated leaf sizes (default 1,2,4,8,16)")
     return ap.parse_args()
 
 
@@ -968,7 +969,8 @@ def run_parity_tree(args, device):
         F_d, V_d = fd.calculate_forces_and_convection(pos, rad)
         vt_d = V_d + F_d / (sf * rad[:, None])
         tc = TreeDropletForceCalculator(num_particles=n, theta=0.5, mpl=1, periodic=False, **PARITY_PHYS)
-        for mpl in PARITY_MPL:
+        mpls = [int(x) for x in args.parity_mpl.split(",")] if args.parity_mpl else list(PARITY_MPL)
+        for mpl in mpls:
             tc.update_params(0.5, mpl)
 
             def step():

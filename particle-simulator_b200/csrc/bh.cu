@@ -974,6 +974,21 @@ int morton_order(dem_ctx *ctx, int n, const double *x, const double *y, const do
     }
     geom_kernel<<<1, 32, 0, counted(s)>>>(periodic ? 1 : 0, L, w.bbox, w.geom);
     keys_kernel<<<g, 256, 0, counted(s)>>>(n, x, y, z, w.geom, w.keys[0], w.idx[0]);
+    return radix_sort_pairs(ctx, n, w, s);
+}
+
+int radix_pass(dem_ctx *ctx, int n, const uint32_t *kin, const int32_t *vin, uint32_t *kout, int32_t *vout, int shift,
+               int32_t *hist, cudaStream_t s) {
+    const int tiles = (n + RS_TILE - 1) / RS_TILE;
+    int32_t *off = hist + 256 * (size_t)tiles + 1;
+    rs_hist_kernel<<<tiles, RS_T, 0, counted(s)>>>(n, kin, shift, tiles, hist);
+    int rc = exclusive_scan<int32_t, int32_t>(ctx, hist, off, 256LL * tiles, s);
+    if (rc) return rc;
+    rs_scatter_kernel<<<tiles, RS_T, 0, counted(s)>>>(n, kin, vin, kout, vout, shift, tiles, off);
+    return dem_check_launch(ctx, "radix pass");
+}
+
+int radix_sort_pairs(dem_ctx *ctx, int n, const MortonWs &w, cudaStream_t s) {
     const int tiles = (n + RS_TILE - 1) / RS_TILE;
     int32_t *hist = w.hist, *off = w.hist + 256 * (size_t)tiles + 1;
     int cur = 0, rc;

@@ -4,6 +4,7 @@
 #include <cstring>
 
 #include "common.cuh"
+#include "scan.cuh"
 
 #define DEM_VERSION "dem_b200 0.1 (sm_100a)"
 
@@ -22,6 +23,7 @@ void dem_count_launches(unsigned long long k) { g_launches.fetch_add(k, std::mem
 extern "C" void dem_count_replayed_launches(unsigned long long k) { dem_count_launches(k); }
 
 namespace dem {
+int sym_sorted_prepare(dem_ctx *ctx);
 int direct_plan(const dem_ctx *ctx, int n, int periodic, int *schedule, int *i_per_thread, int *threads,
                 long long *ctas, int *j_splits);
 }
@@ -200,6 +202,14 @@ int dem_ctx_create(int device, int capacity, dem_ctx **out) {
     if (!rc) rc = dem_check_cuda(ctx, cudaMalloc((void **)&ctx->dscratch, 8 * sizeof(double)), "scratch");
     if (!rc) rc = dem_check_cuda(ctx, cudaMalloc((void **)&ctx->merged_cnt, 4 * sizeof(int32_t)), "scratch");
     if (!rc) rc = dem_ctx_reserve(ctx, capacity);
+    // scan block sums (fixed size) and the sorted pair kernels' shared-memory limit, set up front so
+    // that no later call allocates or changes a kernel attribute (calls may run under stream capture)
+    if (!rc) {
+        const size_t need = sizeof(int64_t) * (dem::SCAN_MAX_BLOCKS + 1);
+        rc = dem_check_cuda(ctx, cudaMalloc(&ctx->scan_tmp, need), "scan workspace");
+        if (!rc) ctx->scan_tmp_bytes = need;
+    }
+    if (!rc) rc = dem::sym_sorted_prepare(ctx);
     if (rc) {
         fprintf(stderr, "dem_ctx_create: %s\n", ctx->last_error.c_str());
         dem_ctx_destroy(ctx);

@@ -629,13 +629,13 @@ __device__ __forceinline__ void sorted_subtile(const SortedArgs &a, const float4
                 const int jo = CI[jj];
                 const int jl = J * B + jo;  // packed position of j
                 if (any && jo >= 0 && jl < v.n) {
-                    const int j = a.perm[jl];
+                    const int j = a.perm[v.o0 + jl];
                     double ex_ = 0.0, ey_ = 0.0, ez_ = 0.0;
 #pragma unroll
                     for (int k = 0; k < IPT; ++k) {
                         const int il = I * B + k * SYM_T + tid;
                         if (ex[k] && il < v.n) {
-                            const int i = a.perm[il];
+                            const int i = a.perm[v.o0 + il];
                             const double3 w1 = FORCE ? near_force_fp64(i, j, a.s.m, PER ? 1 : 0, inv_ell, v.L)
                                                      : near_oseen_fp64(i, j, a.s.m, PER ? 1 : 0, inv_ell,
                                                                        fscale_inv, v.L);
@@ -716,8 +716,9 @@ __global__ void __launch_bounds__(SYM_T, 4) mixed_sym_sorted_kernel(const Sorted
         const float m_amb = (float)(v.L * inv_ell * 2.0 * MIC_MARGIN);
 
         // ---- the lists of block J against block I: count per class, then write ----
-        const float4 blo = a.bounds[2 * I], bhi = a.bounds[2 * I + 1];
-        const uint32_t *occ = a.occ + (size_t)I * 3 * AMB_WORDS;
+        const int gI = v.p0 / B + I;  // block I of this box in the table of all blocks
+        const float4 blo = a.bounds[2 * gI], bhi = a.bounds[2 * gI + 1];
+        const uint32_t *occ = a.occ + (size_t)gI * 3 * AMB_WORDS;
         auto load_entry = [&](int p, float4 &A, float4 &Bv, float4 &Q, float2 &S3) {
             A = a.s.p0[p];
             Bv = a.s.p1[p];
@@ -904,9 +905,15 @@ __global__ void __launch_bounds__(SYM_T, 4) mixed_sym_sorted_kernel(const Sorted
 }
 
 // Per block of the packed layout: the bins of its stored coordinates that hold a droplet, per axis.
-__global__ void sorted_occupancy_kernel(int B, double L, const unsigned long long *__restrict__ scales,
-                                        const float4 *__restrict__ p0, const float4 *__restrict__ p1,
-                                        uint32_t *__restrict__ occ) {
+__global__ void sorted_occupancy_kernel(const SymBoxes t, int B, const float4 *__restrict__ p0,
+                                        const float4 *__restrict__ p1, uint32_t *__restrict__ occ) {
+    double L = t.L1;
+    const unsigned long long *scales = t.scales1;
+    if (t.nbox > 1) {
+        const int b = box_index(t.poff, t.nbox, (int)blockIdx.x * B);
+        L = t.L[b];
+        scales = t.scales + 2 * b;
+    }
     const double inv_ell = pow2_inv_of(scales[0]);
     const float Ls = (float)(L * inv_ell), invLs = (float)(1.0 / (L * inv_ell));
     uint32_t *o = occ + (size_t)blockIdx.x * 3 * AMB_WORDS;
@@ -995,7 +1002,7 @@ __global__ void prep_sym_kernel(const SymBoxes t, const double *__restrict__ x, 
         const int l = p - pb;
         float X = 0.f, Y = 0.f, Z = 0.f, W = 0.f, K = 0.f, Fx = 0.f, Fy = 0.f, Fz = 0.f;
         if (l < nb) {
-            const int i = perm ? perm[l] : o0 + l;  // perm: one box in Morton order
+            const int i = perm ? perm[o0 + l] : o0 + l;  // perm: each box's droplets in Morton order
             const double s = pow2_inv_of(sc[0]);
             const double center = 0.5 * L;
             const double rs = r[i] * s;
@@ -1151,36 +1158,81 @@ size_t sym_workspace_bytes(long long npad_total, long long items_total, int B) {
 // Workspace bytes of the symmetric schedule for one box of n droplets: the
 // packed layout and partial sums, plus the Morton order and the per-block
 // bounds of the sorted kernel.
+size_t sym_sorted_extra_bytes(long long n_total, long long npad_total, int B) {
+    const long long nb = npad_total / B;
+    return align256(morton_ws_bytes(n_total > 0 ? (int)n_total : 1)) + align256((size_t)nb * 2 * sizeof(float4)) +
+           (size_t)nb * 3 * AMB_WORDS * sizeof(uint32_t);
+}
+
 size_t sym_partial_bytes(int n, int ipt) {
     const long long B = (long long)SYM_T * ipt;
     const long long nb = (n + B - 1) / B;
-    return sym_workspace_bytes(nb * B, nb * (nb + 1) / 2, (int)B) + align256(morton_ws_bytes(n > 0 ? n : 1)) +
-           align256((size_t)nb * 2 * sizeof(float4)) + (size_t)nb * 3 * AMB_WORDS * sizeof(uint32_t);
+    return sym_workspace_bytes(nb * B, nb * (nb + 1) / 2, (int)B) + sym_sorted_extra_bytes(n, nb * B, (int)B);
+}
+
+// 30-bit Morton key of each droplet's cell in its box's cube [0, L_b)^3 (1024
+// cells per axis, clamped), the same expression for one box and for every box
+// of an ensemble, so that a box sorts into the same order either way.
+__global__ void box_morton_keys_kernel(const SymBoxes t, const double *__restrict__ x, const double *__restrict__ y,
+                                       const double *__restrict__ z, uint32_t *__restrict__ keys,
+                                       int32_t *__restrict__ idx) {
+    auto spread10 = [](uint32_t v) {  // bit k -> bit 3k
+        v &= 0x3ffu;
+        v = (v | (v << 16)) & 0x030000FFu;
+        v = (v | (v << 8)) & 0x0300F00Fu;
+        v = (v | (v << 4)) & 0x030C30C3u;
+        v = (v | (v << 2)) & 0x09249249u;
+        return v;
+    };
+    auto cell10 = [](double p, double inv) {
+        const int c = (int)floor(p * inv * 1024.0);
+        return (uint32_t)(c < 0 ? 0 : (c > 1023 ? 1023 : c));
+    };
+    for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < t.n_total; d += gridDim.x * blockDim.x) {
+        const double inv = 1.0 / (t.nbox > 1 ? t.L[box_index(t.off, t.nbox, d)] : t.L1);
+        keys[d] = (spread10(cell10(x[d], inv)) << 2) | (spread10(cell10(y[d], inv)) << 1) | spread10(cell10(z[d], inv));
+        idx[d] = d;
+    }
+}
+
+// keys[k] = the box of droplet idx[k] (the last, most significant sort digit of an ensemble).
+__global__ void box_of_kernel(const SymBoxes t, const int32_t *__restrict__ idx, uint32_t *__restrict__ keys) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < t.n_total; k += gridDim.x * blockDim.x)
+        keys[k] = (uint32_t)box_index(t.off, t.nbox, idx[k]);
+}
+
+template <int IPT, bool PER, bool FORCE>
+static cudaError_t sorted_attr() {
+    return cudaFuncSetAttribute(mixed_sym_sorted_kernel<IPT, PER, FORCE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                sorted_smem_bytes<IPT, FORCE>());
+}
+
+// Raises the dynamic shared-memory limit of every sorted pair kernel on the
+// context's (current) device.  Called when a context is created, so that no
+// pass has to do it (possibly inside a stream capture).
+int sym_sorted_prepare(dem_ctx *ctx) {
+    const cudaError_t es[] = {sorted_attr<4, true, true>(),  sorted_attr<4, true, false>(),
+                              sorted_attr<4, false, true>(), sorted_attr<4, false, false>(),
+                              sorted_attr<2, true, true>(),  sorted_attr<2, true, false>(),
+                              sorted_attr<2, false, true>(), sorted_attr<2, false, false>()};
+    for (cudaError_t e : es)
+        if (e != cudaSuccess) return dem_check_cuda(ctx, e, "sorted pass: shared memory attribute");
+    return DEM_OK;
 }
 
 template <int IPT, bool PER, bool FORCE>
 static int launch_sorted(dem_ctx *ctx, const SortedArgs &a, int grid, cudaStream_t s) {
-    constexpr int smem = sorted_smem_bytes<IPT, FORCE>();
-    // the dynamic shared memory limit is raised once per device, on the first (eager) call
-    static bool attr_set[64] = {};
-    const int dev = ctx->device >= 0 && ctx->device < 64 ? ctx->device : 0;
-    if (!attr_set[dev]) {
-        int rc = dem_check_cuda(ctx, cudaFuncSetAttribute(mixed_sym_sorted_kernel<IPT, PER, FORCE>,
-                                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
-                                "sorted pass: shared memory attribute");
-        if (rc) return rc;
-        attr_set[dev] = true;
-    }
-    mixed_sym_sorted_kernel<IPT, PER, FORCE><<<grid, SYM_T, smem, counted(s)>>>(a);
+    mixed_sym_sorted_kernel<IPT, PER, FORCE><<<grid, SYM_T, sorted_smem_bytes<IPT, FORCE>(), counted(s)>>>(a);
     return DEM_OK;
 }
 
-// One box, droplets in Morton order: sort, pack, per-block bounds, the pair
-// kernel with fast and slow lists, then the fixed-order reduction through the
-// permutation.
+// Droplets of every box in Morton order: sort, pack, per-block bounds, the pair
+// kernel with fast, medium and slow lists, then the fixed-order reduction
+// through the permutation.  ctas = 0: one CTA per block pair, else a
+// persistent grid of that many.  At most 256 boxes (the key's box field).
 template <bool FORCE>
-static int run_sym_sorted(dem_ctx *ctx, const SymBoxes &t, int ipt, bool per, const MixedArgs &m, double *work,
-                          double coeff, double *ox, double *oy, double *oz, cudaStream_t s) {
+static int run_sym_sorted(dem_ctx *ctx, const SymBoxes &t, int ipt, int ctas, bool per, const MixedArgs &m,
+                          double *work, double coeff, double *ox, double *oy, double *oz, cudaStream_t s) {
     const int B = SYM_T * ipt;
     const int n = t.n_total;
     const int nb = t.npad_total / B;
@@ -1198,9 +1250,24 @@ static int run_sym_sorted(dem_ctx *ctx, const SymBoxes &t, int ipt, bool per, co
     float4 *bounds = reinterpret_cast<float4 *>(extra + align256(morton_ws_bytes(n)));
     uint32_t *occ = reinterpret_cast<uint32_t *>(extra + align256(morton_ws_bytes(n)) +
                                                  align256((size_t)nb * 2 * sizeof(float4)));
-    int rc = morton_order(ctx, n, m.x, m.y, m.z, per ? 1 : 0, m.L, mw, s);
-    if (rc) return rc;
+    // sorted position -> droplet; box b keeps positions [off[b], off[b + 1]).  An open single box
+    // sorts in its droplets' bounding cube; boxes of an ensemble and periodic boxes in [0, L_b)^3,
+    // then (ensembles) a stable pass on the box index groups every box's droplets
+    int rc;
     const int32_t *perm = mw.idx[0];
+    const int kg = max(1, min(ceil_div(n, 256), 8 * ctx->sm_count));
+    if (t.nbox == 1 && !per) {
+        rc = morton_order(ctx, n, m.x, m.y, m.z, 0, m.L, mw, s);
+    } else {
+        box_morton_keys_kernel<<<kg, 256, 0, counted(s)>>>(t, m.x, m.y, m.z, mw.keys[0], mw.idx[0]);
+        rc = radix_sort_pairs(ctx, n, mw, s);
+        if (!rc && t.nbox > 1) {
+            box_of_kernel<<<kg, 256, 0, counted(s)>>>(t, mw.idx[0], mw.keys[0]);
+            rc = radix_pass(ctx, n, mw.keys[0], mw.idx[0], mw.keys[1], mw.idx[1], 0, mw.hist, s);
+            perm = mw.idx[1];
+        }
+    }
+    if (rc) return rc;
     const int pgrid = max(1, min(ceil_div(t.npad_total, 256), 4 * ctx->sm_count));
     prep_sym_kernel<FORCE><<<pgrid, 256, 0, counted(s)>>>(t, m.x, m.y, m.z, m.r, m.fx, m.fy, m.fz,
                                                           FORCE ? ctx->tuning.near_force : ctx->tuning.near_oseen,
@@ -1209,7 +1276,7 @@ static int run_sym_sorted(dem_ctx *ctx, const SymBoxes &t, int ipt, bool per, co
     if (per) {
         rc = dem_check_cuda(ctx, cudaMemsetAsync(occ, 0, (size_t)nb * 3 * AMB_WORDS * sizeof(uint32_t), s), "memset");
         if (rc) return rc;
-        sorted_occupancy_kernel<<<nb, SYM_T, 0, counted(s)>>>(B, m.L, m.scales, p0, p1, occ);
+        sorted_occupancy_kernel<<<nb, SYM_T, 0, counted(s)>>>(t, B, p0, p1, occ);
     }
     rc = dem_check_launch(ctx, "sorted pass prep");
     if (rc) return rc;
@@ -1226,7 +1293,7 @@ static int run_sym_sorted(dem_ctx *ctx, const SymBoxes &t, int ipt, bool per, co
     a.perm = perm;
     a.bounds = bounds;
     a.occ = occ;
-    const int grid = t.items_total;
+    const int grid = ctas > 0 ? min(ctas, t.items_total) : t.items_total;
     dem_prof_begin(ctx, FORCE ? "mixed_force_pass" : "mixed_convection_pass", s);
     if (ipt == 4)
         rc = per ? launch_sorted<4, true, FORCE>(ctx, a, grid, s) : launch_sorted<4, false, FORCE>(ctx, a, grid, s);
@@ -1241,12 +1308,12 @@ static int run_sym_sorted(dem_ctx *ctx, const SymBoxes &t, int ipt, bool per, co
     return dem_check_launch(ctx, "mixed reduce (symmetric, Morton order)");
 }
 
+// Blocks in the caller's droplet order (DEM_SCHED_SYMMETRIC_PLAIN): every pair
+// takes the minimum image and the tests in mixed_sym_kernel.
 template <bool FORCE>
-int run_sym_boxes(dem_ctx *ctx, const SymBoxes &t, int ipt, int ctas, bool per, const MixedArgs &m, double *work,
-                  double coeff, double *ox, double *oy, double *oz, cudaStream_t s) {
-    ipt = ipt >= 4 ? 4 : 2;
+static int run_sym_plain(dem_ctx *ctx, const SymBoxes &t, int ipt, int ctas, bool per, const MixedArgs &m,
+                         double *work, double coeff, double *ox, double *oy, double *oz, cudaStream_t s) {
     const int B = SYM_T * ipt;
-    if (t.n_total == 0) return DEM_OK;
     char *base = reinterpret_cast<char *>(work);
     const size_t np = (size_t)t.npad_total;
     float4 *p0 = reinterpret_cast<float4 *>(base);
@@ -1282,6 +1349,16 @@ int run_sym_boxes(dem_ctx *ctx, const SymBoxes &t, int ipt, int ctas, bool per, 
     return dem_check_launch(ctx, "mixed reduce (symmetric)");
 }
 
+template <bool FORCE>
+int run_sym_boxes(dem_ctx *ctx, const SymBoxes &t, int ipt, int ctas, bool per, const MixedArgs &m, double *work,
+                  double coeff, double *ox, double *oy, double *oz, cudaStream_t s) {
+    ipt = ipt >= 4 ? 4 : 2;
+    if (t.n_total == 0) return DEM_OK;
+    if (ctx->tuning.schedule == DEM_SCHED_SYMMETRIC_PLAIN || t.nbox > 256)
+        return run_sym_plain<FORCE>(ctx, t, ipt, ctas, per, m, work, coeff, ox, oy, oz, s);
+    return run_sym_sorted<FORCE>(ctx, t, ipt, ctas, per, m, work, coeff, ox, oy, oz, s);
+}
+
 template int run_sym_boxes<true>(dem_ctx *, const SymBoxes &, int, int, bool, const MixedArgs &, double *, double,
                                  double *, double *, double *, cudaStream_t);
 template int run_sym_boxes<false>(dem_ctx *, const SymBoxes &, int, int, bool, const MixedArgs &, double *, double,
@@ -1306,9 +1383,7 @@ int run_sym_pass(dem_ctx *ctx, int n, int ipt, bool per, const MixedArgs &m, dou
     t.scales1 = m.scales;
     MixedArgs mm = m;
     mm.r = r;
-    if (ctx->tuning.schedule == DEM_SCHED_SYMMETRIC_PLAIN)
-        return run_sym_boxes<FORCE>(ctx, t, ipt, 0, per, mm, work, coeff, ox, oy, oz, s);
-    return run_sym_sorted<FORCE>(ctx, t, ipt, per, mm, work, coeff, ox, oy, oz, s);
+    return run_sym_boxes<FORCE>(ctx, t, ipt, 0, per, mm, work, coeff, ox, oy, oz, s);
 }
 
 template int run_sym_pass<true>(dem_ctx *, int, int, bool, const MixedArgs &, double *, const double *, double,

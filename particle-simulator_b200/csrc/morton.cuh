@@ -27,5 +27,11 @@ MortonWs morton_ws_carve(void *base, int n);
 // keys[0] holds the sorted keys.  n >= 1.
 int morton_order(dem_ctx *ctx, int n, const double *x, const double *y, const double *z, int periodic, double L,
                  const MortonWs &w, cudaStream_t s);
+// Stable sort of (keys[0][k], idx[0][k]) by key, k < n: four 8-bit passes; the
+// result is back in keys[0] / idx[0].
+int radix_sort_pairs(dem_ctx *ctx, int n, const MortonWs &w, cudaStream_t s);
+// One stable pass on the 8-bit digit (key >> shift) & 255: (kin, vin) -> (kout, vout).
+int radix_pass(dem_ctx *ctx, int n, const uint32_t *kin, const int32_t *vin, uint32_t *kout, int32_t *vout, int shift,
+               int32_t *hist, cudaStream_t s);
 
 }  // namespace dem
