@@ -427,68 +427,71 @@ __global__ void __launch_bounds__(SYM_T, 4) mixed_sym_kernel(const SymArgs a) {
 //   * far: the minimum-image distance from j to the bounding box of block I
 //     exceeds k (max r_I + r_j) (0.1 % margin), so no pair of j with block I
 //     is near contact;
-//   * unambiguous: no droplet of block I lies within 2^-17 L (twice the
-//     ambiguity margin of the pair test) of the point where its separation
-//     from j would be L/2 on some axis.  Checked against a per-block bitmap of
-//     occupied 1/65,536 L bins per axis;
-//   * fixed image: on every axis one periodic image serves every i of the
-//     block, with the whole separation interval inside the ambiguity margin
-//     (fixed implies unambiguous).
+//   * fixed image on an axis: one periodic image serves every i of the block,
+//     with the whole separation interval inside the ambiguity margin; the
+//     entry is stored with that image applied on that axis;
+//   * unambiguous on an axis that is not fixed: no droplet of block I lies
+//     within 2^-17 L (twice the ambiguity margin of the pair test) of the
+//     point where its separation from j would be L/2.  Checked against a
+//     per-block bitmap of occupied 1/65,536 L bins per axis.
 //
-// Classes and their sub-tile loops:
-//   fast   (far, fixed image): stored with that image applied; the loop takes
-//          d = x_j - x_i and the pair terms, nothing else;
-//   medium (far, unambiguous): the loop takes the FP32 minimum image and the
-//          pair terms, without the near and ambiguity tests and the FP64 branch;
+// A far j that is unambiguous on every axis gets the mask of its axes that
+// are not fixed (0 .. 7); every other j is slow.  The list holds three runs:
+//   fast   (mask 0): the loop takes d = x_j - x_i and the pair terms, nothing
+//          else; padded to a whole sub-tile with zero-weight entries far away;
+//   masked (masks 1 .. 7, in mask order): the loop takes the FP32 minimum
+//          image only on the axes of the sub-tile's mask (the OR of its
+//          entries' masks, uniform over the CTA), then the pair terms, without
+//          the near and ambiguity tests and the FP64 branch; the run is cut to
+//          whole sub-tiles and its last entries (< 32) move to the slow run;
 //   slow   (the rest, and every j of a diagonal item): the loop of
-//          mixed_sym_kernel.
+//          mixed_sym_kernel, padded with zero-weight entries (its near test
+//          keeps a padding entry on top of a droplet harmless).
 // A far, unambiguous pair is one the slow loop would evaluate in FP32 too, so
-// every pair takes the same FP32 / FP64 decision as in mixed_sym_kernel.
-//
-// The lists are filled in j order, fast, medium and slow runs one after the
-// other, each padded to whole 32-entry sub-tiles with zero-weight entries.  All
+// every pair takes the same FP32 / FP64 decision as in mixed_sym_kernel.  All
 // warps walk the same lists, so every warp does the same work between the CTA
 // barriers.  The j block is classified as it is loaded (coalesced vector loads
 // from the L2-resident packed arrays), so it is not staged by TMA.  Results are
 // deterministic: lists, sums and their order depend only on the inputs.
 // ---------------------------------------------------------------------------
 struct SortedArgs {
-    SymArgs s;               // one box; packed layout in Morton order
-    const int32_t *perm;     // packed position -> droplet (first n positions)
-    const float4 *bounds;    // [nb][2]: (min s_x, min s_y, min s_z, max k r), (max s_x, max s_y, max s_z, 0)
-    const uint32_t *occ;     // [nb][3][AMB_BINS / 32]: occupied bins of the stored coordinates per block
+    SymArgs s;               // packed layout of every box in Morton order
+    const int32_t *perm;     // sorted position -> droplet
+    const float4 *bounds;    // [blocks][2]: (min s_x, min s_y, min s_z, max k r), (max s_x, max s_y, max s_z, 0)
+    const uint32_t *occ;     // [blocks][3][AMB_BINS / 32]: occupied bins of the stored coordinates per block
 };
 
-constexpr int SORTED_PAD = 96;      // list slots beyond B: the padding of the three runs (<= 31 each)
+constexpr int SORTED_PAD = 96;      // list slots beyond B: padding of the fast and slow runs (<= 31 each)
 constexpr int AMB_BINS = 65536;     // bins per axis of the occupancy bitmaps (a power of two)
 constexpr int AMB_WORDS = AMB_BINS / 32;
+constexpr int CLS_SLOW = 8;         // classes 0 .. 7: far and unambiguous, with the mask of axes that take the image
+constexpr int NCLS = 9;
 
 template <bool FORCE>
 constexpr int sorted_entry_bytes() {
-    return FORCE ? 16 + 16 + 8 + 4 : 16 + 16 + 16 + 8 + 4;
+    return FORCE ? 16 + 16 + 8 + 4 + 1 : 16 + 16 + 16 + 8 + 4 + 1;
 }
 template <int IPT, bool FORCE>
 constexpr int sorted_smem_bytes() {
-    return (SYM_T * IPT + SORTED_PAD) * sorted_entry_bytes<FORCE>();
+    return ((SYM_T * IPT + SORTED_PAD) * sorted_entry_bytes<FORCE>() + 15) & ~15;
 }
 
 // far entry of the fast run's padding: zero weight, ~10^6 ell from every droplet
 constexpr float SORTED_FAR = 1.0e6f;
 
-enum { CLS_FAST = 0, CLS_MEDIUM = 1, CLS_SLOW = 2 };
-
 __device__ __forceinline__ int amb_bin(float v, float Ls, float invLs) {
     return ((int)floorf(fmaf(v, invLs, 0.5f) * (float)AMB_BINS)) & (AMB_BINS - 1);
 }
 
-// Class of the stored j entry (sc: coordinates, kj: k r_j) against block I; for
-// CLS_FAST sc comes back with the fixed image applied.
+// Class of the stored j entry (sc: coordinates, kj: k r_j) against block I:
+// the mask of the axes that take the minimum image (0 .. 7; sc comes back with
+// the fixed image applied on the other axes), or CLS_SLOW.
 template <bool PER>
 __device__ __forceinline__ int classify_j(float sc[3], float kj, const float4 &blo, const float4 &bhi,
                                           const uint32_t *__restrict__ occ, float Ls, float invLs, float hm_fast,
                                           float m_amb) {
     const float lo3[3] = {blo.x, blo.y, blo.z}, hi3[3] = {bhi.x, bhi.y, bhi.z};
-    bool fixed = true;
+    int mask = 0;
     float g2 = 0.f;
     float u3[3];
 #pragma unroll
@@ -500,7 +503,7 @@ __device__ __forceinline__ int classify_j(float sc[3], float kj, const float4 &b
             u3[c] = u;
             dlo = fmaf(-u, Ls, dlo);
             dhi = fmaf(-u, Ls, dhi);
-            fixed = fixed && dlo >= -hm_fast && dhi <= hm_fast;
+            if (!(dlo >= -hm_fast && dhi <= hm_fast)) mask |= 1 << c;
             // minimum-image distance of the interval from 0: the nearest of its three images
             gap = fmaxf(0.f, fmaxf(dlo, -dhi));
             gap = fminf(gap, fmaxf(0.f, fmaxf(dlo + Ls, -(dhi + Ls))));
@@ -512,22 +515,24 @@ __device__ __forceinline__ int classify_j(float sc[3], float kj, const float4 &b
     }
     const float kk = blo.w + kj;
     if (!(g2 > 1.001f * kk * kk)) return CLS_SLOW;
-    if (!PER) return CLS_FAST;
-    if (fixed) {
+    if (!PER) return 0;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) sc[c] = fmaf(-u3[c], Ls, sc[c]);
-        return CLS_FAST;
+    for (int c = 0; c < 3; ++c) {
+        if (mask & (1 << c)) {  // a droplet of block I near s_j - L/2 on this axis: ambiguous
+            const float a = sc[c] - 0.5f * Ls;
+            const int b0 = amb_bin(a - m_amb, Ls, invLs), b1 = amb_bin(a + m_amb, Ls, invLs);
+            const uint32_t *w = occ + c * AMB_WORDS;
+            if ((w[b0 >> 5] >> (b0 & 31)) & 1u) return CLS_SLOW;
+            if ((w[b1 >> 5] >> (b1 & 31)) & 1u) return CLS_SLOW;
+        } else {
+            sc[c] = fmaf(-u3[c], Ls, sc[c]);
+        }
     }
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {  // a droplet of block I near s_j - L/2 on this axis: ambiguous
-        const float a = sc[c] - 0.5f * Ls;
-        const int b0 = amb_bin(a - m_amb, Ls, invLs), b1 = amb_bin(a + m_amb, Ls, invLs);
-        const uint32_t *w = occ + c * AMB_WORDS;
-        if ((w[b0 >> 5] >> (b0 & 31)) & 1u) return CLS_SLOW;
-        if ((w[b1 >> 5] >> (b1 & 31)) & 1u) return CLS_SLOW;
-    }
-    return CLS_MEDIUM;
+    return mask;
 }
+
+// sub-tile loops: MODE_FAST (no image), MODE_MASKED (image on the axes of a uniform mask), MODE_SLOW
+enum { MODE_FAST = 0, MODE_MASKED = 1, MODE_SLOW = 2 };
 
 template <int IPT, bool PER, bool FORCE, int MODE>
 __device__ __forceinline__ void sorted_subtile(const SortedArgs &a, const float4 *C0, const float4 *C1,
@@ -540,11 +545,11 @@ __device__ __forceinline__ void sorted_subtile(const SortedArgs &a, const float4
                                                const float2 *fzi, float2 *ax, float2 *ay, float2 *az, float *hx,
                                                float *hy, float *hz, float *lx, float *ly, float *lz,
                                                double (*jnear)[3][32], float2 &sx, float2 &sy, float2 &sz,
-                                               bool &had_exact) {
+                                               bool &had_exact, int mask) {
     constexpr int B = SYM_T * IPT;
     constexpr int KP = IPT / 2;
-    constexpr bool TESTS = MODE == CLS_SLOW;
-    constexpr bool IMAGE = MODE != CLS_FAST;
+    constexpr bool TESTS = MODE == MODE_SLOW;
+    const int img = MODE == MODE_SLOW ? 7 : (MODE == MODE_MASKED ? mask : 0);  // axes that take the image
 #pragma unroll 1
     for (int st = 0; st < 32; ++st) {
         const int u = (lane + st) & 31;
@@ -567,12 +572,11 @@ __device__ __forceinline__ void sorted_subtile(const SortedArgs &a, const float4
 #pragma unroll
         for (int kp = 0; kp < KP; ++kp) {
             float2 dx = p_add(pjx, xi[kp]), dy = p_add(pjy, yi[kp]), dz = p_add(pjz, zi[kp]);
-            if (IMAGE) {
-                dx = p_mic<PER>(dx, invL2, magic2, nmagic2, nL2);
-                dy = p_mic<PER>(dy, invL2, magic2, nmagic2, nL2);
-                dz = p_mic<PER>(dz, invL2, magic2, nmagic2, nL2);
-            }
-            const float2 r2 = p_fma(dx, dx, p_fma(dy, dy, p_mul(dz, dz)));
+            if (img & 1) dx = p_mic<PER>(dx, invL2, magic2, nmagic2, nL2);
+            if (img & 2) dy = p_mic<PER>(dy, invL2, magic2, nmagic2, nL2);
+            if (img & 4) dz = p_mic<PER>(dz, invL2, magic2, nmagic2, nL2);
+            const float2 dz2 = p_mul(dz, dz);
+            const float2 r2 = p_fma(dx, dx, p_fma(dy, dy, dz2));
             bool ea = false, eb = false;
             if (TESTS) {
                 const float2 sr = p_add(ki[kp], kj);
@@ -591,7 +595,7 @@ __device__ __forceinline__ void sorted_subtile(const SortedArgs &a, const float4
                     base.x = ea ? 0.f : base.x;
                     base.y = eb ? 0.f : base.y;
                 }
-                const float2 angp = p_fma(p_mul(dup2(-5.f), dz), dz, r2);
+                const float2 angp = p_fma(dz2, dup2(-5.f), r2);  // r^2 - 5 dz^2
                 const float2 angzp = p_fma(dup2(2.f), r2, angp);
                 const float2 gp = p_mul(base, angp);
                 const float2 tx = p_mul(gp, dx), ty = p_mul(gp, dy);
@@ -686,9 +690,12 @@ __global__ void __launch_bounds__(SYM_T, 4) mixed_sym_sorted_kernel(const Sorted
     float4 *C2 = C1 + CAP;  // convection only
     float2 *C3 = reinterpret_cast<float2 *>(C2 + (FORCE ? 0 : CAP));
     int *CI = reinterpret_cast<int *>(C3 + CAP);  // list entry -> j within block J (-1: padding entry)
+    unsigned char *CM = reinterpret_cast<unsigned char *>(CI + CAP);  // list entry -> class (image mask)
     __shared__ double jsum[NW][3][TJ];            // j-side sums of the chunk's list slots, per warp
     __shared__ double jnear[NW][3][32];           // exact j-side terms of the current sub-tile, per warp
-    __shared__ int wcnt[IPT][NW][3];              // entries per round, warp and class
+    __shared__ int wcnt[IPT][NW][NCLS];           // entries per round, warp and class
+    __shared__ int wpre[IPT][NW][NCLS];           // entries of the class before (round, warp)
+    __shared__ int ctot[NCLS], cbase[NCLS];       // entries per class; first entry of a class in the masked run
 
     const int nitems = a.s.t.items_total;
     if ((int)blockIdx.x >= nitems) return;
@@ -732,47 +739,63 @@ __global__ void __launch_bounds__(SYM_T, 4) mixed_sym_sorted_kernel(const Sorted
             if (diag) return (int)CLS_SLOW;
             return classify_j<PER>(sc, FORCE ? S3.x : Bv.z, blo, bhi, occ, Ls, invLs, hm_fast, m_amb);
         };
+        for (int c = tid; c < IPT * NW * NCLS; c += SYM_T) (&wcnt[0][0][0])[c] = 0;
+        __syncthreads();
 #pragma unroll 1
-        for (int k = 0; k < IPT; ++k) {
+        for (int k = 0; k < IPT; ++k) {  // pass 1: entries per (round, warp, class)
             float4 A, Bv, Q;
             float2 S3;
             float sc[3];
             load_entry(v.p0 + J * B + k * SYM_T + tid, A, Bv, Q, S3);
             const int cls = class_of(A, Bv, S3, sc);
-            const unsigned bf = __ballot_sync(0xffffffffu, cls == CLS_FAST);
-            const unsigned bm = __ballot_sync(0xffffffffu, cls == CLS_MEDIUM);
-            if (lane == 0) {
-                wcnt[k][warp][0] = __popc(bf);
-                wcnt[k][warp][1] = __popc(bm);
-                wcnt[k][warp][2] = 32 - __popc(bf) - __popc(bm);
-            }
+            const unsigned peers = __match_any_sync(0xffffffffu, cls);
+            if ((peers & lt) == 0) wcnt[k][warp][cls] = __popc(peers);
         }
         __syncthreads();
-        int tot[3] = {0, 0, 0};
-        for (int k = 0; k < IPT; ++k)
-            for (int w = 0; w < NW; ++w)
-#pragma unroll
-                for (int c = 0; c < 3; ++c) tot[c] += wcnt[k][w][c];
-        const int nf_pad = (tot[0] + 31) & ~31, nm_pad = (tot[1] + 31) & ~31, ns_pad = (tot[2] + 31) & ~31;
-        int run[3] = {0, 0, 0};  // entries of each class in the rounds before k
+        if (tid < NCLS) {  // per class: the entries before each (round, warp), and the total
+            int acc = 0;
+            for (int k = 0; k < IPT; ++k)
+                for (int w = 0; w < NW; ++w) {
+                    wpre[k][w][tid] = acc;
+                    acc += wcnt[k][w][tid];
+                }
+            ctot[tid] = acc;
+        }
+        __syncthreads();
+        if (tid == 0) {  // the masked run holds masks 1 .. 7 in mask order
+            int acc = 0;
+            for (int c = 1; c < CLS_SLOW; ++c) {
+                cbase[c] = acc;
+                acc += ctot[c];
+            }
+            cbase[0] = acc;  // (the masked run's length)
+        }
+        __syncthreads();
+        const int nA = ctot[0], A_pad = (nA + 31) & ~31;    // fast run, padded
+        const int nB = cbase[0], B_used = nB & ~31;          // masked run, cut to whole sub-tiles
+        const int nS = ctot[CLS_SLOW];
+        const int C_len = nS + (nB - B_used), C_pad = (C_len + 31) & ~31;  // slow run (+ the cut entries)
+        const int C0e = A_pad + B_used;                      // first entry of the slow run
 #pragma unroll 1
-        for (int k = 0; k < IPT; ++k) {
+        for (int k = 0; k < IPT; ++k) {  // pass 2: every entry to its place
             float4 A, Bv, Q;
             float2 S3;
             float sc[3];
             const int jb = k * SYM_T + tid;
             load_entry(v.p0 + J * B + jb, A, Bv, Q, S3);
             const int cls = class_of(A, Bv, S3, sc);
-            const unsigned bf = __ballot_sync(0xffffffffu, cls == CLS_FAST);
-            const unsigned bm = __ballot_sync(0xffffffffu, cls == CLS_MEDIUM);
-            const unsigned bs = ~(bf | bm);
-            // this thread's run: base of its class's region + entries of its class before it
-            const bool isf = cls == CLS_FAST, ism = cls == CLS_MEDIUM;
-            int e = isf ? run[0] : (ism ? nf_pad + run[1] : nf_pad + nm_pad + run[2]);
-            const int cc = isf ? 0 : (ism ? 1 : 2);
-            for (int w = 0; w < warp; ++w) e += wcnt[k][w][cc];
-            e += __popc((isf ? bf : (ism ? bm : bs)) & lt);
-            if (cls == CLS_FAST) {
+            const unsigned peers = __match_any_sync(0xffffffffu, cls);
+            const int rank = wpre[k][warp][cls] + __popc(peers & lt);
+            int e;
+            if (cls == 0) {
+                e = rank;
+            } else if (cls < CLS_SLOW) {
+                const int rb = cbase[cls] + rank;
+                e = rb < B_used ? A_pad + rb : C0e + nS + (rb - B_used);
+            } else {
+                e = C0e + rank;
+            }
+            if (cls < CLS_SLOW) {  // the fixed images of the entry's unmasked axes
                 A = make_float4(sc[0], sc[0], sc[1], sc[1]);
                 Bv.x = Bv.y = sc[2];
             }
@@ -781,22 +804,20 @@ __global__ void __launch_bounds__(SYM_T, 4) mixed_sym_sorted_kernel(const Sorted
             if (!FORCE) C2[e] = Q;
             C3[e] = S3;
             CI[e] = jb;
-            for (int w = 0; w < NW; ++w)
-#pragma unroll
-                for (int c = 0; c < 3; ++c) run[c] += wcnt[k][w][c];
+            CM[e] = (unsigned char)cls;
         }
-        // padding of the three runs: zero weight; the fast run's padding lies far from every droplet
-        if (tid < 96) {
-            const int c = tid >> 5, o = tid & 31;
-            const int start = (c == 0 ? tot[0] : (c == 1 ? nf_pad + tot[1] : nf_pad + nm_pad + tot[2])) + o;
-            const int end = c == 0 ? nf_pad : (c == 1 ? nf_pad + nm_pad : nf_pad + nm_pad + ns_pad);
-            if (start < end) {
-                const float f = c == 0 ? SORTED_FAR : 0.f;
-                C0[start] = make_float4(f, f, f, f);
-                C1[start] = make_float4(f, f, 0.f, 0.f);
-                if (!FORCE) C2[start] = make_float4(0.f, 0.f, 0.f, 0.f);
-                C3[start] = make_float2(0.f, 0.f);
-                CI[start] = -1;
+        // padding: the fast run's lies far from every droplet, the slow run's at the centre; zero weight
+        if (tid < 64) {
+            const bool fast_pad = tid < 32;
+            const int e = fast_pad ? nA + tid : C0e + C_len + (tid - 32);
+            if (e < (fast_pad ? A_pad : C0e + C_pad)) {
+                const float f = fast_pad ? SORTED_FAR : 0.f;
+                C0[e] = make_float4(f, f, f, f);
+                C1[e] = make_float4(f, f, 0.f, 0.f);
+                if (!FORCE) C2[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+                C3[e] = make_float2(0.f, 0.f);
+                CI[e] = -1;
+                CM[e] = 0;
             }
         }
 
@@ -828,23 +849,25 @@ __global__ void __launch_bounds__(SYM_T, 4) mixed_sym_sorted_kernel(const Sorted
         for (int k = 0; k < IPT; ++k) hx[k] = hy[k] = hz[k] = lx[k] = ly[k] = lz[k] = 0.f;
         __syncthreads();  // the lists are complete (and wcnt may be rewritten by the next item)
 
-        const int nfs = nf_pad >> 5, nms = nm_pad >> 5, nsub = nfs + nms + (ns_pad >> 5);
+        const int nfs = A_pad >> 5, nms = B_used >> 5, nsub = nfs + nms + (C_pad >> 5);
         double *PJ = a.s.pj + (size_t)q * 3 * plane;
         for (int c0 = 0; c0 < nsub; c0 += TJ / 32) {
             const int c1 = min(c0 + TJ / 32, nsub);
             for (int sub = c0; sub < c1; ++sub) {
                 float2 sx = make_float2(0.f, 0.f), sy = sx, sz = sx;
                 bool had_exact = false;
-#define DEM_SORTED_SUBTILE(MODE)                                                                                    \
+#define DEM_SORTED_SUBTILE(MODE, MASK)                                                                              \
     sorted_subtile<IPT, PER, FORCE, MODE>(a, C0, C1, C2, C3, CI, 32 * sub, lane, tid, warp, I, J, diag, v, inv_ell, \
                                           fscale_inv, invL2, magic2, nmagic2, nL2, hm, xi, yi, zi, ki, wi, fxi, fyi, \
-                                          fzi, ax, ay, az, hx, hy, hz, lx, ly, lz, jnear, sx, sy, sz, had_exact)
-                if (sub < nfs)
-                    DEM_SORTED_SUBTILE(CLS_FAST);
-                else if (sub < nfs + nms)
-                    DEM_SORTED_SUBTILE(CLS_MEDIUM);
-                else
-                    DEM_SORTED_SUBTILE(CLS_SLOW);
+                                          fzi, ax, ay, az, hx, hy, hz, lx, ly, lz, jnear, sx, sy, sz, had_exact, MASK)
+                if (sub < nfs) {
+                    DEM_SORTED_SUBTILE(MODE_FAST, 0);
+                } else if (sub < nfs + nms) {
+                    const int mask = __reduce_or_sync(0xffffffffu, (unsigned)CM[32 * sub + lane]);  // same in every warp
+                    DEM_SORTED_SUBTILE(MODE_MASKED, mask);
+                } else {
+                    DEM_SORTED_SUBTILE(MODE_SLOW, 7);
+                }
 #undef DEM_SORTED_SUBTILE
                 if (!diag) {  // the sums are back with the lanes owning their list entries
                     double vx = (double)(sx.x + sx.y), vy = (double)(sy.x + sy.y), vz = (double)(sz.x + sz.y);
