@@ -534,6 +534,28 @@ __device__ __forceinline__ int classify_j(float sc[3], float kj, const float4 &b
 // sub-tile loops: MODE_FAST (no image), MODE_MASKED (image on the axes of a uniform mask), MODE_SLOW
 enum { MODE_FAST = 0, MODE_MASKED = 1, MODE_SLOW = 2 };
 
+// Build knobs of the sorted pair kernel: resident CTAs per SM its registers are
+// budgeted for, and how the force pass forms r^-7 (1: 2^(-3.5 log2 r^2) from the
+// PTX approximate lg2 / ex2, two MUFU operations and one multiply; 0: rsqrt and
+// four multiplies).  The relative error of either is below 1e-6.
+#ifndef DEM_SORTED_MIN_CTAS
+#define DEM_SORTED_MIN_CTAS 4
+#endif
+#ifndef DEM_FORCE_POW_EXP2
+#define DEM_FORCE_POW_EXP2 1
+#endif
+
+__device__ __forceinline__ float lg2_approx(float x) {
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 template <int IPT, bool PER, bool FORCE, int MODE>
 __device__ __forceinline__ void sorted_subtile(const SortedArgs &a, const float4 *C0, const float4 *C1,
                                                const float4 *C2, const float2 *C3, const int *CI, int e0, int lane,
@@ -586,11 +608,16 @@ __device__ __forceinline__ void sorted_subtile(const SortedArgs &a, const float4
             }
             ex[2 * kp] = ea;
             ex[2 * kp + 1] = eb;
-            float2 rinv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
             if (FORCE) {
+#if DEM_FORCE_POW_EXP2
+                const float2 e7 = p_mul(dup2(-3.5f), make_float2(lg2_approx(r2.x), lg2_approx(r2.y)));
+                float2 base = make_float2(ex2_approx(e7.x), ex2_approx(e7.y));  // r^-7
+#else
+                const float2 rinv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
                 const float2 rinv2 = p_mul(rinv, rinv);
                 const float2 rinv4 = p_mul(rinv2, rinv2);
                 float2 base = p_mul(rinv4, p_mul(rinv2, rinv));  // r^-7
+#endif
                 if (TESTS) {
                     base.x = ea ? 0.f : base.x;
                     base.y = eb ? 0.f : base.y;
@@ -607,6 +634,7 @@ __device__ __forceinline__ void sorted_subtile(const SortedArgs &a, const float4
                 sy = p_fma(wi[kp], ty, sy);
                 sz = p_fma(wi[kp], tz, sz);
             } else {
+                float2 rinv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
                 if (TESTS) {
                     rinv.x = ea ? 0.f : rinv.x;
                     rinv.y = eb ? 0.f : rinv.y;
@@ -678,7 +706,7 @@ __device__ __forceinline__ void sorted_subtile(const SortedArgs &a, const float4
 }
 
 template <int IPT, bool PER, bool FORCE>
-__global__ void __launch_bounds__(SYM_T, 4) mixed_sym_sorted_kernel(const SortedArgs a) {
+__global__ void __launch_bounds__(SYM_T, DEM_SORTED_MIN_CTAS) mixed_sym_sorted_kernel(const SortedArgs a) {
     static_assert(IPT % 2 == 0, "two i's per packed operation");
     constexpr int B = SYM_T * IPT;
     constexpr int KP = IPT / 2;
