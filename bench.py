@@ -350,6 +350,7 @@ def run_ours(args, rank, world, device):
         sampler.start()
         time.sleep(0.4)
     st.ctx.profile(True)
+    st.det._ctx.profile(True)  # the detector has its own context
     from dem._native import launch_count
 
     stream = torch.cuda.current_stream()
@@ -359,12 +360,14 @@ def run_ours(args, rank, world, device):
     launches = launch_count() - launches0
     total_ms = float(sum(step_ms))
     kern = {}
-    for name in ("mixed_force_pass", "mixed_convection_pass", "fp64_force_pass", "fp64_convection_pass",
-                 "hash_detect"):
-        ms, cnt = st.ctx.profile_read(name)
-        if cnt:
-            kern[name] = (ms, cnt)
+    for c, names in ((st.ctx, ("mixed_force_pass", "mixed_convection_pass", "fp64_force_pass", "fp64_convection_pass")),
+                     (st.det._ctx, ("hash_detect",))):
+        for name in names:
+            ms, cnt = c.profile_read(name)
+            if cnt:
+                kern[name] = (ms, cnt)
     st.ctx.profile(False)
+    st.det._ctx.profile(False)
     schedule = st.ctx.plan(st.n, True) if args.precision == "mixed" else "fp64"
     clocks = sampler.stop() if sampler else None
     from dem.replicas import job_time_ms
@@ -819,6 +822,7 @@ def run_tree(args, device):
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     c0 = launch_count()
     ctx.profile(True)
+    det._ctx.profile(True)  # the detector has its own context
     for k in range(args.steps):
         ev[k][0].record()
         step()
@@ -826,11 +830,13 @@ def run_tree(args, device):
     torch.cuda.synchronize()
     launches = launch_count() - c0
     kern = {}
-    for name in ("bh_build", "bh_force_walk", "bh_velocity_walk", "hash_detect"):
-        ms, cnt = ctx.profile_read(name)
-        if cnt:
-            kern[name] = ms / cnt
+    for c, names in ((ctx, ("bh_build", "bh_force_walk", "bh_velocity_walk")), (det._ctx, ("hash_detect",))):
+        for name in names:
+            ms, cnt = c.profile_read(name)
+            if cnt:
+                kern[name] = ms / cnt
     ctx.profile(False)
+    det._ctx.profile(False)
     clocks = sampler.stop()
     step_ms = [a.elapsed_time(b) for a, b in ev]
     st = tc.stats()  # counters of the last walk (velocity); the force walk visits the same tree

@@ -176,7 +176,7 @@ int dem_batch_create(dem_ctx *ctx, int nbox, const int64_t *offsets, const doubl
         ioff[nbox] = (int)it;
         t.npad = (int)np;
         t.items = (int)it;
-        work = std::max(work, sym_workspace_bytes(np, it, t.B) + sym_sorted_extra_bytes(b->n, np, t.B));
+        work = std::max(work, sym_workspace_bytes(np, it, t.B) + sym_sorted_extra_bytes(b->n, np, it, t.B));
         if ((rc = dem_check_cuda(ctx, cudaMalloc((void **)&t.poff, sizeof(int) * (nbox + 1)), "batch tables")) ||
             (rc = dem_check_cuda(ctx, cudaMalloc((void **)&t.ioff, sizeof(int) * (nbox + 1)), "batch tables")) ||
             (rc = dem_check_cuda(ctx, cudaMemcpy(t.poff, poff.data(), sizeof(int) * (nbox + 1), cudaMemcpyHostToDevice),

@@ -513,40 +513,47 @@ __global__ void top_force_partial_kernel(BhNodes nd, TopPlan tp, const double *_
         for (int q = 0; q < 12; ++q) part[(size_t)blockIdx.x * 12 + q] = v[q];
 }
 
-// One thread per top node: its chunk partials added in chunk order, then node_r3_kernel's final step.
-__global__ void top_r3_finish_kernel(BhNodes nd, TopPlan tp, const double *__restrict__ part,
-                                     const double *__restrict__ ps, int cap, const double *__restrict__ geom,
-                                     const uint32_t *__restrict__ keys) {
-    const int total = tp.node0[tp.levels - 1] + tp.nodes[tp.levels - 1] - tp.node0[0];
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= total) return;
-    const int k = tp.node0[0] + t;
+// One warp per top node: lane l adds chunks l, l + 32, ... in order, then the lanes' sums are added by a
+// fixed shuffle tree (deterministic), then node_r3_kernel's final step.
+template <int NV>
+__device__ __forceinline__ void top_partials(const TopPlan &tp, int k, const double *__restrict__ part, double (&v)[NV]) {
+    const int lane = threadIdx.x & 31;
     int l = 0;
     while (l + 1 < tp.levels && k >= tp.node0[l + 1]) ++l;
     const int nc = tp.chunks[l];
     const size_t q0 = (size_t)tp.cta0[l] + (size_t)(k - tp.node0[l]) * nc;
-    double v[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (int c = 0; c < nc; ++c)
-        for (int q = 0; q < 10; ++q) v[q] += part[(q0 + c) * 12 + q];
+    for (int q = 0; q < NV; ++q) v[q] = 0.0;
+    for (int c = lane; c < nc; c += 32)
+        for (int q = 0; q < NV; ++q) v[q] += part[(q0 + c) * 12 + q];
+    for (int q = 0; q < NV; ++q)
+        for (int o = 16; o; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+}
+
+__global__ void top_r3_finish_kernel(BhNodes nd, TopPlan tp, const double *__restrict__ part,
+                                     const double *__restrict__ ps, int cap, const double *__restrict__ geom,
+                                     const uint32_t *__restrict__ keys) {
+    const int total = tp.node0[tp.levels - 1] + tp.nodes[tp.levels - 1] - tp.node0[0];
+    const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (t >= total) return;  // warp-uniform
+    const int k = tp.node0[0] + t;
+    double v[10];
+    top_partials<10>(tp, k, part, v);
+    if ((threadIdx.x & 31) != 0) return;
     const int s0 = nd.start[k], cnt = nd.count[k];
     const double rx = cnt > 0 ? ps[s0] : 0.0, ry = cnt > 0 ? ps[cap + s0] : 0.0,
                  rz = cnt > 0 ? ps[2 * (size_t)cap + s0] : 0.0;
     r3_finish(nd, k, v, rx, ry, rz, s0, cnt, geom[0], geom[1], geom[2], geom[3], keys);
 }
 
-// One thread per top node: force sum and dipole from its chunk partials, in chunk order.
+// One warp per top node: force sum and dipole from its chunk partials (see top_partials).
 __global__ void top_force_finish_kernel(BhNodes nd, TopPlan tp, const double *__restrict__ part) {
     const int total = tp.node0[tp.levels - 1] + tp.nodes[tp.levels - 1] - tp.node0[0];
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= total) return;
+    const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (t >= total) return;  // warp-uniform
     const int k = tp.node0[0] + t;
-    int l = 0;
-    while (l + 1 < tp.levels && k >= tp.node0[l + 1]) ++l;
-    const int nc = tp.chunks[l];
-    const size_t q0 = (size_t)tp.cta0[l] + (size_t)(k - tp.node0[l]) * nc;
-    double v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (int c = 0; c < nc; ++c)
-        for (int q = 0; q < 12; ++q) v[q] += part[(q0 + c) * 12 + q];
+    double v[12];
+    top_partials<12>(tp, k, part, v);
+    if ((threadIdx.x & 31) != 0) return;
     for (int q = 0; q < 3; ++q)  // v = (F, D row-major): the record's order
         nd.fd[3 * (size_t)k + q] = make_float4((float)v[4 * q], (float)v[4 * q + 1], (float)v[4 * q + 2],
                                                (float)v[4 * q + 3]);
@@ -624,76 +631,6 @@ __device__ __forceinline__ void quad_force(float x, float y, float z, const floa
     gz += (a1 * tz + a2 * z - 3.f * Bz) * (1.f / 6.f);
 }
 
-// ---- two accepted nodes at once, in packed FP32x2 (the .x and .y halves are two nodes) ----
-__device__ __forceinline__ float2 q_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 q_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 q_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-__device__ __forceinline__ float2 q_dup(float v) { return make_float2(v, v); }
-constexpr float Q_MAGIC = 12582912.0f;  // 1.5 * 2^23: (x + M) - M == rint(x) for |x| < 2^22
-
-// quad_force for two nodes: x, y, z = D (node centre - target), Q in (qxx, qxy, qxz, qyy, qyz, qzz), tr = trace
-__device__ __forceinline__ void quad_force2(float2 x, float2 y, float2 z, float2 qxx, float2 qxy, float2 qxz,
-                                            float2 qyy, float2 qyz, float2 qzz, float2 tr, float2 r7, float2 rinv2,
-                                            float2 &gx, float2 &gy, float2 &gz) {
-    const float2 r9 = q_mul(r7, rinv2), r11 = q_mul(r9, rinv2);
-    const float2 Qx = q_fma(qxx, x, q_fma(qxy, y, q_mul(qxz, z)));
-    const float2 Qy = q_fma(qxy, x, q_fma(qyy, y, q_mul(qyz, z)));
-    const float2 Qz = q_fma(qxz, x, q_fma(qyz, y, q_mul(qzz, z)));
-    const float2 xQx = q_fma(x, Qx, q_fma(y, Qy, q_mul(z, Qz)));
-    const float2 a1 = q_mul(q_dup(15.f), r7), a2 = q_mul(q_mul(q_dup(-105.f), xQx), r9);
-    const float2 zz = q_mul(z, z);
-    const float2 b1 = q_mul(q_mul(q_dup(35.f), zz), r9);
-    // b2 = -10 qzz r7 + 140 z Qz r9 - 315 z^2 xQx r11
-    const float2 b2 = q_fma(q_mul(q_dup(-10.f), qzz), r7,
-                            q_fma(q_mul(q_dup(140.f), q_mul(z, Qz)), r9, q_mul(q_mul(q_dup(-315.f), q_mul(zz, xQx)), r11)));
-    const float2 tx = q_fma(q_dup(2.f), Qx, q_mul(tr, x)), ty = q_fma(q_dup(2.f), Qy, q_mul(tr, y)),
-                 tz = q_fma(q_dup(2.f), Qz, q_mul(tr, z));
-    const float2 zr7 = q_mul(q_mul(q_dup(-20.f), z), r7);  // -20 z r7
-    const float2 Bx = q_fma(b1, tx, q_fma(b2, x, q_mul(zr7, qxz)));
-    const float2 By = q_fma(b1, ty, q_fma(b2, y, q_mul(zr7, qyz)));
-    // Bz = b1 tz + b2 z - 20 z qzz r7 - 20 Qz r7 - 10 z (tr r7 - 7 xQx r9)
-    const float2 inner = q_fma(tr, r7, q_mul(q_mul(q_dup(-7.f), xQx), r9));
-    const float2 Bz = q_fma(b1, tz, q_fma(b2, z, q_fma(zr7, qzz, q_fma(q_mul(q_dup(-20.f), Qz), r7,
-                                                                         q_mul(q_mul(q_dup(-10.f), z), inner)))));
-    const float2 s6 = q_dup(1.f / 6.f), m3 = q_dup(-3.f);
-    gx = q_fma(q_fma(a1, tx, q_fma(a2, x, q_mul(m3, Bx))), s6, gx);
-    gy = q_fma(q_fma(a1, ty, q_fma(a2, y, q_mul(m3, By))), s6, gy);
-    gz = q_fma(q_fma(a1, tz, q_fma(a2, z, q_mul(m3, Bz))), s6, gz);
-}
-
-// Fields of a listed node (two nodes per float2: .x, .y).  Force walk: centre (3, / ell), R^3, Q (6), trace Q.
-// Velocity walk: centre (3), force sum F (3), the dipole D split as diagonal (D00, D11, D22), symmetric sums
-// (D01 + D10, D02 + D20, D12 + D21), antisymmetric differences a = (D10 - D01, D20 - D02, D21 - D12), -a, and
-// -trace D: then e^T D e = e_x (D00 e_x + s1 e_y + s2 e_z) + e_y (D11 e_y + s3 e_z) + D22 e_z^2 and
-// D^T e - D e = (a1 e_y + a2 e_z, -a1 e_x + a3 e_z, -a2 e_x - a3 e_y).
-constexpr int BH_NF_FORCE = 11, BH_NF_VEL = 19;
-constexpr int BH_LIST = 32;  // node pairs per warp list
-
-// The velocity of a target at e = x_i - c (per node half) from two listed nodes: Stokeslet of the force sum
-// plus the dipole correction (flat_tree.py:1215-1265), accumulated into (ax, ay, az).
-__device__ __forceinline__ void stokes_dipole2(float2 ex, float2 ey, float2 ez, const float2 *f, float2 rinv,
-                                               float2 rinv2, float2 &ax, float2 &ay, float2 &az) {
-    const float2 Fx = f[3], Fy = f[4], Fz = f[5];
-    const float2 dot = q_fma(ex, Fx, q_fma(ey, Fy, q_mul(ez, Fz)));
-    const float2 sc = q_mul(dot, rinv2);
-    ax = q_fma(rinv, q_fma(ex, sc, Fx), ax);
-    ay = q_fma(rinv, q_fma(ey, sc, Fy), ay);
-    az = q_fma(rinv, q_fma(ez, sc, Fz), az);
-    const float2 D00 = f[6], D11 = f[7], D22 = f[8], s1 = f[9], s2 = f[10], s3 = f[11];
-    const float2 a1 = f[12], a2 = f[13], a3 = f[14], na1 = f[15], na2 = f[16], na3 = f[17], ntr = f[18];
-    const float2 t1 = q_fma(D00, ex, q_fma(s1, ey, q_mul(s2, ez)));
-    const float2 t2 = q_fma(D11, ey, q_mul(s3, ez));
-    const float2 q = q_fma(ex, t1, q_fma(ey, t2, q_mul(q_mul(D22, ez), ez)));  // e^T D e
-    const float2 rinv3 = q_mul(rinv, rinv2);
-    const float2 q3 = q_mul(q_mul(q_dup(3.f), q), q_mul(rinv3, rinv2));  // 3 q / r^5
-    const float2 hx = q_fma(a1, ey, q_fma(a2, ez, q_mul(ntr, ex)));
-    const float2 hy = q_fma(na1, ex, q_fma(a3, ez, q_mul(ntr, ey)));
-    const float2 hz = q_fma(na2, ex, q_fma(na3, ey, q_mul(ntr, ez)));
-    ax = q_fma(rinv3, hx, q_fma(q3, ex, ax));
-    ay = q_fma(rinv3, hy, q_fma(q3, ey, ay));
-    az = q_fma(rinv3, hz, q_fma(q3, ez, az));
-}
-
 struct BhWalk {
     int n, cap, node_count;
     const double *ps;                  // sorted x, y, z, r (FP64, metres)
@@ -732,9 +669,6 @@ __global__ void __launch_bounds__(BH_T, FORCE ? 6 : (CORR ? 5 : 7)) bh_walk_kern
                                                        double *__restrict__ ox, double *__restrict__ oy,
                                                        double *__restrict__ oz, double *__restrict__ fsort_out) {
     __shared__ int stack[BH_T / 32][BH_STACK];
-    // accepted nodes awaiting their terms (not for the correction walk): node 2 p + h in half h of pair p
-    constexpr int NF = FORCE ? BH_NF_FORCE : BH_NF_VEL;
-    __shared__ float2 lst[CORR ? 1 : BH_T / 32][CORR ? 1 : BH_LIST][NF];
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
     const int n = w.n, cap = w.cap;
     const double inv_ell = pow2_inv_of(w.scales[0]);
@@ -764,64 +698,6 @@ __global__ void __launch_bounds__(BH_T, FORCE ? 6 : (CORR ? 5 : 7)) bh_walk_kern
         const float ris = (float)(ri * inv_ell);
         float ax = 0.f, ay = 0.f, az = 0.f;
         float cx = 0.f, cy = 0.f, cz = 0.f;  // correction sums (CORR)
-        int nl = 0;                          // listed nodes (warp-uniform)
-        // the terms of the listed nodes, two per packed operation; the list is emptied
-        auto flush = [&]() {
-            if (CORR || nl == 0) return;
-            if (nl & 1) {  // odd count: the last half repeats the first node's centre with zero weights
-                if (lane == 0) {
-                    float *d = reinterpret_cast<float *>(&lst[wp][nl >> 1][0]) + 1;
-                    const float *c0 = reinterpret_cast<const float *>(&lst[wp][0][0]);
-                    for (int f = 0; f < NF; ++f) d[2 * f] = f < 3 ? c0[2 * f] : 0.f;
-                }
-                ++nl;
-            }
-            __syncwarp();
-            float2 gx = make_float2(0.f, 0.f), gy = gx, gz = gx;
-            const float2 mag = q_dup(Q_MAGIC), nmag = q_dup(-Q_MAGIC), nL = q_dup(-Ls), iL = q_dup(invLs);
-            for (int pp = 0; pp < (nl >> 1); ++pp) {
-                const float2 *f = lst[wp][pp];
-                // D = c - x_i (force walk); e = x_i - c (velocity walk); minimum image
-                float2 dx, dy, dz;
-                if (FORCE) {
-                    dx = q_add(f[0], q_dup(-xs));
-                    dy = q_add(f[1], q_dup(-ys));
-                    dz = q_add(f[2], q_dup(-zs));
-                } else {
-                    dx = q_fma(f[0], q_dup(-1.f), q_dup(xs));
-                    dy = q_fma(f[1], q_dup(-1.f), q_dup(ys));
-                    dz = q_fma(f[2], q_dup(-1.f), q_dup(zs));
-                }
-                if (PER) {
-                    dx = q_fma(nL, q_add(q_fma(dx, iL, mag), nmag), dx);
-                    dy = q_fma(nL, q_add(q_fma(dy, iL, mag), nmag), dy);
-                    dz = q_fma(nL, q_add(q_fma(dz, iL, mag), nmag), dz);
-                }
-                const float2 dz2 = q_mul(dz, dz);
-                const float2 sxy = q_fma(dx, dx, q_mul(dy, dy));
-                const float2 D2 = q_add(sxy, dz2);
-                const float2 rinv = make_float2(rsqrtf(D2.x), rsqrtf(D2.y)), rinv2 = q_mul(rinv, rinv);
-                if (FORCE) {
-                    const float2 r7 = q_mul(q_mul(rinv2, rinv2), q_mul(rinv2, rinv));
-                    const float2 b = q_mul(f[3], r7);
-                    const float2 nsxy = q_mul(sxy, q_dup(-1.f));
-                    const float2 ang = q_fma(q_mul(q_dup(4.f), dz), dz, nsxy);      // 4 dz^2 - dx^2 - dy^2
-                    const float2 angz = q_fma(q_mul(q_dup(2.f), dz), dz, q_mul(q_dup(3.f), nsxy));
-                    const float2 bang = q_mul(b, ang);
-                    gx = q_fma(bang, dx, gx);
-                    gy = q_fma(bang, dy, gy);
-                    gz = q_fma(q_mul(b, angz), dz, gz);
-                    quad_force2(dx, dy, dz, f[4], f[5], f[6], f[7], f[8], f[9], f[10], r7, rinv2, gx, gy, gz);
-                } else {
-                    stokes_dipole2(dx, dy, dz, f, rinv, rinv2, gx, gy, gz);
-                }
-            }
-            __syncwarp();  // the list is refilled after this
-            ax += gx.x + gx.y;
-            ay += gy.x + gy.y;
-            az += gz.x + gz.y;
-            nl = 0;
-        };
         int sp = 1;
         if (lane == 0) stack[wp][0] = 0;
         __syncwarp();
@@ -869,48 +745,7 @@ __global__ void __launch_bounds__(BH_T, FORCE ? 6 : (CORR ? 5 : 7)) bh_walk_kern
                 accept = accept && fabsf(dx) < hw && fabsf(dy) < hw && fabsf(dz) < hw;
             }
             accept = accept || !valid;
-            if (!CORR && __all_sync(0xffffffffu, accept)) {  // to the list
-                if (lane == 0) {
-                    float *d = reinterpret_cast<float *>(&lst[wp][nl >> 1][0]) + (nl & 1);
-                    d[0] = cs.x;
-                    d[2] = cs.y;
-                    d[4] = cs.z;
-                    if (FORCE) {
-                        const float4 qa = w.nd.qr[2 * (size_t)node];  // (Qxx, Qxy, Qxz, Qyy); rec = (Qyz, Qzz, R^3, 0)
-                        d[6] = rec.z;
-                        d[8] = qa.x;
-                        d[10] = qa.y;
-                        d[12] = qa.z;
-                        d[14] = qa.w;
-                        d[16] = rec.x;
-                        d[18] = rec.y;
-                        d[20] = qa.x + qa.w + rec.y;
-                    } else {  // rec = (Fx, Fy, Fz, D00); D01 D02 D10 D11 | D12 D20 D21 D22
-                        const float4 d1 = w.nd.fd[3 * (size_t)node + 1], d2 = w.nd.fd[3 * (size_t)node + 2];
-                        const float a1 = d1.z - d1.x, a2 = d2.y - d1.y, a3 = d2.z - d2.x;
-                        d[6] = rec.x;
-                        d[8] = rec.y;
-                        d[10] = rec.z;
-                        d[12] = rec.w;
-                        d[14] = d1.w;
-                        d[16] = d2.w;
-                        d[18] = d1.x + d1.z;
-                        d[20] = d1.y + d2.y;
-                        d[22] = d2.x + d2.z;
-                        d[24] = a1;
-                        d[26] = a2;
-                        d[28] = a3;
-                        d[30] = -a1;
-                        d[32] = -a2;
-                        d[34] = -a3;
-                        d[36] = -(rec.w + d1.w + d2.w);
-                    }
-                }
-                if (valid) ++nodes;
-                if (++nl == 2 * BH_LIST) flush();
-                continue;
-            }
-            if (CORR && __all_sync(0xffffffffu, accept)) {
+            if (__all_sync(0xffffffffu, accept)) {
                 if (valid) {
                     ++nodes;
                     const float rinv = rsqrtf(D2), rinv2 = rinv * rinv;
@@ -997,7 +832,6 @@ __global__ void __launch_bounds__(BH_T, FORCE ? 6 : (CORR ? 5 : 7)) bh_walk_kern
             sp += nch;
             __syncwarp();
         }
-        flush();
         if (broken && lane == 0) raise_device_error(w.err, DEM_DEVERR_NODE_OVERFLOW);
         if (valid) {
             const int i = w.idx[si];
@@ -1371,8 +1205,8 @@ int dem_bh_build(dem_bh *b, int n, const double *x, const double *y, const doubl
     const TopPlan tp = top_plan(b);
     const int top = tp.node0[tp.levels - 1] + tp.nodes[tp.levels - 1];
     top_r3_partial_kernel<<<tp.cta0[tp.levels], TOP_T, 0, counted(s)>>>(b->nd, tp, b->ps, b->capacity, b->top_part);
-    top_r3_finish_kernel<<<(top + 127) / 128, 128, 0, counted(s)>>>(b->nd, tp, b->top_part, b->ps, b->capacity,
-                                                                    b->geom, b->keys[0]);
+    top_r3_finish_kernel<<<(top + 3) / 4, 128, 0, counted(s)>>>(b->nd, tp, b->top_part, b->ps, b->capacity,
+                                                                b->geom, b->keys[0]);
     if (le > top)
         node_r3_kernel<false><<<grid_of(ctx, 32LL * (le - top)), 256, 0, counted(s)>>>(b->nd, top, le, b->ps,
                                                                                        b->capacity, b->geom,
@@ -1453,7 +1287,7 @@ int dem_bh_velocity(dem_bh *b, const double *fx, const double *fy, const double 
     const int top = tp.node0[tp.levels - 1] + tp.nodes[tp.levels - 1];
     top_force_partial_kernel<<<tp.cta0[tp.levels], TOP_T, 0, counted(s)>>>(b->nd, tp, b->ps, b->fsort, b->capacity,
                                                                             b->top_part);
-    top_force_finish_kernel<<<(top + 127) / 128, 128, 0, counted(s)>>>(b->nd, tp, b->top_part);
+    top_force_finish_kernel<<<(top + 3) / 4, 128, 0, counted(s)>>>(b->nd, tp, b->top_part);
     if (le > top)
         node_force_kernel<false><<<grid_of(ctx, 32LL * (le - top)), 256, 0, counted(s)>>>(b->nd, top, le, b->ps,
                                                                                           b->fsort, b->capacity);

@@ -292,7 +292,7 @@ int run_sym_pass(dem_ctx *ctx, int n, int ipt, bool per, const MixedArgs &m, dou
 // 65,536): split best to N = 4,096 (sym4 4.3x slower at N = 2,000), sym2 at
 // 8,192 - 12,288, sym4 from 16,384 on; the crossovers sit at ~3.5 block pairs
 // per SM.
-constexpr size_t SYM_BUDGET = size_t(4) << 30;
+constexpr size_t SYM_BUDGET = size_t(12) << 30;
 static long long sym_block_pairs(int n, int ipt) {
     const long long nb = (n + 128LL * ipt - 1) / (128LL * ipt);
     return nb * (nb + 1) / 2;

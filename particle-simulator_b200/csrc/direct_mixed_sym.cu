@@ -556,7 +556,9 @@ __device__ __forceinline__ float ex2_approx(float x) {
     return y;
 }
 
-template <int IPT, bool PER, bool FORCE, int MODE>
+// MASK: the axes that take the minimum image in MODE_MASKED (a compile-time constant, so that a sub-tile
+// pays only for its own axes).
+template <int IPT, bool PER, bool FORCE, int MODE, int MASK>
 __device__ __forceinline__ void sorted_subtile(const SortedArgs &a, const float4 *C0, const float4 *C1,
                                                const float4 *C2, const float2 *C3, const int *CI, int e0, int lane,
                                                int tid, int warp, int I, int J, bool diag, const BoxView &v,
@@ -567,11 +569,11 @@ __device__ __forceinline__ void sorted_subtile(const SortedArgs &a, const float4
                                                const float2 *fzi, float2 *ax, float2 *ay, float2 *az, float *hx,
                                                float *hy, float *hz, float *lx, float *ly, float *lz,
                                                double (*jnear)[3][32], float2 &sx, float2 &sy, float2 &sz,
-                                               bool &had_exact, int mask) {
+                                               bool &had_exact) {
     constexpr int B = SYM_T * IPT;
     constexpr int KP = IPT / 2;
     constexpr bool TESTS = MODE == MODE_SLOW;
-    const int img = MODE == MODE_SLOW ? 7 : (MODE == MODE_MASKED ? mask : 0);  // axes that take the image
+    constexpr int img = MODE == MODE_SLOW ? 7 : (MODE == MODE_MASKED ? MASK : 0);  // axes that take the image
 #pragma unroll 1
     for (int st = 0; st < 32; ++st) {
         const int u = (lane + st) & 31;
@@ -719,7 +721,6 @@ __global__ void __launch_bounds__(SYM_T, DEM_SORTED_MIN_CTAS) mixed_sym_sorted_k
     float2 *C3 = reinterpret_cast<float2 *>(C2 + (FORCE ? 0 : CAP));
     int *CI = reinterpret_cast<int *>(C3 + CAP);  // list entry -> j within block J (-1: padding entry)
     unsigned char *CM = reinterpret_cast<unsigned char *>(CI + CAP);  // list entry -> class (image mask)
-    __shared__ double jsum[NW][3][TJ];            // j-side sums of the chunk's list slots, per warp
     __shared__ double jnear[NW][3][32];           // exact j-side terms of the current sub-tile, per warp
     __shared__ int wcnt[IPT][NW][NCLS];           // entries per round, warp and class
     __shared__ int wpre[IPT][NW][NCLS];           // entries of the class before (round, warp)
@@ -878,21 +879,30 @@ __global__ void __launch_bounds__(SYM_T, DEM_SORTED_MIN_CTAS) mixed_sym_sorted_k
         __syncthreads();  // the lists are complete (and wcnt may be rewritten by the next item)
 
         const int nfs = A_pad >> 5, nms = B_used >> 5, nsub = nfs + nms + (C_pad >> 5);
-        double *PJ = a.s.pj + (size_t)q * 3 * plane;
-        for (int c0 = 0; c0 < nsub; c0 += TJ / 32) {
-            const int c1 = min(c0 + TJ / 32, nsub);
-            for (int sub = c0; sub < c1; ++sub) {
+        // j-side partials of the item, interleaved per droplet: [j][warp][3] (the reduction adds the warps in order)
+        double *PJ = a.s.pj + (size_t)q * NW * 3 * plane + warp * 3;
+        {
+            for (int sub = 0; sub < nsub; ++sub) {
                 float2 sx = make_float2(0.f, 0.f), sy = sx, sz = sx;
                 bool had_exact = false;
-#define DEM_SORTED_SUBTILE(MODE, MASK)                                                                              \
-    sorted_subtile<IPT, PER, FORCE, MODE>(a, C0, C1, C2, C3, CI, 32 * sub, lane, tid, warp, I, J, diag, v, inv_ell, \
-                                          fscale_inv, invL2, magic2, nmagic2, nL2, hm, xi, yi, zi, ki, wi, fxi, fyi, \
-                                          fzi, ax, ay, az, hx, hy, hz, lx, ly, lz, jnear, sx, sy, sz, had_exact, MASK)
+#define DEM_SORTED_SUBTILE(MODE, MASK)                                                                            \
+    sorted_subtile<IPT, PER, FORCE, MODE, MASK>(a, C0, C1, C2, C3, CI, 32 * sub, lane, tid, warp, I, J, diag, v,   \
+                                                inv_ell, fscale_inv, invL2, magic2, nmagic2, nL2, hm, xi, yi, zi, ki, \
+                                                wi, fxi, fyi, fzi, ax, ay, az, hx, hy, hz, lx, ly, lz, jnear, sx, sy, \
+                                                sz, had_exact)
                 if (sub < nfs) {
                     DEM_SORTED_SUBTILE(MODE_FAST, 0);
                 } else if (sub < nfs + nms) {
                     const int mask = __reduce_or_sync(0xffffffffu, (unsigned)CM[32 * sub + lane]);  // same in every warp
-                    DEM_SORTED_SUBTILE(MODE_MASKED, mask);
+                    switch (mask) {
+                        case 1: DEM_SORTED_SUBTILE(MODE_MASKED, 1); break;
+                        case 2: DEM_SORTED_SUBTILE(MODE_MASKED, 2); break;
+                        case 3: DEM_SORTED_SUBTILE(MODE_MASKED, 3); break;
+                        case 4: DEM_SORTED_SUBTILE(MODE_MASKED, 4); break;
+                        case 5: DEM_SORTED_SUBTILE(MODE_MASKED, 5); break;
+                        case 6: DEM_SORTED_SUBTILE(MODE_MASKED, 6); break;
+                        default: DEM_SORTED_SUBTILE(MODE_MASKED, 7); break;
+                    }
                 } else {
                     DEM_SORTED_SUBTILE(MODE_SLOW, 7);
                 }
@@ -907,10 +917,13 @@ __global__ void __launch_bounds__(SYM_T, DEM_SORTED_MIN_CTAS) mixed_sym_sorted_k
                         jnear[warp][0][lane] = jnear[warp][1][lane] = jnear[warp][2][lane] = 0.0;
                         __syncwarp();
                     }
-                    const int slot = (sub - c0) * 32 + lane;
-                    jsum[warp][0][slot] = vx;
-                    jsum[warp][1][slot] = vy;
-                    jsum[warp][2][slot] = vz;
+                    const int jo = CI[32 * sub + lane];
+                    if (jo >= 0) {
+                        double *d = PJ + (size_t)jo * NW * 3;
+                        d[0] = vx;
+                        d[1] = vy;
+                        d[2] = vz;
+                    }
                 }
                 if ((sub & 1) || sub == nsub - 1) {  // fold the FP32 i-side runs every 64 j and at the end
 #pragma unroll
@@ -925,32 +938,16 @@ __global__ void __launch_bounds__(SYM_T, DEM_SORTED_MIN_CTAS) mixed_sym_sorted_k
                     }
                 }
             }
-            __syncthreads();
-            if (!diag) {  // combine the warps in a fixed order, per list slot, into the j's partial
-                const int sub = c0 + (tid >> 5);
-                if (sub < c1) {
-                    const int jo = CI[32 * sub + (tid & 31)];
-                    if (jo >= 0) {
-#pragma unroll
-                        for (int c = 0; c < 3; ++c) {
-                            double w = 0.0;
-#pragma unroll
-                            for (int wp = 0; wp < NW; ++wp) w += jsum[wp][c][tid];
-                            PJ[c * plane + jo] = w;
-                        }
-                    }
-                }
-            }
-            __syncthreads();
         }
-        double *PI = a.s.pi + (size_t)q * 3 * plane;
+        __syncthreads();  // every warp is done with the lists before the next item rebuilds them
+        double *PI = a.s.pi + (size_t)q * 3 * plane;  // interleaved per droplet: [i][3]
         const double sg = FORCE ? -1.0 : 1.0;
 #pragma unroll
         for (int k = 0; k < IPT; ++k) {
             const int li = k * SYM_T + tid;
-            PI[li] = sg * ((double)hx[k] + (double)lx[k]);
-            PI[plane + li] = sg * ((double)hy[k] + (double)ly[k]);
-            PI[2 * plane + li] = sg * ((double)hz[k] + (double)lz[k]);
+            PI[3 * li] = sg * ((double)hx[k] + (double)lx[k]);
+            PI[3 * li + 1] = sg * ((double)hy[k] + (double)ly[k]);
+            PI[3 * li + 2] = sg * ((double)hz[k] + (double)lz[k]);
         }
     }
 }
@@ -1083,52 +1080,91 @@ __global__ void prep_sym_kernel(const SymBoxes t, const double *__restrict__ x, 
 }
 
 // out_c[d] = factor_d * (sum over items (K, J>=K) of the i side + sum over items (I<K, K) of the j side)
-template <bool FORCE>
-__global__ void reduce_sym_kernel(const SymBoxes t, int B, const double *__restrict__ pi, const double *__restrict__ pj,
-                                  const double *__restrict__ r, double coeff, double *__restrict__ ox,
-                                  double *__restrict__ oy, double *__restrict__ oz, uint32_t *err,
-                                  const int32_t *__restrict__ perm) {
+// PLANAR (mixed_sym_kernel): partials as planes [item][3][B]; else (the sorted kernel) interleaved per droplet,
+// i side [item][B][3] and j side [item][B][JW][3], so that a thread reads contiguous records.
+// RED_SPLIT consecutive lanes share a droplet: lane q of the group adds the items q, q + RED_SPLIT, ... of both
+// sides, and the groups' sums are combined by a fixed butterfly, so the order depends on K and nbk only.
+constexpr int RED_SPLIT = 4;
+
+template <bool FORCE, int JW, bool PLANAR>
+__global__ void __launch_bounds__(256) reduce_sym_kernel(const SymBoxes t, int B, const double *__restrict__ pi,
+                                                         const double *__restrict__ pj, const double *__restrict__ r,
+                                                         double coeff, double *__restrict__ ox,
+                                                         double *__restrict__ oy, double *__restrict__ oz,
+                                                         uint32_t *err, const int32_t *__restrict__ perm) {
     const size_t plane = (size_t)B;
-    // d: position in the packed layout; with perm (one box in Morton order) its droplet is perm[d]
-    for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < t.n_total; d += gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31, q = lane % RED_SPLIT;
+    const int stride = gridDim.x * (blockDim.x / RED_SPLIT);
+    // whole warps walk the droplets together (the butterfly below needs every lane)
+    for (int d0 = (blockIdx.x * blockDim.x + threadIdx.x - lane) / RED_SPLIT; d0 < t.n_total; d0 += stride) {
+        // d: position in the packed layout; with perm (one box in Morton order) its droplet is perm[d]
+        const int d = d0 + lane / RED_SPLIT;
+        const bool live = d < t.n_total;
+        double sx = 0.0, sy = 0.0, sz = 0.0;
         int o0 = 0, nbk = t.npad1 / B, ib = 0;
         const unsigned long long *sc = t.scales1;
-        if (t.nbox > 1) {
-            const int b = box_index(t.off, t.nbox, d);
-            o0 = t.off[b];
-            nbk = (t.poff[b + 1] - t.poff[b]) / B;
-            ib = t.ioff[b];
-            sc = t.scales + 2 * b;
-        }
-        const int l = d - o0;
-        const int K = l / B, lb = l - K * B;
-        double sx = 0.0, sy = 0.0, sz = 0.0;
-        // i side: items (K, K), (K, K+1), ... are consecutive; the loads of
-        // several items are issued before their (ordered) additions
-        {
-            const double *P = pi + (size_t)(ib + rows_before(K, nbk)) * 3 * plane + lb;
-            const size_t step = 3 * plane;
+        if (live) {
+            if (t.nbox > 1) {
+                const int b = box_index(t.off, t.nbox, d);
+                o0 = t.off[b];
+                nbk = (t.poff[b + 1] - t.poff[b]) / B;
+                ib = t.ioff[b];
+                sc = t.scales + 2 * b;
+            }
+            const int l = d - o0;
+            const int K = l / B, lb = l - K * B;
+            // i side: items (K, K + q), (K, K + q + RED_SPLIT), ...
+            {
+                const double *P =
+                    pi + (size_t)(ib + rows_before(K, nbk) + q) * 3 * plane + (PLANAR ? lb : 3 * lb);
+                const size_t step = RED_SPLIT * 3 * plane, cs = PLANAR ? plane : 1;
 #pragma unroll 4
-            for (int Jb = K; Jb < nbk; ++Jb, P += step) {
-                const double a = P[0], b = P[plane], c = P[2 * plane];
-                sx += a;
-                sy += b;
-                sz += c;
+                for (int Jb = K + q; Jb < nbk; Jb += RED_SPLIT, P += step) {
+                    const double a = P[0], b = P[cs], c = P[2 * cs];
+                    sx += a;
+                    sy += b;
+                    sz += c;
+                }
+            }
+            // j side: items (q, K), (q + RED_SPLIT, K), ...; item (Ib, K) = rows_before(Ib) + K - Ib; an item
+            // holds JW sets of j-side partials (one per warp of the sorted kernel), added in order
+            {
+                const size_t wstep = 3 * plane;
+                const size_t off = PLANAR ? (size_t)lb : (size_t)lb * JW * 3;
+#pragma unroll 2
+                for (int Ib = q; Ib < K; Ib += RED_SPLIT) {
+                    const long long item = ib + rows_before(Ib, nbk) + K - Ib;
+                    const double *P = pj + (size_t)item * JW * wstep + off;
+                    double a[JW], b[JW], c[JW];
+#pragma unroll
+                    for (int w = 0; w < JW; ++w) {
+                        if (PLANAR) {
+                            a[w] = P[w * wstep];
+                            b[w] = P[w * wstep + plane];
+                            c[w] = P[w * wstep + 2 * plane];
+                        } else {
+                            a[w] = P[3 * w];
+                            b[w] = P[3 * w + 1];
+                            c[w] = P[3 * w + 2];
+                        }
+                    }
+#pragma unroll
+                    for (int w = 0; w < JW; ++w) {
+                        sx += a[w];
+                        sy += b[w];
+                        sz += c[w];
+                    }
+                }
             }
         }
-        // j side: item (Ib, K) = rows_before(Ib) + K - Ib; the next row starts nbk - Ib items later
-        {
-            long long item = ib + K;  // (0, K)
-#pragma unroll 4
-            for (int Ib = 0; Ib < K; ++Ib) {
-                const double *P = pj + (size_t)item * 3 * plane + lb;
-                const double a = P[0], b = P[plane], c = P[2 * plane];
-                sx += a;
-                sy += b;
-                sz += c;
-                item += nbk - Ib - 1;
-            }
+        // (s0 + s1) + (s2 + s3) on every lane of the group: each add sees the same two operands in either order
+#pragma unroll
+        for (int o = 1; o < RED_SPLIT; o <<= 1) {
+            sx += __shfl_xor_sync(0xffffffffu, sx, o);
+            sy += __shfl_xor_sync(0xffffffffu, sy, o);
+            sz += __shfl_xor_sync(0xffffffffu, sz, o);
         }
+        if (!live || q != 0) continue;
         const double s = pow2_inv_of(sc[0]);
         const int od = perm ? perm[d] : d;
         double f;
@@ -1209,16 +1245,19 @@ size_t sym_workspace_bytes(long long npad_total, long long items_total, int B) {
 // Workspace bytes of the symmetric schedule for one box of n droplets: the
 // packed layout and partial sums, plus the Morton order and the per-block
 // bounds of the sorted kernel.
-size_t sym_sorted_extra_bytes(long long n_total, long long npad_total, int B) {
+size_t sym_sorted_extra_bytes(long long n_total, long long npad_total, long long items_total, int B) {
     const long long nb = npad_total / B;
-    return align256(morton_ws_bytes(n_total > 0 ? (int)n_total : 1)) + align256((size_t)nb * 2 * sizeof(float4)) +
+    // (SYM_T / 32 - 1) more j-side planes per item than the plain kernel's, then the order, bounds and bitmaps
+    return (size_t)((SYM_T / 32 - 1) * items_total * 3 * (long long)B) * sizeof(double) +
+           align256(morton_ws_bytes(n_total > 0 ? (int)n_total : 1)) + align256((size_t)nb * 2 * sizeof(float4)) +
            (size_t)nb * 3 * AMB_WORDS * sizeof(uint32_t);
 }
 
 size_t sym_partial_bytes(int n, int ipt) {
     const long long B = (long long)SYM_T * ipt;
     const long long nb = (n + B - 1) / B;
-    return sym_workspace_bytes(nb * B, nb * (nb + 1) / 2, (int)B) + sym_sorted_extra_bytes(n, nb * B, (int)B);
+    return sym_workspace_bytes(nb * B, nb * (nb + 1) / 2, (int)B) +
+           sym_sorted_extra_bytes(n, nb * B, nb * (nb + 1) / 2, (int)B);
 }
 
 // 30-bit Morton key of each droplet's cell in its box's cube [0, L_b)^3 (1024
@@ -1295,8 +1334,9 @@ static int run_sym_sorted(dem_ctx *ctx, const SymBoxes &t, int ipt, int ctas, bo
     float4 *q0 = p1 + np;
     float2 *k2q1 = reinterpret_cast<float2 *>(q0 + np);
     double *pi = reinterpret_cast<double *>(base + align256(np * 64));
-    double *pj = pi + (size_t)t.items_total * 3 * B;
-    char *extra = base + sym_workspace_bytes(t.npad_total, t.items_total, B);
+    double *pj = pi + (size_t)t.items_total * 3 * B;  // [items][SYM_T / 32][3][B]
+    char *extra = base + sym_workspace_bytes(t.npad_total, t.items_total, B) +
+                  (size_t)((SYM_T / 32 - 1) * (long long)t.items_total * 3 * B) * sizeof(double);
     const MortonWs mw = morton_ws_carve(extra, n);
     float4 *bounds = reinterpret_cast<float4 *>(extra + align256(morton_ws_bytes(n)));
     uint32_t *occ = reinterpret_cast<uint32_t *>(extra + align256(morton_ws_bytes(n)) +
@@ -1354,8 +1394,9 @@ static int run_sym_sorted(dem_ctx *ctx, const SymBoxes &t, int ipt, int ctas, bo
     if (rc) return rc;
     rc = dem_check_launch(ctx, FORCE ? "mixed force (symmetric, Morton order)" : "mixed convection (symmetric, Morton order)");
     if (rc) return rc;
-    const int rgrid = max(1, min(ceil_div(n, 256), 4 * ctx->sm_count));
-    reduce_sym_kernel<FORCE><<<rgrid, 256, 0, counted(s)>>>(t, B, pi, pj, m.r, coeff, ox, oy, oz, m.err, perm);
+    const int rgrid = max(1, min(ceil_div(n, 256 / RED_SPLIT), 8 * ctx->sm_count));
+    reduce_sym_kernel<FORCE, SYM_T / 32, false><<<rgrid, 256, 0, counted(s)>>>(t, B, pi, pj, m.r, coeff, ox, oy, oz,
+                                                                               m.err, perm);
     return dem_check_launch(ctx, "mixed reduce (symmetric, Morton order)");
 }
 
@@ -1394,9 +1435,9 @@ static int run_sym_plain(dem_ctx *ctx, const SymBoxes &t, int ipt, int ctas, boo
     dem_prof_end(ctx, s);
     int rc = dem_check_launch(ctx, FORCE ? "mixed force (symmetric)" : "mixed convection (symmetric)");
     if (rc) return rc;
-    const int rgrid = max(1, min(ceil_div(t.n_total, 256), 4 * ctx->sm_count));
-    reduce_sym_kernel<FORCE><<<rgrid, 256, 0, counted(s)>>>(t, B, a.pi, a.pj, m.r, coeff, ox, oy, oz, m.err,
-                                                            nullptr);
+    const int rgrid = max(1, min(ceil_div(t.n_total, 256 / RED_SPLIT), 8 * ctx->sm_count));
+    reduce_sym_kernel<FORCE, 1, true><<<rgrid, 256, 0, counted(s)>>>(t, B, a.pi, a.pj, m.r, coeff, ox, oy, oz, m.err,
+                                                                     nullptr);
     return dem_check_launch(ctx, "mixed reduce (symmetric)");
 }
 

@@ -44,7 +44,7 @@ __host__ __device__ __forceinline__ int box_index(const int *a, int nbox, int q)
 size_t sym_workspace_bytes(long long npad_total, long long items_total, int B);
 // Bytes that follow it for the passes on droplets in Morton order (the order,
 // per-block bounds and occupancy bitmaps).
-size_t sym_sorted_extra_bytes(long long n_total, long long npad_total, int B);
+size_t sym_sorted_extra_bytes(long long n_total, long long npad_total, long long items_total, int B);
 
 // One symmetric pass over the boxes of `t`.  The scale slots (max r; max |F|
 // for convection) must already hold this call's values.  `m` carries the FP64
