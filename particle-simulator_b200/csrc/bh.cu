@@ -56,11 +56,17 @@ constexpr int RS_T = 256, RS_ITEMS = 8, RS_TILE = RS_T * RS_ITEMS;
 constexpr int BH_T = 128;     // threads per walk CTA (4 warps)
 constexpr int BH_STACK = 96;  // stack entries per warp (depth <= 10, <= 8 children per node)
 constexpr int BH_MAX_LEVEL = 10;
+// meta.w = level | flags: the walks pass over a flagged node without a term (empty, or the reference's
+// skip tests: R^3 sum < 1e-30 m^3, flat_tree.py:861; |F sum|^2 < 1e-60 N^2, flat_tree.py:1155)
+constexpr int BH_LEVEL_MASK = 0xff;
+constexpr int BH_SKIP_FORCE = 0x100;
+constexpr int BH_SKIP_VEL = 0x200;
 
 struct BhNodes {
     int *start, *count, *first_child, *nchild, *level;
     double *cx, *cy, *cz;  // R^3-weighted centre
     float4 *cs;            // walk copy: centre relative to the root cube origin / ell, and side / ell
+    int4 *meta;            // walk copy: count, nchild, first child (a leaf: first droplet), level | skip flags
     // walk records, one 16-byte-aligned group per node so that a visit issues vector loads:
     float4 *qr;  // [M][2] second moment Q = sum r^3 (x - c)(x - c)^T and R^3 sum:
                  //        (Qxx, Qxy, Qxz, Qyy), (Qyz, Qzz, R^3, 0)
@@ -673,12 +679,6 @@ __global__ void __launch_bounds__(BH_T, FORCE ? 6 : (CORR ? 5 : 7)) bh_walk_kern
     const int n = w.n, cap = w.cap;
     const double inv_ell = pow2_inv_of(w.scales[0]);
     const double fsc = FORCE ? 1.0 : pow2_inv_of(w.scales[1]);
-    // the reference's skip thresholds in the walk's units; ell and 2^-q are powers of two, so
-    // scaling the threshold instead of each node's sum gives the same decisions, without divisions
-    const double r3_skip = 1e-30 * (inv_ell * inv_ell * inv_ell), f2_skip = 1e-60 * (fsc * fsc);
-    // A force sum with a component above f_hi has |F|^2 > f2_skip in any rounding (the FP64 sum
-    // of squares is >= the largest square), so only sums below it take the FP64 test.
-    const float f_hi = nextafterf(__double2float_ru(sqrt(f2_skip)), INFINITY);
     CorrF32 cf = w.corr;
     if (CORR) cf.A = (float)(w.corr_A / inv_ell);  // separations are in units of ell
     const float Ls = (float)(w.L * inv_ell), invLs = (float)(1.0 / (w.L * inv_ell));
@@ -710,25 +710,22 @@ __global__ void __launch_bounds__(BH_T, FORCE ? 6 : (CORR ? 5 : 7)) bh_walk_kern
             }
             const int node = stack[wp][--sp];
             __syncwarp();
-            const int cnt = w.nd.count[node];
-            if (cnt == 0) continue;
+            // every record of the node in one round of loads: the walk is bound by their latency
+            const int4 mt = w.nd.meta[node];  // count, nchild, first child / droplet, level
+            const float4 cs = w.nd.cs[node];
+            const float4 rec = FORCE ? w.nd.qr[2 * (size_t)node + 1] : w.nd.fd[3 * (size_t)node];
+            const float4 rq = FORCE ? w.nd.qr[2 * (size_t)node] : w.nd.fd[3 * (size_t)node + 1];
+            const float4 rd = FORCE ? make_float4(0.f, 0.f, 0.f, 0.f) : w.nd.fd[3 * (size_t)node + 2];
+            const int cnt = mt.x;
+            if (mt.w & (FORCE ? BH_SKIP_FORCE : BH_SKIP_VEL)) continue;  // empty, or :861 / :1155
             float fnx = 0.f, fny = 0.f, fnz = 0.f, r3n = 0.f;
-            float4 rec = make_float4(0.f, 0.f, 0.f, 0.f);  // qr[1] (force) or fd[0] (velocity)
             if (FORCE) {
-                rec = w.nd.qr[2 * (size_t)node + 1];
                 r3n = rec.z;
-                if ((double)r3n < r3_skip) continue;  // :861, R^3 sum < 1e-30 m^3
             } else {
-                rec = w.nd.fd[3 * (size_t)node];
                 fnx = rec.x;
                 fny = rec.y;
                 fnz = rec.z;
-                if (!(fmaxf(fabsf(fnx), fmaxf(fabsf(fny), fabsf(fnz))) > f_hi)) {
-                    const double fx = fnx, fy = fny, fz = fnz;  // force sums in units of 2^q newtons
-                    if (fx * fx + fy * fy + fz * fz < f2_skip) continue;  // :1155, |F sum|^2 < 1e-60 N^2
-                }
             }
-            const float4 cs = w.nd.cs[node];
             float dx = cs.x - xs, dy = cs.y - ys, dz = cs.z - zs;
             if (PER) {  // minimum image
                 dx = fmaf(-Ls, rintf(dx * invLs), dx);
@@ -738,7 +735,7 @@ __global__ void __launch_bounds__(BH_T, FORCE ? 6 : (CORR ? 5 : 7)) bh_walk_kern
             const float D2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
             const float side = cs.w;
             bool accept = side * side < w.theta2 * D2 && D2 > 0.f;
-            if (PER && w.window_level > 0 && w.nd.level[node] < w.window_level) {
+            if (PER && w.window_level > 0 && (mt.w & BH_LEVEL_MASK) < w.window_level) {
                 // cells larger than L / 2^window_level: the whole cell inside the target's
                 // minimum-image window (else its droplets take different images)
                 const float hw = (float)(w.halfL * inv_ell) - side;
@@ -755,14 +752,14 @@ __global__ void __launch_bounds__(BH_T, FORCE ? 6 : (CORR ? 5 : 7)) bh_walk_kern
                         ax = fmaf(b * ang, dx, ax);
                         ay = fmaf(b * ang, dy, ay);
                         az = fmaf(b * fmaf(2.f * dz, dz, -3.f * fmaf(dx, dx, dy * dy)), dz, az);
-                        quad_force(dx, dy, dz, w.nd.qr[2 * (size_t)node], rec, rinv, rinv2, ax, ay, az);
+                        quad_force(dx, dy, dz, rq, rec, rinv, rinv2, ax, ay, az);
                     } else {  // e = x_i - c = -D
                         const float ex = -dx, ey = -dy, ez = -dz;
                         const float dot = fmaf(ex, fnx, fmaf(ey, fny, ez * fnz));
                         ax = fmaf(rinv, fmaf(ex, dot * rinv2, fnx), ax);
                         ay = fmaf(rinv, fmaf(ey, dot * rinv2, fny), ay);
                         az = fmaf(rinv, fmaf(ez, dot * rinv2, fnz), az);
-                        const float4 d1 = w.nd.fd[3 * (size_t)node + 1], d2 = w.nd.fd[3 * (size_t)node + 2];
+                        const float4 d1 = rq, d2 = rd;
                         const float Dm[9] = {rec.w, d1.x, d1.y, d1.z, d1.w, d2.x, d2.y, d2.z, d2.w};  // D_ab
                         const float Ux = Dm[0] * ex + Dm[3] * ey + Dm[6] * ez;  // D^T e
                         const float Uy = Dm[1] * ex + Dm[4] * ey + Dm[7] * ez;
@@ -781,9 +778,9 @@ __global__ void __launch_bounds__(BH_T, FORCE ? 6 : (CORR ? 5 : 7)) bh_walk_kern
                 }
                 continue;
             }
-            const int nch = w.nd.nchild[node];
+            const int nch = mt.y;
             if (nch == 0) {  // leaf: exact pair terms (contact cut r^2 >= (r_i + r_j)^2)
-                const int s0 = w.nd.start[node];
+                const int s0 = mt.z;
                 if (valid) pairs += cnt;
                 // d = x_j - x_i = (x_j - c_leaf) + MIC(c_leaf - x_i): the first part stored per droplet in
                 // FP32, the second taken in FP64 once per leaf, so d carries ~1e-7 of |d|, not of |x|
@@ -828,7 +825,7 @@ __global__ void __launch_bounds__(BH_T, FORCE ? 6 : (CORR ? 5 : 7)) bh_walk_kern
                 broken = true;
                 break;
             }
-            if (lane < nch) stack[wp][sp + lane] = w.nd.first_child[node] + lane;
+            if (lane < nch) stack[wp][sp + lane] = mt.z + lane;
             sp += nch;
             __syncwarp();
         }
@@ -926,6 +923,7 @@ __global__ void scale_nodes_kernel(BhNodes nd, int nc, const unsigned long long 
     const double fsc = pow2_inv_of(scales[1]);
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nc; k += gridDim.x * blockDim.x) {
         if (what == 0) {
+            const int nch = nd.nchild[k], cnt = nd.count[k];
             nd.cs[k] = make_float4((float)((nd.cx[k] - geom[0]) * inv_ell), (float)((nd.cy[k] - geom[1]) * inv_ell),
                                    (float)((nd.cz[k] - geom[2]) * inv_ell),
                                    (float)(ldexp(geom[3], -nd.level[k]) * inv_ell));
@@ -933,10 +931,20 @@ __global__ void scale_nodes_kernel(BhNodes nd, int nc, const unsigned long long 
             float *qr = reinterpret_cast<float *>(nd.qr + 2 * (size_t)k);  // Q[0..5], R^3
             for (int q = 0; q < 6; ++q) qr[q] = (float)((double)qr[q] * s5);
             qr[6] = (float)((double)qr[6] * s3);
+            // the skip threshold in the walk's units (ell is a power of two: the same decision as in metres)
+            const bool skip = cnt == 0 || (double)qr[6] < 1e-30 * s3;
+            nd.meta[k] = make_int4(cnt, nch, nch ? nd.first_child[k] : nd.start[k],
+                                   nd.level[k] | (skip ? BH_SKIP_FORCE : 0) | (cnt == 0 ? BH_SKIP_VEL : 0));
         } else {
             float *fd = reinterpret_cast<float *>(nd.fd + 3 * (size_t)k);  // F[0..2], D[0..8]
             for (int q = 0; q < 3; ++q) fd[q] = (float)((double)fd[q] * fsc);
             for (int q = 3; q < 12; ++q) fd[q] = (float)((double)fd[q] * fsc * inv_ell);
+            const double f0 = fd[0], f1 = fd[1], f2 = fd[2];  // force sum in units of 2^q newtons
+            const double f2sum = __dadd_rn(__dadd_rn(__dmul_rn(f0, f0), __dmul_rn(f1, f1)), __dmul_rn(f2, f2));
+            int4 mt = nd.meta[k];
+            const bool skip = mt.x == 0 || f2sum < 1e-60 * (fsc * fsc);
+            mt.w = (mt.w & ~BH_SKIP_VEL) | (skip ? BH_SKIP_VEL : 0);
+            nd.meta[k] = mt;
         }
     }
 }
@@ -1024,7 +1032,7 @@ static int bh_alloc(dem_ctx *ctx, T **p, size_t count, const char *what) {
 
 static void bh_free_nodes(BhNodes &nd) {
     void *ptrs[] = {nd.start, nd.count, nd.first_child, nd.nchild, nd.level, nd.cx,
-                    nd.cy,    nd.cz,    nd.cs,          nd.qr,     nd.fd};
+                    nd.cy,    nd.cz,    nd.cs,          nd.meta,   nd.qr, nd.fd};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     nd = BhNodes{};
@@ -1040,7 +1048,7 @@ static int bh_nodes_reserve(dem_bh *b, int m, int keep, cudaStream_t s) {
         (rc = bh_alloc(ctx, &nn.first_child, m, "bh nodes")) || (rc = bh_alloc(ctx, &nn.nchild, m, "bh nodes")) ||
         (rc = bh_alloc(ctx, &nn.level, m, "bh nodes")) || (rc = bh_alloc(ctx, &nn.cx, m, "bh nodes")) ||
         (rc = bh_alloc(ctx, &nn.cy, m, "bh nodes")) || (rc = bh_alloc(ctx, &nn.cz, m, "bh nodes")) ||
-        (rc = bh_alloc(ctx, &nn.cs, m, "bh nodes")) ||
+        (rc = bh_alloc(ctx, &nn.cs, m, "bh nodes")) || (rc = bh_alloc(ctx, &nn.meta, m, "bh nodes")) ||
         (rc = bh_alloc(ctx, &nn.qr, 2 * (size_t)m, "bh nodes")) ||
         (rc = bh_alloc(ctx, &nn.fd, 3 * (size_t)m, "bh nodes"))) {
         bh_free_nodes(nn);

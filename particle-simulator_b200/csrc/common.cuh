@@ -56,6 +56,7 @@ struct dem_ctx {
     int32_t *bucket_cursor = nullptr; // table
     int32_t *sorted_idx = nullptr;    // particles grouped by bucket
     double2 *hash_pos = nullptr;      // (x, y), (z, r) of the particles in bucket order (2 per particle)
+    float4 *hash_pos32 = nullptr;     // (x, y, z, r) rounded to FP32, bucket order (the far test)
     int32_t *pair_count = nullptr;    // per particle (capacity + 1)
     int64_t *pair_offset = nullptr;   // per particle (capacity + 1), exclusive scan
     int64_t table_capacity = 0;

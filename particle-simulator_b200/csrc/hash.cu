@@ -136,11 +136,20 @@ __device__ __forceinline__ bool contact_rn(double d2, double s) {
 // neighbour cells) and calls f(j, multiplicity) for those in contact.
 // PACKED: the droplets' (x, y), (z, r) in bucket order are in P (two double2
 // per bucket slot, slot ti holding droplet i), so a bucket's candidates are
-// read as contiguous 32-byte records instead of four scattered gathers.
+// read as contiguous 32-byte records instead of four scattered gathers, and
+// their FP32 roundings in P32 reject the clearly separated candidates first.
+// That test only drops a candidate whose FP32 distance exceeds the contact
+// distance by far more than FP32 rounding can account for (a margin of
+// 2^-17 (max |x_i| + L) plus 2^-18 of the radii sum; the per-axis distance is
+// bounded below by the smaller of |d| and ||d| - L|, which covers either image
+// the FP64 test may take); NaNs and overflowed bounds fail the comparison and
+// go to the FP64 test, and a margin below 2^-100 turns the far test off.  So
+// every pair the FP64 test accepts is still found.
 template <bool PACKED, typename F>
 __device__ __forceinline__ void for_each_contact(int i, int ti, const double *__restrict__ x,
                                                  const double *__restrict__ y, const double *__restrict__ z,
                                                  const double *__restrict__ r, const double2 *__restrict__ P,
+                                                 const float4 *__restrict__ P32,
                                                  const HashParams &p, int periodic, double L, double halfL,
                                                  int32_t mask, int n, const int32_t *__restrict__ bstart,
                                                  const int32_t *__restrict__ sorted_idx, F &&f) {
@@ -160,6 +169,15 @@ __device__ __forceinline__ void for_each_contact(int i, int ti, const double *__
     const int32_t cx = cell_coord(xi, p.cell, p.grid, periodic);
     const int32_t cy = cell_coord(yi, p.cell, p.grid, periodic);
     const int32_t cz = cell_coord(zi, p.cell, p.grid, periodic);
+    float4 qi = make_float4(0.f, 0.f, 0.f, 0.f);
+    float Lf = 0.f, marg = 0.f;
+    if (PACKED) {
+        qi = P32[ti];
+        Lf = (float)L;
+        marg = (float)(0x1p-17 * (fmax(fabs(xi), fmax(fabs(yi), fabs(zi))) + fabs(L)));
+        qi.w = qi.w * (1.f + 0x1p-18f) + marg;  // r_i, widened: the far test adds r_j (1 + 2^-18)
+        if (!(marg >= 0x1p-100f)) qi.w = INFINITY;  // coordinates near FP32's subnormal range: no far test
+    }
     auto bucket = [&](const double xj, const double yj, const double zj, const double rj, int32_t j, int m) {
         double dx = xj - xi, dy = yj - yi, dz = zj - zi;
         if (periodic) {
@@ -173,6 +191,15 @@ __device__ __forceinline__ void for_each_contact(int i, int ti, const double *__
         const int32_t j = sorted_idx[s];
         if (!(i < j)) return;
         if (PACKED) {
+            const float4 q = P32[s];
+            float ax = fabsf(q.x - qi.x), ay = fabsf(q.y - qi.y), az = fabsf(q.z - qi.z);
+            if (periodic) {
+                ax = fminf(ax, fabsf(ax - Lf));
+                ay = fminf(ay, fabsf(ay - Lf));
+                az = fminf(az, fabsf(az - Lf));
+            }
+            const float sf = fmaf(q.w, 1.f + 0x1p-18f, qi.w);
+            if (fmaf(ax, ax, fmaf(ay, ay, az * az)) > sf * sf) return;  // clearly apart
             const double2 a = P[2 * s], b = P[2 * s + 1];
             bucket(a.x, a.y, b.x, b.y, j, m);
         } else {
@@ -252,19 +279,22 @@ __device__ __forceinline__ void for_each_contact(int i, int ti, const double *__
 __global__ void bucket_positions_kernel(int n, const double *__restrict__ x, const double *__restrict__ y,
                                         const double *__restrict__ z, const double *__restrict__ r,
                                         const HashParams *__restrict__ hp, const int32_t *__restrict__ sorted_idx,
-                                        double2 *__restrict__ P) {
+                                        double2 *__restrict__ P, float4 *__restrict__ P32) {
     if (!hp->valid) return;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
         const int j = sorted_idx[s];
-        P[2 * s] = make_double2(x[j], y[j]);
-        P[2 * s + 1] = make_double2(z[j], r[j]);
+        const double xj = x[j], yj = y[j], zj = z[j], rj = r[j];
+        P[2 * s] = make_double2(xj, yj);
+        P[2 * s + 1] = make_double2(zj, rj);
+        P32[s] = make_float4((float)xj, (float)yj, (float)zj, (float)rj);
     }
 }
 
 template <bool PACKED>
 __global__ void count_pairs_kernel(int n, const double *__restrict__ x, const double *__restrict__ y,
                                    const double *__restrict__ z, const double *__restrict__ r,
-                                   const double2 *__restrict__ P, const HashParams *__restrict__ hp, int periodic,
+                                   const double2 *__restrict__ P, const float4 *__restrict__ P32,
+                                   const HashParams *__restrict__ hp, int periodic,
                                    double L, int32_t mask, const int32_t *__restrict__ bstart,
                                    const int32_t *__restrict__ sorted_idx, int32_t *__restrict__ pair_count,
                                    unsigned long long *__restrict__ raw) {
@@ -274,8 +304,8 @@ __global__ void count_pairs_kernel(int n, const double *__restrict__ x, const do
         const int i = p.valid ? sorted_idx[t] : t;  // bucket order (the buckets are filled when valid)
         int32_t c = 0;
         if (p.valid) {
-            for_each_contact<PACKED>(i, t, x, y, z, r, P, p, periodic, L, 0.5 * L, mask, n, bstart, sorted_idx,
-                                     [&](int32_t, int m) {
+            for_each_contact<PACKED>(i, t, x, y, z, r, P, P32, p, periodic, L, 0.5 * L, mask, n, bstart,
+                                     sorted_idx, [&](int32_t, int m) {
                                          ++c;
                                          local_raw += (unsigned long long)m;
                                      });
@@ -288,8 +318,8 @@ __global__ void count_pairs_kernel(int n, const double *__restrict__ x, const do
 template <bool PACKED>
 __global__ void write_pairs_kernel(int n, const double *__restrict__ x, const double *__restrict__ y,
                                    const double *__restrict__ z, const double *__restrict__ r,
-                                   const double2 *__restrict__ P, const HashParams *__restrict__ hp, int periodic,
-                                   double L, int32_t mask,
+                                   const double2 *__restrict__ P, const float4 *__restrict__ P32,
+                                   const HashParams *__restrict__ hp, int periodic, double L, int32_t mask,
                                    const int32_t *__restrict__ bstart, const int32_t *__restrict__ sorted_idx,
                                    const int64_t *__restrict__ offset, int32_t *__restrict__ pairs, int64_t cap,
                                    int64_t *__restrict__ counts, uint32_t *err) {
@@ -310,7 +340,7 @@ __global__ void write_pairs_kernel(int n, const double *__restrict__ x, const do
         // pairs[o0 .. o0 + len); once the run holds m entries the largest drops out, so a cut row
         // keeps its m smallest j and the buffer holds the lexicographically first cap pairs
         int64_t len = 0;
-        for_each_contact<PACKED>(i, t, x, y, z, r, P, p, periodic, L, 0.5 * L, mask, n, bstart, sorted_idx,
+        for_each_contact<PACKED>(i, t, x, y, z, r, P, P32, p, periodic, L, 0.5 * L, mask, n, bstart, sorted_idx,
                                  [&](int32_t j, int) {
             int64_t q;
             if (len < m) {
@@ -369,16 +399,19 @@ int launch_hash_detect(dem_ctx *ctx, int n, const double *x, const double *y, co
                         "cursor copy");
     if (rc) return rc;
     scatter_kernel<<<grid, 256, 0, counted(s)>>>(n, ctx->cell_hash, hp, ctx->bucket_cursor, ctx->sorted_idx);
-    bucket_positions_kernel<<<grid, 256, 0, counted(s)>>>(n, x, y, z, r, hp, ctx->sorted_idx, ctx->hash_pos);
+    bucket_positions_kernel<<<grid, 256, 0, counted(s)>>>(n, x, y, z, r, hp, ctx->sorted_idx, ctx->hash_pos,
+                                                          ctx->hash_pos32);
     const int dgrid = ceil_div(n, 128);
-    count_pairs_kernel<true><<<dgrid, 128, 0, counted(s)>>>(n, x, y, z, r, ctx->hash_pos, hp, periodic, L, mask,
+    count_pairs_kernel<true><<<dgrid, 128, 0, counted(s)>>>(n, x, y, z, r, ctx->hash_pos, ctx->hash_pos32, hp,
+                                                            periodic, L, mask,
                                                             ctx->bucket_start, ctx->sorted_idx, ctx->pair_count,
                                                             reinterpret_cast<unsigned long long *>(counts + 1));
     rc = dem_check_launch(ctx, "hash count");
     if (rc) return rc;
     rc = exclusive_scan<int32_t, int64_t>(ctx, ctx->pair_count, ctx->pair_offset, n, s);
     if (rc) return rc;
-    write_pairs_kernel<true><<<dgrid, 128, 0, counted(s)>>>(n, x, y, z, r, ctx->hash_pos, hp, periodic, L, mask,
+    write_pairs_kernel<true><<<dgrid, 128, 0, counted(s)>>>(n, x, y, z, r, ctx->hash_pos, ctx->hash_pos32, hp,
+                                                            periodic, L, mask,
                                                             ctx->bucket_start, ctx->sorted_idx, ctx->pair_offset,
                                                             pairs, cap, counts, ctx->d_err);
     dem_prof_end(ctx, s);
@@ -496,14 +529,14 @@ extern "C" int dem_hash_detect_noalloc(int n, const double *x, const double *y, 
         return DEM_E_CUDA;
     scatter_kernel<<<grid, 256, 0, counted(s)>>>(n, cell_hash, hp, bucket_cursor, sorted_idx);
     const int dgrid = ceil_div(n, 128);
-    count_pairs_kernel<false><<<dgrid, 128, 0, counted(s)>>>(n, x, y, z, r, nullptr, hp, periodic, L, mask,
+    count_pairs_kernel<false><<<dgrid, 128, 0, counted(s)>>>(n, x, y, z, r, nullptr, nullptr, hp, periodic, L, mask,
                                                              bucket_start, sorted_idx, pair_count,
                                                              reinterpret_cast<unsigned long long *>(counts + 1));
     if (cudaGetLastError() != cudaSuccess) return DEM_E_CUDA;
     if (exclusive_scan_into<int32_t, int64_t>(pair_count, pair_offset, n, static_cast<int64_t *>(sums), s) !=
         cudaSuccess)
         return DEM_E_CUDA;
-    write_pairs_kernel<false><<<dgrid, 128, 0, counted(s)>>>(n, x, y, z, r, nullptr, hp, periodic, L, mask,
+    write_pairs_kernel<false><<<dgrid, 128, 0, counted(s)>>>(n, x, y, z, r, nullptr, nullptr, hp, periodic, L, mask,
                                                              bucket_start, sorted_idx, pair_offset, pairs,
                                                              pair_capacity, counts, err);
     return cudaGetLastError() == cudaSuccess ? DEM_OK : DEM_E_CUDA;
