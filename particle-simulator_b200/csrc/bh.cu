@@ -20,10 +20,13 @@
 //           R^3-weighted second moment Q of the node about that centre; after the force
 //           walk, sum F and the dipole D = sum (x - c) F^T (= P - c F^T of
 //           flat_tree.py:556-777).
-//   walks   one warp per 32 consecutive sorted targets; the warp shares a
-//           shared-memory stack and opens a node when any of its lanes fails
-//           the reference's acceptance test s^2 < theta^2 D^2 (flat_tree.py:871),
-//           so every lane sees a tree cut at least as fine as its own; in a
+//   walks   one warp per 64 consecutive sorted targets, two per lane, their
+//           terms evaluated in packed FP32x2 (bh_walk2_kernel; with the
+//           periodic-image correction, one target per lane: bh_walk_kernel); the
+//           warp shares a shared-memory stack and opens a node when any of its
+//           targets fails the reference's acceptance test s^2 < theta^2 D^2
+//           (flat_tree.py:871), so every target sees a tree cut at least as fine
+//           as its own; in a
 //           periodic box a node of level < window_level is also opened
 //           unless its whole cell lies in the target's minimum-image window
 //           (|D_axis| + s < L/2), where all its droplets take the image of its
@@ -55,6 +58,14 @@ namespace dem {
 constexpr int RS_T = 256, RS_ITEMS = 8, RS_TILE = RS_T * RS_ITEMS;
 constexpr int BH_T = 128;     // threads per walk CTA (4 warps)
 constexpr int BH_STACK = 96;  // stack entries per warp (depth <= 10, <= 8 children per node)
+// resident CTAs per SM the two-target walks are compiled for (5: 94-96 registers, none spilled; 0.4 %
+// faster at N = 2^20 than 4 CTAs with 107-108 registers)
+#ifndef BH_WALK2_CTAS_FORCE
+#define BH_WALK2_CTAS_FORCE 5
+#endif
+#ifndef BH_WALK2_CTAS_VEL
+#define BH_WALK2_CTAS_VEL 5
+#endif
 constexpr int BH_MAX_LEVEL = 10;
 // meta.w = level | flags: the walks pass over a flagged node without a term (empty, or the reference's
 // skip tests: R^3 sum < 1e-30 m^3, flat_tree.py:861; |F sum|^2 < 1e-60 N^2, flat_tree.py:1155)
@@ -880,6 +891,284 @@ __global__ void __launch_bounds__(BH_T, FORCE ? 6 : (CORR ? 5 : 7)) bh_walk_kern
     }
 }
 
+// ---------------------------------------------------------------------------
+// Two targets per lane: a warp walks 64 consecutive sorted targets (lane l holds
+// targets base + l and base + 32 + l) and evaluates each accepted node and leaf
+// pair for both at once in packed FP32x2 arithmetic.  The tree cut is the one
+// the 64 targets need together (a node is opened when any target fails the
+// acceptance test), and the per-node work -- pop, loads, tests, vote -- is
+// shared by twice the targets.  Terms are the same expressions as
+// bh_walk_kernel's, evaluated per lane of a float2.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 p_rsqrt(float2 v) { return make_float2(rsqrtf(v.x), rsqrtf(v.y)); }
+
+template <bool PER>
+__device__ __forceinline__ float2 p_mic(float2 d, float2 invL, float2 nL) {
+    if (!PER) return d;
+    const float2 u = p_add(p_fma(d, invL, dup2(RINT_MAGIC)), dup2(-RINT_MAGIC));  // rint(d / L)
+    return p_fma(nL, u, d);
+}
+
+// quad_force for two targets: x, y, z = D = c - x_i per lane, r7 = |D|^-7, rinv2 = |D|^-2.
+__device__ __forceinline__ void quad_force2(float2 x, float2 y, float2 z, const float4 qa, const float4 qb, float2 r7,
+                                            float2 rinv2, float2 &gx, float2 &gy, float2 &gz) {
+    const float2 r9 = p_mul(r7, rinv2), r11 = p_mul(r9, rinv2);
+    const float2 qxx = dup2(qa.x), qxy = dup2(qa.y), qxz = dup2(qa.z), qyy = dup2(qa.w), qyz = dup2(qb.x),
+                 qzz = dup2(qb.y);
+    const float2 tr = dup2(qa.x + qa.w + qb.y);
+    const float2 Qx = p_fma(qxx, x, p_fma(qxy, y, p_mul(qxz, z)));
+    const float2 Qy = p_fma(qxy, x, p_fma(qyy, y, p_mul(qyz, z)));
+    const float2 Qz = p_fma(qxz, x, p_fma(qyz, y, p_mul(qzz, z)));
+    const float2 xQx = p_fma(x, Qx, p_fma(y, Qy, p_mul(z, Qz)));
+    // from |d|^-3: 15 [(tr x + 2 Q x) r^-7 - 7 (x.Qx) x r^-9]
+    const float2 a1 = p_mul(dup2(15.f), r7), a2 = p_mul(p_mul(dup2(-105.f), xQx), r9);
+    // from dz^2 |d|^-5 (times -3 below)
+    const float2 zz = p_mul(z, z), zr7 = p_mul(z, r7);
+    const float2 b1 = p_mul(p_mul(dup2(35.f), zz), r9);
+    const float2 b2 = p_fma(dup2(-10.f * qb.y), r7,
+                            p_fma(p_mul(dup2(140.f), p_mul(z, Qz)), r9, p_mul(p_mul(dup2(-315.f), p_mul(zz, xQx)), r11)));
+    const float2 tx = p_fma(dup2(2.f), Qx, p_mul(tr, x)), ty = p_fma(dup2(2.f), Qy, p_mul(tr, y)),
+                 tz = p_fma(dup2(2.f), Qz, p_mul(tr, z));
+    const float2 Bx = p_fma(b1, tx, p_fma(b2, x, p_mul(dup2(-20.f * qa.z), zr7)));
+    const float2 By = p_fma(b1, ty, p_fma(b2, y, p_mul(dup2(-20.f * qb.x), zr7)));
+    const float2 Bz = p_fma(
+        b1, tz,
+        p_fma(b2, z,
+              p_fma(dup2(-20.f * qb.y), zr7,
+                    p_fma(dup2(-20.f), p_mul(Qz, r7),
+                          p_mul(p_mul(dup2(-10.f), z), p_fma(tr, r7, p_mul(dup2(-7.f), p_mul(xQx, r9))))))));
+    gx = p_fma(dup2(1.f / 6.f), p_fma(a1, tx, p_fma(a2, x, p_mul(dup2(-3.f), Bx))), gx);
+    gy = p_fma(dup2(1.f / 6.f), p_fma(a1, ty, p_fma(a2, y, p_mul(dup2(-3.f), By))), gy);
+    gz = p_fma(dup2(1.f / 6.f), p_fma(a1, tz, p_fma(a2, z, p_mul(dup2(-3.f), Bz))), gz);
+}
+
+// The pair force r_j^3 P(d) / |d|^7 (b = r_j^3 |d|^-7, per lane) added to (ax, ay, az).
+__device__ __forceinline__ void mono_force2(float2 dx, float2 dy, float2 dz, float2 b, float2 &ax, float2 &ay,
+                                            float2 &az) {
+    const float2 zz = p_mul(dz, dz), xy2 = p_fma(dx, dx, p_mul(dy, dy));
+    const float2 ang = p_fma(dup2(-1.f), xy2, p_mul(dup2(4.f), zz));   // 4 dz^2 - dx^2 - dy^2
+    const float2 angz = p_fma(dup2(-3.f), xy2, p_mul(dup2(2.f), zz));  // 2 dz^2 - 3 dx^2 - 3 dy^2
+    const float2 ba = p_mul(b, ang);
+    ax = p_fma(ba, dx, ax);
+    ay = p_fma(ba, dy, ay);
+    az = p_fma(p_mul(b, angz), dz, az);
+}
+
+// The Stokeslet G(e) F / 8 pi eta without constants: (F + e (e.F) / |e|^2) / |e|, added to (ax, ay, az).
+__device__ __forceinline__ void stokeslet2(float2 ex, float2 ey, float2 ez, float2 fx, float2 fy, float2 fz,
+                                           float2 rinv, float2 rinv2, float2 &ax, float2 &ay, float2 &az) {
+    const float2 dot = p_fma(ex, fx, p_fma(ey, fy, p_mul(ez, fz)));
+    const float2 sc = p_mul(dot, rinv2);
+    ax = p_fma(rinv, p_fma(ex, sc, fx), ax);
+    ay = p_fma(rinv, p_fma(ey, sc, fy), ay);
+    az = p_fma(rinv, p_fma(ez, sc, fz), az);
+}
+
+template <bool PER, bool FORCE>
+__global__ void __launch_bounds__(BH_T, FORCE ? BH_WALK2_CTAS_FORCE : BH_WALK2_CTAS_VEL)
+    bh_walk2_kernel(const BhWalk w, double coeff, double stokes, double *__restrict__ ox, double *__restrict__ oy,
+                    double *__restrict__ oz, double *__restrict__ fsort_out) {
+    __shared__ int stack[BH_T / 32][BH_STACK];
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    const int n = w.n, cap = w.cap;
+    const double inv_ell = pow2_inv_of(w.scales[0]);
+    const double fsc = FORCE ? 1.0 : pow2_inv_of(w.scales[1]);
+    const float Ls = (float)(w.L * inv_ell), invLs = (float)(1.0 / (w.L * inv_ell));
+    const float2 nL2 = dup2(-Ls), invL2 = dup2(invLs);
+    const float edge = (float)(w.L * inv_ell * (0.5 - 1e-6));  // leaf pairs: FP32 separations err by < 1e-6 L
+    const double gox = w.geom[0], goy = w.geom[1], goz = w.geom[2];
+    unsigned long long pairs = 0, nodes = 0;
+    const int warps = gridDim.x * (BH_T / 32);
+    for (int base = (blockIdx.x * (BH_T / 32) + wp) * 64; base < n; base += warps * 64) {
+        const int si0 = base + lane, si1 = base + 32 + lane;
+        const bool v0 = si0 < n, v1 = si1 < n;
+        const int nv = (int)v0 + (int)v1;
+        const int sl0 = v0 ? si0 : base, sl1 = v1 ? si1 : base;  // padding targets shadow a real droplet
+        const double xi0 = w.ps[sl0], yi0 = w.ps[cap + sl0], zi0 = w.ps[2 * (size_t)cap + sl0],
+                     ri0 = w.ps[3 * (size_t)cap + sl0];
+        const double xi1 = w.ps[sl1], yi1 = w.ps[cap + sl1], zi1 = w.ps[2 * (size_t)cap + sl1],
+                     ri1 = w.ps[3 * (size_t)cap + sl1];
+        // targets in the nodes' FP32 frame
+        const float2 xs = make_float2((float)((xi0 - gox) * inv_ell), (float)((xi1 - gox) * inv_ell));
+        const float2 ys = make_float2((float)((yi0 - goy) * inv_ell), (float)((yi1 - goy) * inv_ell));
+        const float2 zs = make_float2((float)((zi0 - goz) * inv_ell), (float)((zi1 - goz) * inv_ell));
+        const float2 ris = make_float2((float)(ri0 * inv_ell), (float)(ri1 * inv_ell));
+        float2 ax = make_float2(0.f, 0.f), ay = ax, az = ax;
+        int sp = 1;
+        if (lane == 0) stack[wp][0] = 0;
+        __syncwarp();
+        int iters = 0;
+        bool broken = false;
+        while (sp > 0) {
+            if (++iters > w.node_count + 1) {  // a tree is visited at most once per node
+                broken = true;
+                break;
+            }
+            const int node = stack[wp][--sp];
+            __syncwarp();
+            const int4 mt = w.nd.meta[node];  // count, nchild, first child / droplet, level | flags
+            const float4 cs = w.nd.cs[node];
+            const float4 rec = FORCE ? w.nd.qr[2 * (size_t)node + 1] : w.nd.fd[3 * (size_t)node];
+            const float4 rq = FORCE ? w.nd.qr[2 * (size_t)node] : w.nd.fd[3 * (size_t)node + 1];
+            const float4 rd = FORCE ? make_float4(0.f, 0.f, 0.f, 0.f) : w.nd.fd[3 * (size_t)node + 2];
+            const int cnt = mt.x;
+            if (mt.w & (FORCE ? BH_SKIP_FORCE : BH_SKIP_VEL)) continue;  // empty, or :861 / :1155
+            // force walk: D = c - x_i; velocity walk: e = x_i - c (= -D, the minimum image is odd)
+            float2 dx = FORCE ? p_add(dup2(cs.x), p_mul(dup2(-1.f), xs)) : p_add(xs, dup2(-cs.x));
+            float2 dy = FORCE ? p_add(dup2(cs.y), p_mul(dup2(-1.f), ys)) : p_add(ys, dup2(-cs.y));
+            float2 dz = FORCE ? p_add(dup2(cs.z), p_mul(dup2(-1.f), zs)) : p_add(zs, dup2(-cs.z));
+            dx = p_mic<PER>(dx, invL2, nL2);
+            dy = p_mic<PER>(dy, invL2, nL2);
+            dz = p_mic<PER>(dz, invL2, nL2);
+            const float2 D2 = p_fma(dx, dx, p_fma(dy, dy, p_mul(dz, dz)));
+            const float side = cs.w, s2 = side * side;
+            bool acc0 = s2 < w.theta2 * D2.x && D2.x > 0.f, acc1 = s2 < w.theta2 * D2.y && D2.y > 0.f;
+            if (PER && w.window_level > 0 && (mt.w & BH_LEVEL_MASK) < w.window_level) {
+                const float hw = (float)(w.halfL * inv_ell) - side;
+                acc0 = acc0 && fabsf(dx.x) < hw && fabsf(dy.x) < hw && fabsf(dz.x) < hw;
+                acc1 = acc1 && fabsf(dx.y) < hw && fabsf(dy.y) < hw && fabsf(dz.y) < hw;
+            }
+            if (__all_sync(0xffffffffu, (acc0 || !v0) && (acc1 || !v1))) {
+                if (nv) {
+                    nodes += nv;
+                    const float2 rinv = p_rsqrt(D2), rinv2 = p_mul(rinv, rinv);
+                    if (FORCE) {
+                        const float2 r7 = p_mul(p_mul(rinv2, rinv2), p_mul(rinv2, rinv));
+                        mono_force2(dx, dy, dz, p_mul(dup2(rec.z), r7), ax, ay, az);
+                        quad_force2(dx, dy, dz, rq, rec, r7, rinv2, ax, ay, az);
+                    } else {
+                        const float2 fnx = dup2(rec.x), fny = dup2(rec.y), fnz = dup2(rec.z);
+                        stokeslet2(dx, dy, dz, fnx, fny, fnz, rinv, rinv2, ax, ay, az);
+                        // dipole: D^T e, D e, e.D e, tr D (D_ab from the records, row a, column b)
+                        const float d00 = rec.w, d01 = rq.x, d02 = rq.y, d10 = rq.z, d11 = rq.w, d12 = rd.x,
+                                    d20 = rd.y, d21 = rd.z, d22 = rd.w;
+                        const float2 Ux = p_fma(dup2(d00), dx, p_fma(dup2(d10), dy, p_mul(dup2(d20), dz)));
+                        const float2 Uy = p_fma(dup2(d01), dx, p_fma(dup2(d11), dy, p_mul(dup2(d21), dz)));
+                        const float2 Uz = p_fma(dup2(d02), dx, p_fma(dup2(d12), dy, p_mul(dup2(d22), dz)));
+                        const float2 Wx = p_fma(dup2(d00), dx, p_fma(dup2(d01), dy, p_mul(dup2(d02), dz)));
+                        const float2 Wy = p_fma(dup2(d10), dx, p_fma(dup2(d11), dy, p_mul(dup2(d12), dz)));
+                        const float2 Wz = p_fma(dup2(d20), dx, p_fma(dup2(d21), dy, p_mul(dup2(d22), dz)));
+                        const float2 ntr = dup2(-(d00 + d11 + d22));
+                        const float2 q = p_fma(dx, Wx, p_fma(dy, Wy, p_mul(dz, Wz)));
+                        const float2 rinv3 = p_mul(rinv, rinv2), rinv5 = p_mul(rinv3, rinv2);
+                        const float2 q3 = p_mul(p_mul(dup2(3.f), q), rinv5);
+                        const float2 Vx = p_fma(ntr, dx, p_add(Ux, p_mul(dup2(-1.f), Wx)));
+                        const float2 Vy = p_fma(ntr, dy, p_add(Uy, p_mul(dup2(-1.f), Wy)));
+                        const float2 Vz = p_fma(ntr, dz, p_add(Uz, p_mul(dup2(-1.f), Wz)));
+                        ax = p_fma(rinv3, Vx, p_fma(dx, q3, ax));
+                        ay = p_fma(rinv3, Vy, p_fma(dy, q3, ay));
+                        az = p_fma(rinv3, Vz, p_fma(dz, q3, az));
+                    }
+                }
+                continue;
+            }
+            const int nch = mt.y;
+            if (nch == 0) {  // leaf: exact pair terms (contact cut r^2 >= (r_i + r_j)^2)
+                const int s0 = mt.z;
+                pairs += (unsigned long long)cnt * nv;
+                // d = x_j - x_i = (x_j - c_leaf) + MIC(c_leaf - x_i): the first part per droplet in FP32,
+                // the second in FP64 once per leaf and target
+                const double lcx = w.nd.cx[node], lcy = w.nd.cy[node], lcz = w.nd.cz[node];
+                const float2 lx = make_float2((float)(bh_mic<PER>(lcx - xi0, w.L, w.halfL) * inv_ell),
+                                              (float)(bh_mic<PER>(lcx - xi1, w.L, w.halfL) * inv_ell));
+                const float2 ly = make_float2((float)(bh_mic<PER>(lcy - yi0, w.L, w.halfL) * inv_ell),
+                                              (float)(bh_mic<PER>(lcy - yi1, w.L, w.halfL) * inv_ell));
+                const float2 lz = make_float2((float)(bh_mic<PER>(lcz - zi0, w.L, w.halfL) * inv_ell),
+                                              (float)(bh_mic<PER>(lcz - zi1, w.L, w.halfL) * inv_ell));
+                for (int k = 0; k < cnt; ++k) {
+                    const int sj = s0 + k;
+                    const float4 o = w.loff[sj];
+                    float2 dx = p_add(dup2(o.x), lx), dy = p_add(dup2(o.y), ly), dz = p_add(dup2(o.z), lz);
+                    // within 1e-6 L of the image boundary (or past it: a leaf reaching across L/2 in a
+                    // shallow tree) the image and the separation come from the FP64 positions
+                    if (PER) {
+                        if (fmaxf(fabsf(dx.x), fmaxf(fabsf(dy.x), fabsf(dz.x))) > edge) {
+                            dx.x = (float)(bh_mic<PER>(w.ps[sj] - xi0, w.L, w.halfL) * inv_ell);
+                            dy.x = (float)(bh_mic<PER>(w.ps[cap + sj] - yi0, w.L, w.halfL) * inv_ell);
+                            dz.x = (float)(bh_mic<PER>(w.ps[2 * (size_t)cap + sj] - zi0, w.L, w.halfL) * inv_ell);
+                        }
+                        if (fmaxf(fabsf(dx.y), fmaxf(fabsf(dy.y), fabsf(dz.y))) > edge) {
+                            dx.y = (float)(bh_mic<PER>(w.ps[sj] - xi1, w.L, w.halfL) * inv_ell);
+                            dy.y = (float)(bh_mic<PER>(w.ps[cap + sj] - yi1, w.L, w.halfL) * inv_ell);
+                            dz.y = (float)(bh_mic<PER>(w.ps[2 * (size_t)cap + sj] - zi1, w.L, w.halfL) * inv_ell);
+                        }
+                    }
+                    const float2 r2 = p_fma(dx, dx, p_fma(dy, dy, p_mul(dz, dz)));
+                    const float2 rs = p_add(ris, dup2(o.w)), rs2 = p_mul(rs, rs);
+                    // excluded: padding target, the target itself, or closer than r_i + r_j
+                    const bool e0 = !v0 || sj == si0 || r2.x < rs2.x, e1 = !v1 || sj == si1 || r2.y < rs2.y;
+                    if (e0 && e1) continue;
+                    const float2 rinv = p_rsqrt(make_float2(e0 ? 1.f : r2.x, e1 ? 1.f : r2.y));
+                    const float2 rinv2 = p_mul(rinv, rinv);
+                    const float2 keep = make_float2(e0 ? 0.f : 1.f, e1 ? 0.f : 1.f);
+                    if (FORCE) {
+                        const float rj3 = o.w * o.w * o.w;
+                        const float2 r7 = p_mul(p_mul(rinv2, rinv2), p_mul(rinv2, rinv));
+                        mono_force2(dx, dy, dz, p_mul(p_mul(dup2(rj3), keep), r7), ax, ay, az);
+                    } else {  // e = x_i - x_j = -d
+                        const float4 fj = w.fs32[sj];
+                        const float2 ex = p_mul(dup2(-1.f), dx), ey = p_mul(dup2(-1.f), dy),
+                                     ez = p_mul(dup2(-1.f), dz);
+                        stokeslet2(ex, ey, ez, dup2(fj.x), dup2(fj.y), dup2(fj.z), p_mul(rinv, keep), rinv2, ax, ay,
+                                   az);
+                    }
+                }
+                continue;
+            }
+            if (sp + nch > BH_STACK) {  // cannot happen for depth <= 10; kept bounded anyway
+                broken = true;
+                break;
+            }
+            if (lane < nch) stack[wp][sp + lane] = mt.z + lane;
+            sp += nch;
+            __syncwarp();
+        }
+        if (broken && lane == 0) raise_device_error(w.err, DEM_DEVERR_NODE_OVERFLOW);
+#pragma unroll
+        for (int t = 0; t < 2; ++t) {
+            const bool valid = t ? v1 : v0;
+            if (!valid) continue;
+            const int si = t ? si1 : si0;
+            const double ri = t ? ri1 : ri0;
+            const float gx = t ? ax.y : ax.x, gy = t ? ay.y : ay.x, gz = t ? az.y : az.x;
+            const int i = w.idx[si];
+            double vx, vy, vz;
+            if (FORCE) {  // F = m r_i^3 acc / ell
+                const double f = coeff * ri * ri * ri * inv_ell;
+                vx = f * gx;
+                vy = f * gy;
+                vz = f * gz;
+                fsort_out[si] = vx;
+                fsort_out[cap + si] = vy;
+                fsort_out[2 * (size_t)cap + si] = vz;
+            } else {  // u = eta / (ell 2^-q) acc  (+ F / (stokes r))
+                const double f = coeff * inv_ell / fsc;
+                vx = f * gx;
+                vy = f * gy;
+                vz = f * gz;
+                if (stokes > 0.0) {
+                    const double a = 1.0 / (stokes * ri);
+                    vx += w.fsort[si] * a;
+                    vy += w.fsort[cap + si] * a;
+                    vz += w.fsort[2 * (size_t)cap + si] * a;
+                }
+            }
+            ox[i] = vx;
+            oy[i] = vy;
+            oz[i] = vz;
+        }
+        __syncwarp();
+    }
+    for (int o = 16; o; o >>= 1) {  // per-target counts, summed over the warp
+        pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
+        nodes += __shfl_xor_sync(0xffffffffu, nodes, o);
+    }
+    if (lane == 0) {
+        atomicAdd(&w.counters[0], pairs);
+        atomicAdd(&w.counters[1], nodes);
+    }
+}
+
 __global__ void forces_to_sorted_kernel(int n, int cap, const int32_t *__restrict__ idx, const double *__restrict__ fx,
                                         const double *__restrict__ fy, const double *__restrict__ fz,
                                         double *__restrict__ fsort) {
@@ -1257,6 +1546,8 @@ static BhWalk walk_args(dem_bh *b, float theta) {
 }
 
 static int walk_grid(dem_bh *b) { return std::max(1, (b->n + BH_T - 1) / BH_T); }
+// bh_walk2_kernel: 64 targets per warp
+static int walk2_grid(dem_bh *b) { return std::max(1, (b->n + 2 * BH_T - 1) / (2 * BH_T)); }
 
 int dem_bh_forces(dem_bh *b, double m_const, double theta, double *fx, double *fy, double *fz, void *stream) {
     if (!b || !(theta >= 0)) return DEM_E_INVALID;
@@ -1268,9 +1559,9 @@ int dem_bh_forces(dem_bh *b, double m_const, double theta, double *fx, double *f
     const BhWalk w = walk_args(b, (float)theta);
     dem_prof_begin(ctx, "bh_force_walk", s);
     if (b->periodic)
-        bh_walk_kernel<true, true><<<walk_grid(b), BH_T, 0, counted(s)>>>(w, m_const, 0.0, fx, fy, fz, b->fsort);
+        bh_walk2_kernel<true, true><<<walk2_grid(b), BH_T, 0, counted(s)>>>(w, m_const, 0.0, fx, fy, fz, b->fsort);
     else
-        bh_walk_kernel<false, true><<<walk_grid(b), BH_T, 0, counted(s)>>>(w, m_const, 0.0, fx, fy, fz, b->fsort);
+        bh_walk2_kernel<false, true><<<walk2_grid(b), BH_T, 0, counted(s)>>>(w, m_const, 0.0, fx, fy, fz, b->fsort);
     dem_prof_end(ctx, s);
     return dem_check_launch(ctx, "bh force walk");
 }
@@ -1313,11 +1604,11 @@ int dem_bh_velocity(dem_bh *b, const double *fx, const double *fy, const double 
             bh_walk_kernel<false, false, true><<<walk_grid(b), BH_T, 0, counted(s)>>>(w, eta_const, stokes_factor, vx,
                                                                                       vy, vz, nullptr);
     } else if (b->periodic) {
-        bh_walk_kernel<true, false><<<walk_grid(b), BH_T, 0, counted(s)>>>(w, eta_const, stokes_factor, vx, vy, vz,
-                                                                           nullptr);
+        bh_walk2_kernel<true, false><<<walk2_grid(b), BH_T, 0, counted(s)>>>(w, eta_const, stokes_factor, vx, vy, vz,
+                                                                             nullptr);
     } else {
-        bh_walk_kernel<false, false><<<walk_grid(b), BH_T, 0, counted(s)>>>(w, eta_const, stokes_factor, vx, vy, vz,
-                                                                            nullptr);
+        bh_walk2_kernel<false, false><<<walk2_grid(b), BH_T, 0, counted(s)>>>(w, eta_const, stokes_factor, vx, vy,
+                                                                              vz, nullptr);
     }
     dem_prof_end(ctx, s);
     return dem_check_launch(ctx, "bh velocity walk");

@@ -42,11 +42,6 @@
 
 namespace dem {
 
-__device__ __forceinline__ float2 p_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 p_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 p_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-__device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
-
 // Packed layout of the symmetric passes (npad_total entries, zero padded):
 //   force:       p0 = (x, x, y, y)      p1 = (z, z, r^3, r^3)   k2 = (k r, k r)
 //   convection:  p0 = -(x, x, y, y)     p1 = (-z, -z, k r, k r)

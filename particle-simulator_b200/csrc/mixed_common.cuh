@@ -30,6 +30,13 @@ struct MixedArgs {
     uint32_t *err;
 };
 
+// Packed FP32x2 arithmetic (sm_100 add/mul/fma.f32x2, round to nearest): one
+// instruction on two independent lanes of a float2.
+__device__ __forceinline__ float2 p_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 p_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 p_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
+
 __device__ __forceinline__ void two_sum_fold(float &hi, float &lo, float a) {
     const float s = hi + a;
     const float bp = s - hi;
