@@ -260,6 +260,18 @@ DEM_API int dem_direct_convection(dem_ctx *ctx, int n, const double *x, const do
                           const double *fx, const double *fy, const double *fz, double eta_const, double L,
                           int periodic, int precision, double *vx, double *vy, double *vz, void *stream);
 
+/* Forces, then the Oseen convection of those forces (correction off): the
+ * two calls above on the same positions, in one call.  With DEM_PREC_MIXED
+ * the convection pass reuses the Morton order the force pass sorted the
+ * droplets into (the results equal those of the two calls, bit for bit).
+ * r may not be NULL.
+ * Replaces DirectDropletForceCalculator.calculate_forces_and_convection,
+ * dem/force_calculator/direct_droplet_force_calculator.py:470-527. */
+DEM_API int dem_direct_forces_and_convection(dem_ctx *ctx, int n, const double *x, const double *y, const double *z,
+                                             const double *r, double m_const, double eta_const, double L,
+                                             int periodic, int precision, double *fx, double *fy, double *fz,
+                                             double *vx, double *vy, double *vz, void *stream);
+
 /* ---- periodic-image Oseen correction (COMSOL lattice grid) ------------ */
 /* A correction grid uploaded to the device.  grid_u/v/w: HOST arrays of n^3
  * doubles in C order [ix][iy][iz], the velocity of the periodic images of a

@@ -130,7 +130,10 @@ static int batch_step(dem_batch *b, double *x, double *y, double *z, const doubl
                       double *vz, cudaStream_t s) {
     int rc = batch_forces(b, x, y, z, r, m_const, fx, fy, fz, s);
     if (rc) return rc;
-    if ((rc = batch_convection(b, x, y, z, r, fx, fy, fz, eta, vx, vy, vz, s))) return rc;
+    b->ctx->sym_reuse_order = true;  // the same positions: the force pass's Morton order holds
+    rc = batch_convection(b, x, y, z, r, fx, fy, fz, eta, vx, vy, vz, s);
+    b->ctx->sym_reuse_order = false;
+    if (rc) return rc;
     return launch_euler_direct_boxes(b->ctx, b->n, b->nbox, b->off, b->L, x, y, z, r, fx, fy, fz, vx, vy, vz, stokes,
                                      dt, b->periodic, x, y, z, s);
 }

@@ -60,6 +60,18 @@ int dem_direct_forces(dem_ctx *ctx, int n, const double *x, const double *y, con
     return dem_set_error(ctx, DEM_E_INVALID, "unknown precision");
 }
 
+int dem_direct_forces_and_convection(dem_ctx *ctx, int n, const double *x, const double *y, const double *z,
+                                     const double *r, double m_const, double eta_const, double L, int periodic,
+                                     int precision, double *fx, double *fy, double *fz, double *vx, double *vy,
+                                     double *vz, void *stream) {
+    int rc = dem_direct_forces(ctx, n, x, y, z, r, m_const, L, periodic, precision, fx, fy, fz, stream);
+    if (rc || n == 0) return rc;
+    ctx->sym_reuse_order = precision == DEM_PREC_MIXED;  // the positions are the force pass's
+    rc = dem_direct_convection(ctx, n, x, y, z, r, fx, fy, fz, eta_const, L, periodic, precision, vx, vy, vz, stream);
+    ctx->sym_reuse_order = false;
+    return rc;
+}
+
 int dem_direct_convection(dem_ctx *ctx, int n, const double *x, const double *y, const double *z, const double *r,
                             const double *fx, const double *fy, const double *fz, double eta_const, double L,
                             int periodic, int precision, double *vx, double *vy, double *vz, void *stream) {

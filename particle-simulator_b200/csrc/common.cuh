@@ -48,6 +48,15 @@ struct dem_ctx {
     double *partial = nullptr;  // mixed: [splits][3][capacity] chunk partial sums
     double *sym_partial = nullptr;  // mixed, symmetric schedule: per block-pair partial sums
     size_t sym_partial_bytes = 0;
+    // The Morton permutation a symmetric pass left in its workspace, and the layout it was
+    // made for.  A caller that runs the convection pass on the positions of the force pass it
+    // just ran (dem_direct_forces_and_convection, dem_batch_step) sets sym_reuse_order for
+    // that pass, which then skips the sort when the layout matches.
+    struct {
+        const void *work = nullptr;
+        int n_total = -1, npad_total = -1, nbox = 0, ipt = 0, per = -1;
+    } sym_order;
+    bool sym_reuse_order = false;
     int partial_splits = 0;
     double *dscratch = nullptr;     // 8 doubles: reductions (max radius, ...)
     int32_t *cell_hash = nullptr;   // hash bucket per particle

@@ -1339,21 +1339,32 @@ static int run_sym_sorted(dem_ctx *ctx, const SymBoxes &t, int ipt, int ctas, bo
     // sorted position -> droplet; box b keeps positions [off[b], off[b + 1]).  An open single box
     // sorts in its droplets' bounding cube; boxes of an ensemble and periodic boxes in [0, L_b)^3,
     // then (ensembles) a stable pass on the box index groups every box's droplets
-    int rc;
-    const int32_t *perm = mw.idx[0];
+    int rc = DEM_OK;
+    const int32_t *perm = t.nbox > 1 ? mw.idx[1] : mw.idx[0];
     const int kg = max(1, min(ceil_div(n, 256), 8 * ctx->sm_count));
-    if (t.nbox == 1 && !per) {
-        rc = morton_order(ctx, n, m.x, m.y, m.z, 0, m.L, mw, s);
-    } else {
-        box_morton_keys_kernel<<<kg, 256, 0, counted(s)>>>(t, m.x, m.y, m.z, mw.keys[0], mw.idx[0]);
-        rc = radix_sort_pairs(ctx, n, mw, s);
-        if (!rc && t.nbox > 1) {
-            box_of_kernel<<<kg, 256, 0, counted(s)>>>(t, mw.idx[0], mw.keys[0]);
-            rc = radix_pass(ctx, n, mw.keys[0], mw.idx[0], mw.keys[1], mw.idx[1], 0, mw.hist, s);
-            perm = mw.idx[1];
+    auto &ord = ctx->sym_order;
+    const bool reuse = ctx->sym_reuse_order && ord.work == work && ord.n_total == n &&
+                       ord.npad_total == t.npad_total && ord.nbox == t.nbox && ord.ipt == ipt && ord.per == (int)per;
+    if (!reuse) {  // (reuse: the caller's previous pass sorted these positions into this workspace)
+        ord.work = nullptr;
+        if (t.nbox == 1 && !per) {
+            rc = morton_order(ctx, n, m.x, m.y, m.z, 0, m.L, mw, s);
+        } else {
+            box_morton_keys_kernel<<<kg, 256, 0, counted(s)>>>(t, m.x, m.y, m.z, mw.keys[0], mw.idx[0]);
+            rc = radix_sort_pairs(ctx, n, mw, s);
+            if (!rc && t.nbox > 1) {
+                box_of_kernel<<<kg, 256, 0, counted(s)>>>(t, mw.idx[0], mw.keys[0]);
+                rc = radix_pass(ctx, n, mw.keys[0], mw.idx[0], mw.keys[1], mw.idx[1], 0, mw.hist, s);
+            }
         }
+        if (rc) return rc;
+        ord.work = work;
+        ord.n_total = n;
+        ord.npad_total = t.npad_total;
+        ord.nbox = t.nbox;
+        ord.ipt = ipt;
+        ord.per = (int)per;
     }
-    if (rc) return rc;
     const int pgrid = max(1, min(ceil_div(t.npad_total, 256), 4 * ctx->sm_count));
     prep_sym_kernel<FORCE><<<pgrid, 256, 0, counted(s)>>>(t, m.x, m.y, m.z, m.r, m.fx, m.fy, m.fz,
                                                           FORCE ? ctx->tuning.near_force : ctx->tuning.near_oseen,

@@ -187,11 +187,12 @@ __device__ __forceinline__ void for_each_contact(int i, int ti, const double *__
         }
         if (contact_rn(dx * dx + dy * dy + dz * dz, ri + rj)) f(j, m);  // dist <= r_i + r_j
     };
+    // PACKED: the slot's index and FP32 record are loaded together (one round of loads per candidate)
     auto candidate = [&](int32_t s, int m) {
         const int32_t j = sorted_idx[s];
-        if (!(i < j)) return;
         if (PACKED) {
             const float4 q = P32[s];
+            if (!(i < j)) return;
             float ax = fabsf(q.x - qi.x), ay = fabsf(q.y - qi.y), az = fabsf(q.z - qi.z);
             if (periodic) {
                 ax = fminf(ax, fabsf(ax - Lf));
@@ -203,6 +204,7 @@ __device__ __forceinline__ void for_each_contact(int i, int ti, const double *__
             const double2 a = P[2 * s], b = P[2 * s + 1];
             bucket(a.x, a.y, b.x, b.y, j, m);
         } else {
+            if (!(i < j)) return;
             bucket(x[j], y[j], z[j], r[j], j, m);
         }
     };
@@ -229,6 +231,35 @@ __device__ __forceinline__ void for_each_contact(int i, int ti, const double *__
 #pragma unroll
             for (int m = 0; m < c; ++m) dup |= h[c] >= 0 && h[c] == h[m];
         if (!dup) {
+            if (PACKED) {
+                // the next cell's bucket range is loaded while this cell's candidates are tested, and
+                // candidates are taken two at a time: the loop is bound by load latency, not arithmetic
+                int32_t start = 0, end = 0;
+                if (h[0] >= 0) {
+                    start = bstart[h[0]];
+                    end = bstart[h[0] + 1];
+                }
+#pragma unroll 1
+                for (int c = 0; c < 27; ++c) {
+                    int32_t ns = 0, ne = 0;
+                    const int32_t hn = c + 1 < 27 ? cell_hash(c + 1) : -1;
+                    if (hn >= 0) {
+                        ns = bstart[hn];
+                        ne = bstart[hn + 1];
+                    }
+                    if (end > n) end = n;  // :199-201
+                    int32_t s = start;
+#pragma unroll 1
+                    for (; s + 1 < end; s += 2) {
+                        candidate(s, 1);
+                        candidate(s + 1, 1);
+                    }
+                    if (s < end) candidate(s, 1);
+                    start = ns;
+                    end = ne;
+                }
+                return;
+            }
             for (int c = 0; c < 27; ++c) {
                 const int32_t hc = cell_hash(c);
                 if (hc < 0) continue;

@@ -90,6 +90,8 @@ SIGNATURES = {
     "dem_soa_to_aos": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp]),
     "dem_direct_forces": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _d, _d, _i, _i, _vp, _vp, _vp, _vp]),
     "dem_direct_convection": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _d, _d, _i, _i, _vp, _vp, _vp, _vp]),
+    "dem_direct_forces_and_convection": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _d, _d, _d, _i, _i, _vp, _vp, _vp, _vp,
+                                              _vp, _vp, _vp]),
     "dem_euler_update": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _d, _d, _d, _i, _vp, _vp, _vp, _vp]),
     "dem_euler_update_total": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _d, _d, _i, _vp, _vp, _vp, _vp]),
     "dem_hash_detect": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _d, _i, _i, _vp, _i64, _vp, _vp]),
@@ -303,6 +305,15 @@ class Context:
                                         ptr(F[1]), ptr(F[2]), float(eta_const), float(L), int(periodic),
                                         int(precision), ptr(out[0]), ptr(out[1]), ptr(out[2]), self.stream()),
             "direct_convection",
+        )
+
+    def direct_forces_and_convection(self, n, pos, r, m_const, eta_const, L, periodic, precision, F, V):
+        self._check(
+            lib().dem_direct_forces_and_convection(self.handle, n, ptr(pos[0]), ptr(pos[1]), ptr(pos[2]), ptr(r),
+                                                   float(m_const), float(eta_const), float(L), int(periodic),
+                                                   int(precision), ptr(F[0]), ptr(F[1]), ptr(F[2]), ptr(V[0]),
+                                                   ptr(V[1]), ptr(V[2]), self.stream()),
+            "direct_forces_and_convection",
         )
 
     def direct_convection_corr(self, corr: "Correction", n, pos, r, F, eta_const, L, periodic, precision, out):

@@ -107,6 +107,18 @@ class DirectDropletForceCalculator(ForceCalculator):
                                         N.PRECISIONS[self.precision], V)
         return V
 
+    def _both_dev(self, st):
+        """Forces and the convection of those forces on one state (one library call
+        without the correction: the convection pass reuses the force pass's droplet order)."""
+        if self._corr is not None:
+            F = self._forces_dev(st)
+            return F, self._convection_dev(st, F)
+        F = self._io.buf.dev("forces", (3, st.n))
+        V = self._io.buf.dev("velocities", (3, st.n))
+        self._ctx.direct_forces_and_convection(st.n, st.pos, st.r, self.m_const, self.eta_const, self.L,
+                                               self.periodic, N.PRECISIONS[self.precision], F, V)
+        return F, V
+
     def calculate(self, positions, radii):
         """Forces (N, 3): direct_droplet_force_calculator.py:260-305."""
         self.num_particles = len(radii)
@@ -133,8 +145,7 @@ class DirectDropletForceCalculator(ForceCalculator):
         self.num_particles = len(radii)
         self._reserve(self.num_particles)
         st, on_dev = self._io.positions(positions, radii)
-        F = self._forces_dev(st)
-        V = self._convection_dev(st, F)
+        F, V = self._both_dev(st)
         if on_dev:
             return self._io.to_aos_tensor(F, st.n), self._io.to_aos_tensor(V, st.n)
         f, v = self._io.download([F, V], st.n)
@@ -150,9 +161,7 @@ class DirectDropletForceCalculator(ForceCalculator):
 
         st = _S()
         st.n, st.pos, st.r = n, pos_soa, r
-        F = self._forces_dev(st)
-        V = self._convection_dev(st, F)
-        return F, V
+        return self._both_dev(st)
 
     def set_tuning(self, **kw):
         """Tune the mixed-precision kernels (see dem_direct_set_tuning)."""

@@ -127,6 +127,36 @@ def test_symmetric_morton_blocks_against_oracle_and_plain_blocks(periodic, n):
     assert fc._ctx.device_errors() == 0
 
 
+@pytest.mark.parametrize("periodic,n,schedule", [(True, 20000, "symmetric"), (False, 9000, "symmetric"),
+                                                  (True, 3000, "split"), (True, 5000, "symmetric_plain")])
+def test_fused_call_equals_the_two_passes(periodic, n, schedule):
+    """dem_direct_forces_and_convection (the convection pass reuses the force
+    pass's Morton order) against dem_direct_forces + dem_direct_convection."""
+    import torch
+
+    pos, r, L = lognormal_state(n, seed=13, periodic=periodic)
+    m, eta, _ = consts()
+    fc = _calc(n, L, periodic, precision="mixed")
+    fc.set_tuning(schedule=schedule)
+    st, _ = fc._io.positions(pos, r)
+    from dem import _native as N
+
+    ctx, prec = fc._ctx, N.PREC_MIXED
+    F1 = torch.empty((3, n), dtype=torch.float64, device="cuda")
+    V1, F2, V2 = torch.empty_like(F1), torch.empty_like(F1), torch.empty_like(F1)
+    ctx.direct_forces(n, st.pos, st.r, fc.m_const, L, periodic, prec, F1)
+    ctx.direct_convection(n, st.pos, st.r, F1, fc.eta_const, L, periodic, prec, V1)
+    ctx.direct_forces_and_convection(n, st.pos, st.r, fc.m_const, fc.eta_const, L, periodic, prec, F2, V2)
+    assert torch.equal(F1, F2) and torch.equal(V1, V2)
+    # and once more after a pass on other positions (the kept order must not leak into a later call)
+    other, _, _ = lognormal_state(n, seed=14, periodic=periodic)
+    st2, _ = fc._io.positions(other, r, tag="other")
+    ctx.direct_forces(n, st2.pos, st.r, fc.m_const, L, periodic, prec, F1)
+    ctx.direct_convection(n, st.pos, st.r, F2, fc.eta_const, L, periodic, prec, V1)
+    assert torch.equal(V1, V2)
+    assert ctx.device_errors() == 0
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_open_boundary_and_contact_cut(golden, precision):
     g = golden("direct_contact_n48.npz")  # many pairs inside r_i + r_j
