@@ -70,6 +70,8 @@ def parse():
                          "correction: Oseen convection with the periodic-image correction (48^3 grid) at --n; "
                          "trajectory: --traj-steps direct steps in FP64 and mixed from one state, compared")
     ap.add_argument("--traj-steps", type=int, default=1000)
+    ap.add_argument("--adjoint-steps", type=int, default=200,
+                    help="adjoint: Euler steps per gradient (200: the measured configuration; fewer for a profile)")
     ap.add_argument("--accuracy", action="store_true", help="tree: errors on 4,096 droplets against direct FP64 sums")
     ap.add_argument("--fd", type=int, default=0, help="adjoint: central-difference checks on this many coordinates")
     ap.add_argument("--boxes", type=int, default=64)
@@ -647,7 +649,7 @@ def report_batched(args, res, world):
             "peak": peak,
             "unit": "TFLOP/s",
             "frac": achieved / peak,
-            "traffic": None,
+            "traffic": ncu_traffic("batched_step_pair_passes"),
             "flops_per_pair": FLOPS_FORCE_PAIR + FLOPS_OSEEN_PAIR,
             "units_per_launch": f"sum_b N_b(N_b-1) = {int(pairs)} ordered pairs per step",
         },
@@ -677,7 +679,7 @@ def run_adjoint(args, device):
     x0 = torch.tensor(pos, dtype=torch.float64, device=device)
     rr = torch.tensor(r, dtype=torch.float64, device=device)
     E0 = torch.tensor(PHYS["E"], dtype=torch.float64, device=device)
-    steps = 200
+    steps = args.adjoint_steps
     phys = dict(eps_oil=PHYS["eps_oil"], eta_oil=PHYS["eta_oil"], eta_water=PHYS["eta_water"])
 
     def loss(sim, x, rad, E):
@@ -700,9 +702,15 @@ def run_adjoint(args, device):
         torch.cuda.synchronize()
         if k >= max(args.warmup, 1):
             times.append((t0.elapsed_time(t1), t1.elapsed_time(t2)))
+        if k == max(args.warmup, 1) - 1:  # the timed gradients: per-kernel events on the trajectory's context
+            sim._ctx.profile(True)
+            sim._ctx.profile_reset()
+    vjp_ms, vjp_launches = sim._ctx.profile_read("vjp_pass")
+    sim._ctx.profile(False)
     fwd = float(np.median([a for a, _ in times]))
     bwd = float(np.median([b for _, b in times]))
-    out = dict(n=n, steps=steps, forward_ms=fwd, backward_ms=bwd, loss=float(val.detach()))
+    out = dict(n=n, steps=steps, forward_ms=fwd, backward_ms=bwd, loss=float(val.detach()),
+               vjp_pass_ms_per_launch=vjp_ms / max(vjp_launches, 1), vjp_pass_launches=vjp_launches)
     if args.fd > 0:
         # Central differences need a smooth forward map.  In a periodic box the
         # minimum image of a pair switches when a separation crosses L/2 (about
@@ -746,10 +754,30 @@ def run_adjoint(args, device):
     return out
 
 
+# FP64 operations of vjp_pair_kernel per ordered pair (adds and multiplies 1, FMA 2), counted
+# from its source: separation and |d|^-1 (Newton) 20, force-term Hessian and radius terms 76,
+# the two Oseen K terms 90
+FLOPS_VJP_PAIR = 186
+FP64_PEAK_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12  # SMs x FP64 lanes x 2 flop x max SM clock
+
+
+def ncu_traffic(kernel):
+    """DRAM bytes (read + write) per launch of a kernel from one ncu capture
+    (profiles/traffic.json, written from the captures summarised in profiles/), or None."""
+    prof = ROOT / "profiles" / "traffic.json"
+    try:
+        return json.loads(prof.read_text()).get(kernel)
+    except (OSError, ValueError):
+        return None
+
+
 def report_adjoint(args, res):
     total = res["forward_ms"] + res["backward_ms"]
+    n, steps = res["n"], res["steps"]
+    vjp_ms = res["vjp_pass_ms_per_launch"]
+    achieved = FLOPS_VJP_PAIR * n * (n - 1) / (vjp_ms * 1e-3) / 1e12 if vjp_ms > 0 else 0.0
     line = {
-        "metric": "DEM adjoint: gradient evaluations/s (N=16384, 200 steps)",
+        "metric": f"DEM adjoint: gradient evaluations/s (N={n}, {steps} steps)",
         "value": 1000.0 / total,
         "unit": "gradients/s",
         "n_gpus": 1,
@@ -761,10 +789,17 @@ def report_adjoint(args, res):
         "vs_baseline": None,
         "dtype": "forward f32 pair terms + f64 near pairs/sums; VJP f64",
         "data": "synthetic (seeded lognormal droplets, 2% volume fraction)",
-        "config": {"workload": "adjoint: 200 Euler steps at N=16384, collisions frozen, checkpoint every 20 steps; "
-                               "loss = mean squared z displacement + pair softplus((2.5 (r_i+r_j) - |r_ij|) / 1 um); "
-                               "gradients w.r.t. initial positions, radii and |E|",
+        "config": {"workload": f"adjoint: {steps} Euler steps at N={n}, collisions frozen, checkpoint every 20 "
+                               "steps; loss = mean squared z displacement + pair softplus((2.5 (r_i+r_j) - |r_ij|) "
+                               "/ 1 um); gradients w.r.t. initial positions, radii and |E|",
                    **res},
+        "roofline": {"kernel": "vjp_pass (vjp_pair_kernel + its fixed-order finish)", "bound": "fp64_pipe",
+                     "achieved": achieved, "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s",
+                     "frac": achieved / FP64_PEAK_TFLOPS,
+                     "peak_source": "148 SMs x 64 FP64 lanes x 2 flop x 1965 MHz (max SM clock); "
+                                    "MEASURED_PEAKS.json holds no FP64 figure",
+                     "flops_per_pair": FLOPS_VJP_PAIR, "units_per_launch": f"N(N-1) = {n * (n - 1)} ordered pairs",
+                     "traffic": ncu_traffic("vjp_pass") if n == 16384 else None},
     }
     print(json.dumps(line), flush=True)
 
@@ -910,7 +945,7 @@ def report_tree(args, res):
             "peak": peak,
             "unit": "TFLOP/s",
             "frac": achieved / peak if achieved else None,
-            "traffic": None,
+            "traffic": ncu_traffic("bh_force_walk"),
             "units_per_launch": "leaf pair terms x 33 flops + node terms x 103 flops (monopole + quadrupole)",
         },
         "clocks": clocks,
@@ -1373,13 +1408,7 @@ def main():
     lanes = FP32_LANES_PER_SM if prec == "mixed" else FP32_LANES_PER_SM // 2
     peak = SM_COUNT_B200 * lanes * 2 * max_mhz * 1e6 / 1e12
     peak_at_clock = SM_COUNT_B200 * lanes * 2 * (clocks.get("sm_mhz") or max_mhz) * 1e6 / 1e12
-    traffic = None
-    prof = ROOT / "profiles" / "traffic.json"
-    if prof.exists():
-        try:
-            traffic = json.loads(prof.read_text()).get(dom)
-        except Exception:
-            traffic = None
+    traffic = ncu_traffic(dom)
     line = {
         "metric": f"DEM steps/s (direct, N={n})",
         "value": steps_per_s,

@@ -307,22 +307,40 @@ __device__ __forceinline__ int digit_lower_bound(const uint32_t *keys, int lo, i
     return lo;
 }
 
+// Split points of the nodes [ls, le): eight lanes per node, lane o searching the first droplet
+// of octant o over the whole node (the digits never decrease inside a node's run, so this
+// equals a search that starts from octant o - 1's point) -- the eight searches run side by
+// side instead of one after another, which matters for the few huge nodes of the top levels.
 __global__ void level_count_kernel(BhNodes nd, const uint32_t *__restrict__ keys, int ls, int le, int leaf_size,
                                    int32_t *__restrict__ bounds, int M, int32_t *__restrict__ nchild_out) {
-    for (int k = ls + blockIdx.x * blockDim.x + threadIdx.x; k < le; k += gridDim.x * blockDim.x) {
-        const int s0 = nd.start[k], c = nd.count[k], lv = nd.level[k];
-        int nch = 0;
-        if (c > leaf_size && lv < BH_MAX_LEVEL) {
-            const int shift = 27 - 3 * lv;
-            int b[9];
-            b[0] = s0;
-            b[8] = s0 + c;
-            for (uint32_t o = 1; o < 8; ++o) b[o] = digit_lower_bound(keys, b[o - 1], s0 + c, shift, o);
-            for (int o = 0; o < 9; ++o) bounds[o * M + k] = b[o];
-            for (int o = 0; o < 8; ++o) nch += b[o + 1] > b[o];
+    const int lane = threadIdx.x & 31;
+    const long long total = 8LL * (le - ls);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    // whole warps iterate together (the octant counts below are warp votes)
+    for (long long base = (long long)blockIdx.x * blockDim.x + threadIdx.x - lane; base < total; base += stride) {
+        const long long t = base + lane;
+        const bool live = t < total;
+        const int k = live ? ls + (int)(t >> 3) : ls, o = (int)(t & 7);
+        int s0 = 0, c = 0, bo = 0;
+        bool split = false;
+        if (live) {
+            s0 = nd.start[k];
+            c = nd.count[k];
+            split = c > leaf_size && nd.level[k] < BH_MAX_LEVEL;
+            if (split) bo = o == 0 ? s0 : digit_lower_bound(keys, s0, s0 + c, 27 - 3 * nd.level[k], (uint32_t)o);
         }
-        nd.nchild[k] = nch;
-        nchild_out[k - ls] = nch;
+        const int next = __shfl_down_sync(0xffffffffu, bo, 1);  // octant o + 1's point (lanes of one node)
+        const int hi = o == 7 ? s0 + c : next;
+        const unsigned nonempty = __ballot_sync(0xffffffffu, split && hi > bo);
+        const int nch = __popc((nonempty >> (lane & ~7)) & 0xffu);
+        if (live && split) {
+            bounds[o * M + k] = bo;
+            if (o == 7) bounds[8 * M + k] = s0 + c;
+        }
+        if (live && o == 0) {
+            nd.nchild[k] = nch;
+            nchild_out[k - ls] = nch;
+        }
     }
 }
 
@@ -1476,8 +1494,9 @@ int dem_bh_build(dem_bh *b, int n, const double *x, const double *y, const doubl
         const int width = le - ls;
         int total = 0;
         for (int attempt = 0; attempt < 2; ++attempt) {
-            level_count_kernel<<<grid_of(ctx, width), 256, 0, counted(s)>>>(b->nd, b->keys[0], ls, le, leaf_size,
-                                                                           b->bounds, b->max_nodes, b->scan_in);
+            level_count_kernel<<<grid_of(ctx, 8LL * width), 256, 0, counted(s)>>>(b->nd, b->keys[0], ls, le,
+                                                                                 leaf_size, b->bounds, b->max_nodes,
+                                                                                 b->scan_in);
             if ((rc = exclusive_scan<int32_t, int32_t>(ctx, b->scan_in, b->coff, width, s))) return rc;
             if ((rc = dem_check_cuda(
                      ctx, cudaMemcpyAsync(&total, b->coff + width, sizeof(int), cudaMemcpyDeviceToHost, s),
