@@ -11,12 +11,20 @@ eta_water 0.001, dt = 1e-4 s.  One step = collision detection (spatial hash)
 update with the periodic wrap, all on the device.
 
 Printed JSON (rank 0, one line):
-  value        steps/s of the whole job, inputs resident in HBM
+  value        steps/s of the whole job, inputs resident in HBM (20 timed steps
+               after 500 untimed ones and the warm-up, so coalescence happens)
   e2e          steps/s through the public numpy API (host buffers every step:
                detection + forces/convection uploads, results downloaded)
-  roofline     the dominant kernel (mixed force pass) against the FP32 pipe
+  roofline     the dominant kernel (the longer of the two mixed pair passes)
+               against the FP32 pipe; traffic from profiles/traffic.json
+  memory_bound hash detection against the measured HBM copy bandwidth
+  fp64_gpu     the bit-exact FP64 GPU step on the same state, and the speed-up
+  accuracy_mixed_vs_fp64  forces and convection, mixed against FP64
   cpu_baseline the CPU oracle (restatement of the reference kernels, all host
                threads) on a bounded row sample, extrapolated to a full step
+Other workloads (--workload): batched (64 boxes), adjoint, tree (Barnes-Hut at
+N = 2^20), parity_tree (the reference-parity FP64 tree), correction (Oseen pass
+with the periodic-image correction), trajectory (mixed against FP64 over a run).
 Multi-GPU (torchrun): every rank integrates its own independent box (replicas;
 weak scaling); value sums the ranks' steps/s over the max-over-ranks time.
 """
