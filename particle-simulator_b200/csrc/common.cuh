@@ -60,6 +60,7 @@ struct dem_ctx {
     int partial_splits = 0;
     double *dscratch = nullptr;     // 8 doubles: reductions (max radius, ...)
     int32_t *cell_hash = nullptr;   // hash bucket per particle
+    int32_t *cell_xyz = nullptr;    // cell coordinates per particle, [3][capacity] (the count pass)
     int32_t *bucket_count = nullptr;  // table
     int32_t *bucket_start = nullptr;  // table (exclusive scan)
     int32_t *bucket_cursor = nullptr; // table

@@ -174,6 +174,7 @@ int dem_ctx_reserve(dem_ctx *ctx, int capacity) {
     if ((rc = grow(ctx, &ctx->pack_a, n, "workspace"))) return rc;
     if ((rc = grow(ctx, &ctx->pack_b, n, "workspace"))) return rc;
     if ((rc = grow(ctx, &ctx->cell_hash, n, "workspace"))) return rc;
+    if ((rc = grow(ctx, &ctx->cell_xyz, 3 * n, "workspace"))) return rc;
     if ((rc = grow(ctx, &ctx->sorted_idx, n, "workspace"))) return rc;
     if ((rc = grow(ctx, &ctx->hash_pos, 2 * n, "workspace"))) return rc;
     if ((rc = grow(ctx, &ctx->hash_pos32, n, "workspace"))) return rc;
@@ -224,7 +225,7 @@ void dem_ctx_destroy(dem_ctx *ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     void *ptrs[] = {ctx->d_err,         ctx->pack_a,      ctx->pack_b,     ctx->partial,    ctx->dscratch,
-                    ctx->cell_hash,     ctx->bucket_count, ctx->bucket_start, ctx->bucket_cursor, ctx->sorted_idx, ctx->hash_pos, ctx->hash_pos32,
+                    ctx->cell_hash,     ctx->cell_xyz, ctx->bucket_count, ctx->bucket_start, ctx->bucket_cursor, ctx->sorted_idx, ctx->hash_pos, ctx->hash_pos32,
                     ctx->pair_count,    ctx->pair_offset, ctx->flags,      ctx->keep_off,   ctx->merged_buf,
                     ctx->merged_cnt,    ctx->scan_tmp,    ctx->sym_partial};
     for (void *p : ptrs)

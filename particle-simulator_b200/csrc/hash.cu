@@ -88,6 +88,12 @@ __device__ __forceinline__ int32_t floor_mod(int32_t a, int32_t m) {
     return q < 0 ? q + m : q;
 }
 
+// floor_mod(a, m) for a in [-1, m] (a neighbour of a periodic cell coordinate)
+__device__ __forceinline__ int32_t wrap1(int32_t a, int32_t m) {
+    a += a < 0 ? m : 0;
+    return a >= m ? a - m : a;
+}
+
 __device__ __forceinline__ int32_t cell_coord(double p, double cell, int32_t grid, bool periodic) {
     int32_t v = (int32_t)floor(p / cell);
     if (periodic) return floor_mod(v, grid);
@@ -96,7 +102,8 @@ __device__ __forceinline__ int32_t cell_coord(double p, double cell, int32_t gri
 
 __global__ void assign_kernel(int n, const double *__restrict__ x, const double *__restrict__ y,
                               const double *__restrict__ z, const HashParams *__restrict__ hp, int periodic,
-                              int32_t mask, int32_t *__restrict__ cell_hash, int32_t *__restrict__ bucket_count) {
+                              int32_t mask, int32_t *__restrict__ cell_hash, int32_t *__restrict__ bucket_count,
+                              int32_t *__restrict__ cell_xyz) {
     const HashParams p = *hp;
     if (!p.valid) return;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -105,6 +112,11 @@ __global__ void assign_kernel(int n, const double *__restrict__ x, const double 
         const int32_t iz = cell_coord(z[i], p.cell, p.grid, periodic);
         const int32_t h = hash_cell(ix, iy, iz, mask);
         cell_hash[i] = h;
+        if (cell_xyz) {  // [3][n], for the count pass
+            cell_xyz[i] = ix;
+            cell_xyz[n + i] = iy;
+            cell_xyz[2 * (size_t)n + i] = iz;
+        }
         atomicAdd(&bucket_count[h], 1);
     }
 }
@@ -211,10 +223,10 @@ __device__ __forceinline__ void for_each_contact(int i, int ti, const double *__
     // Neighbour cell c = 9 (di + 1) + 3 (dj + 1) + (dk + 1): its bucket, or -1 outside an open box.
     auto cell_hash = [&](int c) -> int32_t {
         int32_t nx = cx + c / 9 - 1, ny = cy + (c / 3) % 3 - 1, nz = cz + c % 3 - 1;
-        if (periodic) {
-            nx = floor_mod(nx, p.grid);
-            ny = floor_mod(ny, p.grid);
-            nz = floor_mod(nz, p.grid);
+        if (periodic) {  // cx, cy, cz lie in [0, grid): one step wraps (= floor_mod)
+            nx = wrap1(nx, p.grid);
+            ny = wrap1(ny, p.grid);
+            nz = wrap1(nz, p.grid);
         } else if (nx < 0 || ny < 0 || nz < 0 || nx >= p.grid || ny >= p.grid || nz >= p.grid) {
             return -1;
         }
@@ -258,15 +270,15 @@ __device__ __forceinline__ void for_each_contact(int i, int ti, const double *__
                     start = ns;
                     end = ne;
                 }
-                return;
-            }
-            for (int c = 0; c < 27; ++c) {
-                const int32_t hc = cell_hash(c);
-                if (hc < 0) continue;
-                const int32_t start = bstart[hc];
-                int32_t end = bstart[hc + 1];
-                if (end > n) end = n;  // :199-201
-                for (int32_t s = start; s < end; ++s) candidate(s, 1);
+            } else {
+                for (int c = 0; c < 27; ++c) {
+                    const int32_t hc = cell_hash(c);
+                    if (hc < 0) continue;
+                    const int32_t start = bstart[hc];
+                    int32_t end = bstart[hc + 1];
+                    if (end > n) end = n;  // :199-201
+                    for (int32_t s = start; s < end; ++s) candidate(s, 1);
+                }
             }
             return;
         }
@@ -346,6 +358,206 @@ __global__ void count_pairs_kernel(int n, const double *__restrict__ x, const do
     if (local_raw) atomicAdd(raw, local_raw);
 }
 
+// Count pass of the context entry point: one warp per occupied bucket.  The
+// droplets of a bucket share their 27 neighbour buckets when they lie in one
+// cell (the usual case), so the warp loads the 27 bucket ranges once, lays
+// their candidates out as one list and tests 32 candidates at a time, each lane
+// against every droplet of the bucket (staged in shared memory): the lanes stay
+// converged and each candidate is read once per bucket, not once per droplet.
+// A bucket holding droplets of several cells (hash aliasing) is taken one cell
+// at a time.  The tests are for_each_contact's (the FP32 far test, then the same
+// FP64 contact test); a cell with a neighbour bucket seen from two of its
+// neighbour cells, and a bucket of more than 32 droplets, take for_each_contact
+// per droplet.  Counts per droplet do not depend on the order.
+constexpr int CB_WARPS = 4;
+constexpr int CB_LIST = 1024;  // candidate slots staged per warp (more: found by search)
+
+__global__ void __launch_bounds__(32 * CB_WARPS)
+    count_pairs_bucket_kernel(int n, int table, const double *__restrict__ x, const double *__restrict__ y,
+                              const double *__restrict__ z, const double *__restrict__ r,
+                              const double2 *__restrict__ P, const float4 *__restrict__ P32,
+                              const HashParams *__restrict__ hp, int periodic, double L, int32_t mask,
+                              const int32_t *__restrict__ bstart, const int32_t *__restrict__ sorted_idx,
+                              const int32_t *__restrict__ cell_xyz, int32_t *__restrict__ pair_count,
+                              unsigned long long *__restrict__ raw) {
+    __shared__ float4 s_q[CB_WARPS][32];                       // FP32 record, radius widened (far test)
+    __shared__ double2 s_a[CB_WARPS][32], s_b[CB_WARPS][32];  // FP64 (x, y), (z, r)
+    __shared__ int s_i[CB_WARPS][32], s_cnt[CB_WARPS][32], s_st[CB_WARPS][32], s_pre[CB_WARPS][32];
+    __shared__ int s_list[CB_WARPS][CB_LIST];  // the cell's candidate slots (when they fit)
+    const HashParams p = *hp;
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    if (!p.valid) {
+        for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) pair_count[t] = 0;
+        return;
+    }
+    const double halfL = 0.5 * L;
+    const float Lf = (float)L;
+    unsigned long long local_raw = 0;
+    const int warps_total = gridDim.x * CB_WARPS;
+    for (long long g = (long long)blockIdx.x * CB_WARPS + wp; g * 32 < table; g += warps_total) {
+        const long long bb = g * 32 + lane;
+        int t0 = 0, m = 0;
+        if (bb < table) {
+            t0 = bstart[bb];
+            m = bstart[bb + 1] - t0;
+        }
+        unsigned occ = __ballot_sync(0xffffffffu, m > 0);
+        while (occ) {
+            const int src = __ffs(occ) - 1;
+            occ &= occ - 1;
+            const int bt0 = __shfl_sync(0xffffffffu, t0, src), bm = __shfl_sync(0xffffffffu, m, src);
+            if (bm > 32) {  // a crowded bucket: per droplet
+                for (int k = lane; k < bm; k += 32) {
+                    const int t = bt0 + k;
+                    const int ii = sorted_idx[t];
+                    int32_t c = 0;
+                    for_each_contact<true>(ii, t, x, y, z, r, P, P32, p, periodic, L, halfL, mask, n, bstart,
+                                           sorted_idx, [&](int32_t, int mult) {
+                                               ++c;
+                                               local_raw += (unsigned long long)mult;
+                                           });
+                    pair_count[ii] = c;
+                }
+                continue;
+            }
+            // the bucket's droplets, one per lane, grouped by cell (a bucket can hold several cells)
+            int i = -1;
+            int32_t cx = 0, cy = 0, cz = 0;
+            double2 a = make_double2(0.0, 0.0), b = a;
+            if (lane < bm) {
+                const int t = bt0 + lane;
+                i = sorted_idx[t];
+                a = P[2 * t];
+                b = P[2 * t + 1];
+                cx = cell_xyz[i];  // cell_coord of the droplet (assign_kernel)
+                cy = cell_xyz[n + i];
+                cz = cell_xyz[2 * (size_t)n + i];
+            }
+            // lanes of the same cell (cell coordinates are >= 0; idle lanes get distinct negative x)
+            const unsigned same_cell = __match_any_sync(0xffffffffu, lane < bm ? cx : -1 - lane) &
+                                       __match_any_sync(0xffffffffu, cy) & __match_any_sync(0xffffffffu, cz);
+            unsigned todo = __ballot_sync(0xffffffffu, lane < bm);
+            while (todo) {
+                const int leader = __ffs(todo) - 1;
+                const unsigned grp = __shfl_sync(0xffffffffu, same_cell, leader);
+                todo &= ~grp;
+                const bool mine = (grp >> lane) & 1u;
+                const int32_t cx0 = __shfl_sync(0xffffffffu, cx, leader), cy0 = __shfl_sync(0xffffffffu, cy, leader),
+                              cz0 = __shfl_sync(0xffffffffu, cz, leader);
+                // neighbour cell c = lane: 9 (di + 1) + 3 (dj + 1) + (dk + 1), as in for_each_contact
+                int32_t h = -1;
+                if (lane < 27) {
+                    int32_t nx = cx0 + lane / 9 - 1, ny = cy0 + (lane / 3) % 3 - 1, nz = cz0 + lane % 3 - 1;
+                    if (periodic) {
+                        h = hash_cell(wrap1(nx, p.grid), wrap1(ny, p.grid), wrap1(nz, p.grid), mask);
+                    } else if (!(nx < 0 || ny < 0 || nz < 0 || nx >= p.grid || ny >= p.grid || nz >= p.grid)) {
+                        h = hash_cell(nx, ny, nz, mask);
+                    }
+                }
+                const unsigned peers = __match_any_sync(0xffffffffu, lane < 27 ? h : -2 - lane);
+                if (__any_sync(0xffffffffu, lane < 27 && h >= 0 && __popc(peers) > 1)) {
+                    // a neighbour bucket seen from two cells: per droplet, with multiplicities
+                    if (mine) {
+                        const int t = bt0 + lane;
+                        int32_t c = 0;
+                        for_each_contact<true>(i, t, x, y, z, r, P, P32, p, periodic, L, halfL, mask, n, bstart,
+                                               sorted_idx, [&](int32_t, int mult) {
+                                                   ++c;
+                                                   local_raw += (unsigned long long)mult;
+                                               });
+                        pair_count[i] = c;
+                    }
+                    continue;
+                }
+                int st = 0, len = 0;
+                if (h >= 0) {
+                    st = bstart[h];
+                    int e = bstart[h + 1];
+                    if (e > n) e = n;  // :199-201
+                    len = e > st ? e - st : 0;
+                }
+                int inc = len;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int v = __shfl_up_sync(0xffffffffu, inc, o);
+                    if (lane >= o) inc += v;
+                }
+                const int total = __shfl_sync(0xffffffffu, inc, 31);
+                const int gm = __popc(grp);
+                s_st[wp][lane] = st;
+                s_pre[wp][lane] = inc - len;
+                const bool listed = total <= CB_LIST;
+                if (listed)
+                    for (int e = 0; e < len; ++e) s_list[wp][inc - len + e] = st + e;
+                if (mine) {  // the group's droplets at slots 0 .. gm - 1
+                    const int slot = __popc(grp & ((1u << lane) - 1u));
+                    const float marg = (float)(0x1p-17 * (fmax(fabs(a.x), fmax(fabs(a.y), fabs(b.x))) + fabs(L)));
+                    float4 q = P32[bt0 + lane];
+                    q.w = q.w * (1.f + 0x1p-18f) + marg;  // as for_each_contact's qi
+                    if (!(marg >= 0x1p-100f)) q.w = INFINITY;
+                    s_q[wp][slot] = q;
+                    s_a[wp][slot] = a;
+                    s_b[wp][slot] = b;
+                    s_i[wp][slot] = i;
+                    s_cnt[wp][slot] = 0;
+                }
+                __syncwarp();
+                const int *wi = s_i[wp];
+                const float4 *wq = s_q[wp];
+                for (int t = lane; t - lane < total; t += 32) {  // every lane takes the same number of rounds
+                    if (t >= total) continue;
+                    int sl;
+                    if (listed) {
+                        sl = s_list[wp][t];
+                    } else {  // the neighbour bucket holding list entry t: the last c with s_pre[c] <= t
+                        int lo = 0, hi = 26;
+                        while (lo < hi) {
+                            const int mid = (lo + hi + 1) >> 1;
+                            if (s_pre[wp][mid] <= t)
+                                lo = mid;
+                            else
+                                hi = mid - 1;
+                        }
+                        sl = s_st[wp][lo] + (t - s_pre[wp][lo]);
+                    }
+                    const int32_t j = sorted_idx[sl];
+                    const float4 q = P32[sl];
+                    const float qw = q.w * (1.f + 0x1p-18f);
+#pragma unroll 4
+                    for (int k = 0; k < gm; ++k) {
+                        const float4 qi = wq[k];
+                        float ax = fabsf(q.x - qi.x), ay = fabsf(q.y - qi.y), az = fabsf(q.z - qi.z);
+                        if (periodic) {
+                            ax = fminf(ax, fabsf(ax - Lf));
+                            ay = fminf(ay, fabsf(ay - Lf));
+                            az = fminf(az, fabsf(az - Lf));
+                        }
+                        const float sf = qw + qi.w;
+                        // i < j, and not clearly apart: the exact test (rare)
+                        if (!(wi[k] < j) || fmaf(ax, ax, fmaf(ay, ay, az * az)) > sf * sf) continue;
+                        const double2 ca = P[2 * sl], cb = P[2 * sl + 1];
+                        const double2 ka = s_a[wp][k], kb = s_b[wp][k];
+                        double dx = ca.x - ka.x, dy = ca.y - ka.y, dz = cb.x - kb.x;
+                        if (periodic) {
+                            dx = mic64(dx, L, halfL);
+                            dy = mic64(dy, L, halfL);
+                            dz = mic64(dz, L, halfL);
+                        }
+                        if (contact_rn(dx * dx + dy * dy + dz * dz, kb.y + cb.y)) {  // dist <= r_i + r_j
+                            atomicAdd(&s_cnt[wp][k], 1);
+                            ++local_raw;
+                        }
+                    }
+                }
+                __syncwarp();
+                if (lane < gm) pair_count[s_i[wp][lane]] = s_cnt[wp][lane];
+                __syncwarp();  // shared memory is rewritten by the next group
+            }
+        }
+    }
+    if (local_raw) atomicAdd(raw, local_raw);
+}
+
 template <bool PACKED>
 __global__ void write_pairs_kernel(int n, const double *__restrict__ x, const double *__restrict__ y,
                                    const double *__restrict__ z, const double *__restrict__ r,
@@ -420,7 +632,8 @@ int launch_hash_detect(dem_ctx *ctx, int n, const double *x, const double *y, co
     dem_prof_begin(ctx, "hash_detect", s);
     max_kernel<<<grid, 256, 0, counted(s)>>>(n, r, slot);
     hash_params_kernel<<<1, 1, 0, counted(s)>>>(slot, L, even_cells, hp);
-    assign_kernel<<<grid, 256, 0, counted(s)>>>(n, x, y, z, hp, periodic, mask, ctx->cell_hash, ctx->bucket_count);
+    assign_kernel<<<grid, 256, 0, counted(s)>>>(n, x, y, z, hp, periodic, mask, ctx->cell_hash, ctx->bucket_count,
+                                                ctx->cell_xyz);
     rc = dem_check_launch(ctx, "hash assign");
     if (rc) return rc;
     rc = exclusive_scan<int32_t, int32_t>(ctx, ctx->bucket_count, ctx->bucket_start, table_size, s);
@@ -433,10 +646,10 @@ int launch_hash_detect(dem_ctx *ctx, int n, const double *x, const double *y, co
     bucket_positions_kernel<<<grid, 256, 0, counted(s)>>>(n, x, y, z, r, hp, ctx->sorted_idx, ctx->hash_pos,
                                                           ctx->hash_pos32);
     const int dgrid = ceil_div(n, 128);
-    count_pairs_kernel<true><<<dgrid, 128, 0, counted(s)>>>(n, x, y, z, r, ctx->hash_pos, ctx->hash_pos32, hp,
-                                                            periodic, L, mask,
-                                                            ctx->bucket_start, ctx->sorted_idx, ctx->pair_count,
-                                                            reinterpret_cast<unsigned long long *>(counts + 1));
+    const int cgrid = max(1, min(ceil_div(table_size, 32 * CB_WARPS), 32 * ctx->sm_count));
+    count_pairs_bucket_kernel<<<cgrid, 32 * CB_WARPS, 0, counted(s)>>>(
+        n, table_size, x, y, z, r, ctx->hash_pos, ctx->hash_pos32, hp, periodic, L, mask, ctx->bucket_start,
+        ctx->sorted_idx, ctx->cell_xyz, ctx->pair_count, reinterpret_cast<unsigned long long *>(counts + 1));
     rc = dem_check_launch(ctx, "hash count");
     if (rc) return rc;
     rc = exclusive_scan<int32_t, int64_t>(ctx, ctx->pair_count, ctx->pair_offset, n, s);
@@ -550,7 +763,7 @@ extern "C" int dem_hash_detect_noalloc(int n, const double *x, const double *y, 
     if (n == 0) return DEM_OK;
     max_kernel<<<grid, 256, 0, counted(s)>>>(n, r, slot);
     hash_params_kernel<<<1, 1, 0, counted(s)>>>(slot, L, 0, hp);
-    assign_kernel<<<grid, 256, 0, counted(s)>>>(n, x, y, z, hp, periodic, mask, cell_hash, bucket_count);
+    assign_kernel<<<grid, 256, 0, counted(s)>>>(n, x, y, z, hp, periodic, mask, cell_hash, bucket_count, nullptr);
     if (cudaGetLastError() != cudaSuccess) return DEM_E_CUDA;
     if (exclusive_scan_into<int32_t, int32_t>(bucket_count, bucket_start, table_size, static_cast<int32_t *>(sums),
                                               s) != cudaSuccess)
