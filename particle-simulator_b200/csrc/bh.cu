@@ -19,7 +19,9 @@
 //           octree_node.py:98-114), side = root side / 2^level, and the
 //           R^3-weighted second moment Q of the node about that centre; after the force
 //           walk, sum F and the dipole D = sum (x - c) F^T (= P - c F^T of
-//           flat_tree.py:556-777).
+//           flat_tree.py:556-777).  Both bottom up, one level per launch: a leaf
+//           sums its droplets, an inner node its children's FP64 sums moved to
+//           its own reference point (first droplet, resp. centre).
 //   walks   one warp per 64 consecutive sorted targets, two per lane, their
 //           terms evaluated in packed FP32x2 (bh_walk2_kernel; with the
 //           periodic-image correction, one target per lane: bh_walk_kernel); the
@@ -76,6 +78,7 @@ constexpr int BH_SKIP_VEL = 0x200;
 struct BhNodes {
     int *start, *count, *first_child, *nchild, *level;
     double *cx, *cy, *cz;  // R^3-weighted centre
+    double *mom;           // [22][M] FP64 moment sums of the bottom-up pass (node_r3_up / node_force_up)
     float4 *cs;            // walk copy: centre relative to the root cube origin / ell, and side / ell
     int4 *meta;            // walk copy: count, nchild, first child (a leaf: first droplet), level | skip flags
     // walk records, one 16-byte-aligned group per node so that a visit issues vector loads:
@@ -110,7 +113,6 @@ struct dem_bh {
     int32_t *scan_in = nullptr, *coff = nullptr;  // [max_nodes + 1] children per node of a level, offsets
     BhNodes nd{};
     std::vector<int> level_off;
-    double *top_part = nullptr;  // [TOP_PARTIALS][12] chunk partials of the top levels' moments
     const dem_corr *corr = nullptr;  // periodic-image correction of the velocity walk (borrowed), or none
 };
 
@@ -374,7 +376,7 @@ __global__ void level_write_kernel(BhNodes nd, int ls, int le, const int32_t *__
 __device__ void r3_finish(BhNodes nd, int k, const double *v, double rx, double ry, double rz, int s0, int c, double ox,
                           double oy, double oz, double box, const uint32_t *__restrict__ keys) {
     {
-        {  // (kept as one block: the body of node_r3_kernel's final step)
+        {
             const double w = v[0];
             float Q[6];
             if (w > 0.0) {
@@ -404,235 +406,106 @@ __device__ void r3_finish(BhNodes nd, int k, const double *v, double rx, double 
     }
 }
 
-// R^3 and R^3-weighted centre of nodes [a, b), one CTA (big nodes) or one warp per node
-template <bool BLOCK>
-__global__ void node_r3_kernel(BhNodes nd, int a, int b, const double *__restrict__ ps, int cap,
-                               const double *__restrict__ geom, const uint32_t *__restrict__ keys) {
+// Node moments bottom up, one level per launch (deepest first), one thread per node; every node
+// keeps its FP64 sums in nd.mom ([22][M]: 10 R^3 sums, then 12 force sums), so each droplet is
+// read once, by its leaf, and an inner node combines at most 8 children.
+//
+// R^3 sums relative to the node's first droplet r (as r3_finish expects): a leaf sums its droplets,
+// w = r_j^3, S1 = sum w (x - r), S2 = sum w (x - r)(x - r)^T; an inner node adds its children's
+// sums moved from the child's first droplet r_c to its own (its first child's): with delta = r_c - r,
+//   W += W_c,  S1 += S1_c + W_c delta,  S2 += S2_c + S1_c delta^T + delta S1_c^T + W_c delta delta^T.
+__global__ void node_r3_up_kernel(BhNodes nd, int a, int b, int M, const double *__restrict__ ps, int cap,
+                                  const double *__restrict__ geom, const uint32_t *__restrict__ keys) {
     const double ox = geom[0], oy = geom[1], oz = geom[2], box = geom[3];
-    const int per = BLOCK ? 1 : blockDim.x / 32;
-    const int lane = BLOCK ? threadIdx.x : (threadIdx.x & 31);
-    const int stride = BLOCK ? blockDim.x : 32;
-    __shared__ double red[10][32];
-    for (int k = a + blockIdx.x * per + (BLOCK ? 0 : (int)(threadIdx.x >> 5)); k < b; k += gridDim.x * per) {
-        const int s0 = nd.start[k], c = nd.count[k];
-        // sums relative to the node's first droplet (keeps the second moment free of cancellation)
+    for (int k = a + blockIdx.x * blockDim.x + threadIdx.x; k < b; k += gridDim.x * blockDim.x) {
+        const int s0 = nd.start[k], c = nd.count[k], nch = nd.nchild[k];
         const double rx = c > 0 ? ps[s0] : 0.0, ry = c > 0 ? ps[cap + s0] : 0.0,
                      rz = c > 0 ? ps[2 * (size_t)cap + s0] : 0.0;
         double v[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};  // w, w d (3), w d d^T (6)
-        for (int t = lane; t < c; t += stride) {
-            const double r = ps[3 * (size_t)cap + s0 + t];
-            const double w = r * r * r;
-            const double dx = ps[s0 + t] - rx, dy = ps[cap + s0 + t] - ry, dz = ps[2 * (size_t)cap + s0 + t] - rz;
-            v[0] += w;
-            v[1] += w * dx;
-            v[2] += w * dy;
-            v[3] += w * dz;
-            v[4] += w * dx * dx;
-            v[5] += w * dx * dy;
-            v[6] += w * dx * dz;
-            v[7] += w * dy * dy;
-            v[8] += w * dy * dz;
-            v[9] += w * dz * dz;
+        if (nch == 0) {
+            for (int t = 0; t < c; ++t) {
+                const double r = ps[3 * (size_t)cap + s0 + t];
+                const double w = r * r * r;
+                const double dx = ps[s0 + t] - rx, dy = ps[cap + s0 + t] - ry, dz = ps[2 * (size_t)cap + s0 + t] - rz;
+                v[0] += w;
+                v[1] += w * dx;
+                v[2] += w * dy;
+                v[3] += w * dz;
+                v[4] += w * dx * dx;
+                v[5] += w * dx * dy;
+                v[6] += w * dx * dz;
+                v[7] += w * dy * dy;
+                v[8] += w * dy * dz;
+                v[9] += w * dz * dz;
+            }
+        } else {
+            const int f = nd.first_child[k];
+            for (int q = 0; q < nch; ++q) {
+                const int ch = f + q, cs0 = nd.start[ch];
+                const double dx = ps[cs0] - rx, dy = ps[cap + cs0] - ry, dz = ps[2 * (size_t)cap + cs0] - rz;
+                double u[10];
+#pragma unroll
+                for (int p = 0; p < 10; ++p) u[p] = nd.mom[(size_t)p * M + ch];
+                v[0] += u[0];
+                v[1] += u[1] + u[0] * dx;
+                v[2] += u[2] + u[0] * dy;
+                v[3] += u[3] + u[0] * dz;
+                v[4] += u[4] + 2.0 * u[1] * dx + u[0] * dx * dx;
+                v[5] += u[5] + u[1] * dy + dx * u[2] + u[0] * dx * dy;
+                v[6] += u[6] + u[1] * dz + dx * u[3] + u[0] * dx * dz;
+                v[7] += u[7] + 2.0 * u[2] * dy + u[0] * dy * dy;
+                v[8] += u[8] + u[2] * dz + dy * u[3] + u[0] * dy * dz;
+                v[9] += u[9] + 2.0 * u[3] * dz + u[0] * dz * dz;
+            }
         }
-        for (int q = 0; q < 10; ++q)
-            for (int o = 16; o; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
-        if (BLOCK) {
-            const int wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-            if ((threadIdx.x & 31) == 0)
-                for (int q = 0; q < 10; ++q) red[q][wp] = v[q];
-            __syncthreads();
-            if (threadIdx.x == 0)
-                for (int q = 0; q < 10; ++q) {
-                    v[q] = 0;
-                    for (int u = 0; u < nw; ++u) v[q] += red[q][u];
-                }
-            __syncthreads();
-        }
-        if (lane == 0) r3_finish(nd, k, v, rx, ry, rz, s0, c, ox, oy, oz, box, keys);
+#pragma unroll
+        for (int p = 0; p < 10; ++p) nd.mom[(size_t)p * M + k] = v[p];
+        r3_finish(nd, k, v, rx, ry, rz, s0, c, ox, oy, oz, box, keys);
     }
 }
 
-// ---------------------------------------------------------------------------
-// The top three levels (the root, its children and grandchildren) cover every
-// droplet once per level, in a few huge nodes: one CTA per node would leave the
-// root's 2^20 droplets to one SM.  Their moments are summed in chunks instead,
-// TOP_CHUNKS >> (3 level) CTAs per node, each writing one partial, and a second
-// kernel adds a node's partials in chunk order (deterministic).  The sums are
-// the same as node_r3_kernel's / node_force_kernel's (relative to the node's
-// first droplet / to its centre), in another order.
-// ---------------------------------------------------------------------------
-constexpr int TOP_LEVELS = 3;
-constexpr int TOP_CHUNKS = 512;  // chunks of the root; a level-l node gets TOP_CHUNKS >> (3 l)
-constexpr int TOP_T = 256;
-constexpr int TOP_PARTIALS = 3 * TOP_CHUNKS;  // each full level of the top three holds TOP_CHUNKS chunks in all
-
-struct TopPlan {
-    int levels;
-    int node0[TOP_LEVELS], nodes[TOP_LEVELS], chunks[TOP_LEVELS];
-    int cta0[TOP_LEVELS + 1];  // first CTA (partial) of each level; cta0[levels] = total
-};
-
-__device__ __forceinline__ void top_locate(const TopPlan &tp, int q, int &node, int &chunk, int &nchunk) {
-    int l = 0;
-    while (l + 1 < tp.levels && q >= tp.cta0[l + 1]) ++l;
-    const int local = q - tp.cta0[l];
-    nchunk = tp.chunks[l];
-    node = tp.node0[l] + local / nchunk;
-    chunk = local % nchunk;
-}
-
-template <int NV>
-__device__ __forceinline__ void block_sum(double (&v)[NV], double (*red)[TOP_T / 32]) {
-    for (int q = 0; q < NV; ++q)
-        for (int o = 16; o; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
-    const int wp = threadIdx.x >> 5;
-    if ((threadIdx.x & 31) == 0)
-        for (int q = 0; q < NV; ++q) red[q][wp] = v[q];
-    __syncthreads();
-    if (threadIdx.x == 0)
-        for (int q = 0; q < NV; ++q) {
-            v[q] = 0;
-            for (int u = 0; u < TOP_T / 32; ++u) v[q] += red[q][u];
-        }
-}
-
-__global__ void __launch_bounds__(TOP_T) top_r3_partial_kernel(BhNodes nd, TopPlan tp, const double *__restrict__ ps,
-                                                               int cap, double *__restrict__ part) {
-    __shared__ double red[10][TOP_T / 32];
-    int k, c, nc;
-    top_locate(tp, blockIdx.x, k, c, nc);
-    const int s0 = nd.start[k], cnt = nd.count[k];
-    const double rx = cnt > 0 ? ps[s0] : 0.0, ry = cnt > 0 ? ps[cap + s0] : 0.0,
-                 rz = cnt > 0 ? ps[2 * (size_t)cap + s0] : 0.0;
-    const int t0 = (int)((long long)cnt * c / nc), t1 = (int)((long long)cnt * (c + 1) / nc);
-    double v[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (int t = t0 + threadIdx.x; t < t1; t += TOP_T) {
-        const double r = ps[3 * (size_t)cap + s0 + t];
-        const double w = r * r * r;
-        const double dx = ps[s0 + t] - rx, dy = ps[cap + s0 + t] - ry, dz = ps[2 * (size_t)cap + s0 + t] - rz;
-        v[0] += w;
-        v[1] += w * dx;
-        v[2] += w * dy;
-        v[3] += w * dz;
-        v[4] += w * dx * dx;
-        v[5] += w * dx * dy;
-        v[6] += w * dx * dz;
-        v[7] += w * dy * dy;
-        v[8] += w * dy * dz;
-        v[9] += w * dz * dz;
-    }
-    block_sum<10>(v, red);
-    if (threadIdx.x == 0)
-        for (int q = 0; q < 10; ++q) part[(size_t)blockIdx.x * 12 + q] = v[q];
-}
-
-__global__ void top_force_partial_kernel(BhNodes nd, TopPlan tp, const double *__restrict__ ps,
-                                         const double *__restrict__ fsort, int cap, double *__restrict__ part) {
-    __shared__ double red[12][TOP_T / 32];
-    int k, c, nc;
-    top_locate(tp, blockIdx.x, k, c, nc);
-    const int s0 = nd.start[k], cnt = nd.count[k];
-    const double cx = nd.cx[k], cy = nd.cy[k], cz = nd.cz[k];
-    const int t0 = (int)((long long)cnt * c / nc), t1 = (int)((long long)cnt * (c + 1) / nc);
-    double v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (int t = t0 + threadIdx.x; t < t1; t += TOP_T) {
-        const int si = s0 + t;
-        const double F[3] = {fsort[si], fsort[cap + si], fsort[2 * (size_t)cap + si]};
-        const double d[3] = {ps[si] - cx, ps[cap + si] - cy, ps[2 * (size_t)cap + si] - cz};
-        for (int q = 0; q < 3; ++q) v[q] += F[q];
-        for (int pp = 0; pp < 3; ++pp)
-            for (int q = 0; q < 3; ++q) v[3 + 3 * pp + q] += d[pp] * F[q];
-    }
-    block_sum<12>(v, red);
-    if (threadIdx.x == 0)
-        for (int q = 0; q < 12; ++q) part[(size_t)blockIdx.x * 12 + q] = v[q];
-}
-
-// One warp per top node: lane l adds chunks l, l + 32, ... in order, then the lanes' sums are added by a
-// fixed shuffle tree (deterministic), then node_r3_kernel's final step.
-template <int NV>
-__device__ __forceinline__ void top_partials(const TopPlan &tp, int k, const double *__restrict__ part, double (&v)[NV]) {
-    const int lane = threadIdx.x & 31;
-    int l = 0;
-    while (l + 1 < tp.levels && k >= tp.node0[l + 1]) ++l;
-    const int nc = tp.chunks[l];
-    const size_t q0 = (size_t)tp.cta0[l] + (size_t)(k - tp.node0[l]) * nc;
-    for (int q = 0; q < NV; ++q) v[q] = 0.0;
-    for (int c = lane; c < nc; c += 32)
-        for (int q = 0; q < NV; ++q) v[q] += part[(q0 + c) * 12 + q];
-    for (int q = 0; q < NV; ++q)
-        for (int o = 16; o; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
-}
-
-__global__ void top_r3_finish_kernel(BhNodes nd, TopPlan tp, const double *__restrict__ part,
-                                     const double *__restrict__ ps, int cap, const double *__restrict__ geom,
-                                     const uint32_t *__restrict__ keys) {
-    const int total = tp.node0[tp.levels - 1] + tp.nodes[tp.levels - 1] - tp.node0[0];
-    const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (t >= total) return;  // warp-uniform
-    const int k = tp.node0[0] + t;
-    double v[10];
-    top_partials<10>(tp, k, part, v);
-    if ((threadIdx.x & 31) != 0) return;
-    const int s0 = nd.start[k], cnt = nd.count[k];
-    const double rx = cnt > 0 ? ps[s0] : 0.0, ry = cnt > 0 ? ps[cap + s0] : 0.0,
-                 rz = cnt > 0 ? ps[2 * (size_t)cap + s0] : 0.0;
-    r3_finish(nd, k, v, rx, ry, rz, s0, cnt, geom[0], geom[1], geom[2], geom[3], keys);
-}
-
-// One warp per top node: force sum and dipole from its chunk partials (see top_partials).
-__global__ void top_force_finish_kernel(BhNodes nd, TopPlan tp, const double *__restrict__ part) {
-    const int total = tp.node0[tp.levels - 1] + tp.nodes[tp.levels - 1] - tp.node0[0];
-    const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (t >= total) return;  // warp-uniform
-    const int k = tp.node0[0] + t;
-    double v[12];
-    top_partials<12>(tp, k, part, v);
-    if ((threadIdx.x & 31) != 0) return;
-    for (int q = 0; q < 3; ++q)  // v = (F, D row-major): the record's order
-        nd.fd[3 * (size_t)k + q] = make_float4((float)v[4 * q], (float)v[4 * q + 1], (float)v[4 * q + 2],
-                                               (float)v[4 * q + 3]);
-}
-
-// sum F and dipole D = sum (x - c) F^T of nodes [a, b)
-template <bool BLOCK>
-__global__ void node_force_kernel(BhNodes nd, int a, int b, const double *__restrict__ ps,
-                                  const double *__restrict__ fsort, int cap) {
-    const int per = BLOCK ? 1 : blockDim.x / 32;
-    const int lane = BLOCK ? threadIdx.x : (threadIdx.x & 31);
-    const int stride = BLOCK ? blockDim.x : 32;
-    __shared__ double red[12][32];
-    for (int k = a + blockIdx.x * per + (BLOCK ? 0 : (int)(threadIdx.x >> 5)); k < b; k += gridDim.x * per) {
-        const int s0 = nd.start[k], c = nd.count[k];
+// Force sum F and dipole D = sum (x - c) F^T about the node's centre c: a leaf sums its droplets; an
+// inner node adds its children's, moved to its centre: F += F_c, D += D_c + (c_c - c) F_c^T.
+__global__ void node_force_up_kernel(BhNodes nd, int a, int b, int M, const double *__restrict__ ps,
+                                     const double *__restrict__ fsort, int cap) {
+    double *fm = nd.mom + (size_t)10 * M;
+    for (int k = a + blockIdx.x * blockDim.x + threadIdx.x; k < b; k += gridDim.x * blockDim.x) {
+        const int s0 = nd.start[k], c = nd.count[k], nch = nd.nchild[k];
         const double cx = nd.cx[k], cy = nd.cy[k], cz = nd.cz[k];
-        double v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-        for (int t = lane; t < c; t += stride) {
-            const int s = s0 + t;
-            const double F[3] = {fsort[s], fsort[cap + s], fsort[2 * (size_t)cap + s]};
-            const double d[3] = {ps[s] - cx, ps[cap + s] - cy, ps[2 * (size_t)cap + s] - cz};
-            for (int q = 0; q < 3; ++q) v[q] += F[q];
-            for (int p = 0; p < 3; ++p)
-                for (int q = 0; q < 3; ++q) v[3 + 3 * p + q] += d[p] * F[q];
+        double v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};  // F (3), D row-major (9)
+        if (nch == 0) {
+            for (int t = 0; t < c; ++t) {
+                const int sj = s0 + t;
+                const double F[3] = {fsort[sj], fsort[cap + sj], fsort[2 * (size_t)cap + sj]};
+                const double d[3] = {ps[sj] - cx, ps[cap + sj] - cy, ps[2 * (size_t)cap + sj] - cz};
+#pragma unroll
+                for (int q = 0; q < 3; ++q) v[q] += F[q];
+#pragma unroll
+                for (int p = 0; p < 3; ++p)
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) v[3 + 3 * p + q] += d[p] * F[q];
+            }
+        } else {
+            const int f = nd.first_child[k];
+            for (int q0 = 0; q0 < nch; ++q0) {
+                const int ch = f + q0;
+                const double d[3] = {nd.cx[ch] - cx, nd.cy[ch] - cy, nd.cz[ch] - cz};
+                double u[12];
+#pragma unroll
+                for (int p = 0; p < 12; ++p) u[p] = fm[(size_t)p * M + ch];
+#pragma unroll
+                for (int q = 0; q < 3; ++q) v[q] += u[q];
+#pragma unroll
+                for (int p = 0; p < 3; ++p)
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) v[3 + 3 * p + q] += u[3 + 3 * p + q] + d[p] * u[q];
+            }
         }
-        for (int q = 0; q < 12; ++q)
-            for (int o = 16; o; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
-        if (BLOCK) {
-            const int wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-            if ((threadIdx.x & 31) == 0)
-                for (int q = 0; q < 12; ++q) red[q][wp] = v[q];
-            __syncthreads();
-            if (threadIdx.x == 0)
-                for (int q = 0; q < 12; ++q) {
-                    v[q] = 0;
-                    for (int u = 0; u < nw; ++u) v[q] += red[q][u];
-                }
-            __syncthreads();
-        }
-        if (lane == 0) {  // node-major: one node's aggregates are contiguous for the walk
-            for (int q = 0; q < 3; ++q)  // v = (F, D row-major): the record's order
-                nd.fd[3 * (size_t)k + q] = make_float4((float)v[4 * q], (float)v[4 * q + 1], (float)v[4 * q + 2],
-                                                       (float)v[4 * q + 3]);
-        }
+#pragma unroll
+        for (int p = 0; p < 12; ++p) fm[(size_t)p * M + k] = v[p];
+        for (int q = 0; q < 3; ++q)  // v = (F, D row-major): the record's order
+            nd.fd[3 * (size_t)k + q] = make_float4((float)v[4 * q], (float)v[4 * q + 1], (float)v[4 * q + 2],
+                                                   (float)v[4 * q + 3]);
     }
 }
 
@@ -1338,8 +1211,8 @@ static int bh_alloc(dem_ctx *ctx, T **p, size_t count, const char *what) {
 }
 
 static void bh_free_nodes(BhNodes &nd) {
-    void *ptrs[] = {nd.start, nd.count, nd.first_child, nd.nchild, nd.level, nd.cx,
-                    nd.cy,    nd.cz,    nd.cs,          nd.meta,   nd.qr, nd.fd};
+    void *ptrs[] = {nd.start, nd.count, nd.first_child, nd.nchild, nd.level, nd.cx, nd.cy,
+                    nd.cz,    nd.mom,   nd.cs,          nd.meta,   nd.qr,    nd.fd};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     nd = BhNodes{};
@@ -1356,6 +1229,7 @@ static int bh_nodes_reserve(dem_bh *b, int m, int keep, cudaStream_t s) {
         (rc = bh_alloc(ctx, &nn.level, m, "bh nodes")) || (rc = bh_alloc(ctx, &nn.cx, m, "bh nodes")) ||
         (rc = bh_alloc(ctx, &nn.cy, m, "bh nodes")) || (rc = bh_alloc(ctx, &nn.cz, m, "bh nodes")) ||
         (rc = bh_alloc(ctx, &nn.cs, m, "bh nodes")) || (rc = bh_alloc(ctx, &nn.meta, m, "bh nodes")) ||
+        (rc = bh_alloc(ctx, &nn.mom, 22 * (size_t)m, "bh nodes")) ||
         (rc = bh_alloc(ctx, &nn.qr, 2 * (size_t)m, "bh nodes")) ||
         (rc = bh_alloc(ctx, &nn.fd, 3 * (size_t)m, "bh nodes"))) {
         bh_free_nodes(nn);
@@ -1385,7 +1259,7 @@ static int bh_nodes_reserve(dem_bh *b, int m, int keep, cudaStream_t s) {
 static void bh_free(dem_bh *b) {
     cudaSetDevice(b->ctx->device);
     bh_free_nodes(b->nd);
-    void *ptrs[] = {b->top_part, b->keys[0], b->keys[1], b->idx[0],   b->idx[1], b->hist,    b->ps,  b->fsort, b->loff, b->fs32,
+    void *ptrs[] = {b->keys[0], b->keys[1], b->idx[0],   b->idx[1], b->hist,    b->ps,  b->fsort, b->loff, b->fs32,
                     b->bounds,  b->bbox,    b->geom,     b->counters, b->scales, b->scan_in, b->coff};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -1399,19 +1273,8 @@ static inline int grid_of(dem_ctx *ctx, long long work, int threads = 256) {
     return (int)g;
 }
 
-// The chunked sums of the top levels (levels 0 .. min(3, nlevels) - 1).
-static TopPlan top_plan(const dem_bh *b) {
-    TopPlan tp{};
-    tp.levels = std::min(TOP_LEVELS, b->nlevels);
-    tp.cta0[0] = 0;
-    for (int l = 0; l < tp.levels; ++l) {
-        tp.node0[l] = b->level_off[l];
-        tp.nodes[l] = (l + 1 < b->nlevels ? b->level_off[l + 1] : b->node_count) - b->level_off[l];
-        tp.chunks[l] = TOP_CHUNKS >> (3 * l);
-        tp.cta0[l + 1] = tp.cta0[l] + tp.nodes[l] * tp.chunks[l];
-    }
-    return tp;
-}
+// One past the last node of level l.
+static int level_end(const dem_bh *b, int l) { return l + 1 < b->nlevels ? b->level_off[l + 1] : b->node_count; }
 
 extern "C" {
 
@@ -1432,7 +1295,6 @@ int dem_bh_create(dem_ctx *ctx, int capacity, dem_bh **out) {
         (rc = bh_alloc(ctx, &b->loff, n, "bh")) || (rc = bh_alloc(ctx, &b->fs32, n, "bh")) ||
         (rc = bh_alloc(ctx, &b->bbox, 6, "bh")) || (rc = bh_alloc(ctx, &b->geom, 4, "bh")) ||
         (rc = bh_alloc(ctx, &b->counters, 2, "bh")) || (rc = bh_alloc(ctx, &b->scales, 2, "bh")) ||
-        (rc = bh_alloc(ctx, &b->top_part, (size_t)TOP_PARTIALS * 12, "bh")) ||
         (rc = bh_nodes_reserve(b, std::max(4096, capacity / 4), 0, nullptr))) {
         bh_free(b);
         return rc;
@@ -1517,16 +1379,12 @@ int dem_bh_build(dem_bh *b, int n, const double *x, const double *y, const doubl
     }
     b->node_count = le;
     b->nlevels = (int)b->level_off.size();
-    // node R^3 and centres: chunked sums on the top three levels, one warp per node below
-    const TopPlan tp = top_plan(b);
-    const int top = tp.node0[tp.levels - 1] + tp.nodes[tp.levels - 1];
-    top_r3_partial_kernel<<<tp.cta0[tp.levels], TOP_T, 0, counted(s)>>>(b->nd, tp, b->ps, b->capacity, b->top_part);
-    top_r3_finish_kernel<<<(top + 3) / 4, 128, 0, counted(s)>>>(b->nd, tp, b->top_part, b->ps, b->capacity,
-                                                                b->geom, b->keys[0]);
-    if (le > top)
-        node_r3_kernel<false><<<grid_of(ctx, 32LL * (le - top)), 256, 0, counted(s)>>>(b->nd, top, le, b->ps,
-                                                                                       b->capacity, b->geom,
-                                                                                       b->keys[0]);
+    // node R^3 and centres, bottom up (the deepest level first)
+    for (int l = b->nlevels - 1; l >= 0; --l) {
+        const int a = b->level_off[l], e = level_end(b, l);
+        node_r3_up_kernel<<<grid_of(ctx, e - a), 256, 0, counted(s)>>>(b->nd, a, e, b->max_nodes, b->ps,
+                                                                       b->capacity, b->geom, b->keys[0]);
+    }
     scale_nodes_kernel<<<grid_of(ctx, le), 256, 0, counted(s)>>>(b->nd, le, b->scales, b->geom, 0);
     leaf_offsets_kernel<<<grid_of(ctx, le), 256, 0, counted(s)>>>(b->nd, le, b->ps, b->capacity, b->scales,
                                                                    b->loff);
@@ -1601,14 +1459,11 @@ int dem_bh_velocity(dem_bh *b, const double *fx, const double *fy, const double 
         return rc;
     maxabs_kernel<<<grid_of(ctx, n), 256, 0, counted(s)>>>(n, fs, fs + b->capacity, fs + 2 * (size_t)b->capacity,
                                                            b->scales + 1);
-    const TopPlan tp = top_plan(b);
-    const int top = tp.node0[tp.levels - 1] + tp.nodes[tp.levels - 1];
-    top_force_partial_kernel<<<tp.cta0[tp.levels], TOP_T, 0, counted(s)>>>(b->nd, tp, b->ps, b->fsort, b->capacity,
-                                                                            b->top_part);
-    top_force_finish_kernel<<<(top + 3) / 4, 128, 0, counted(s)>>>(b->nd, tp, b->top_part);
-    if (le > top)
-        node_force_kernel<false><<<grid_of(ctx, 32LL * (le - top)), 256, 0, counted(s)>>>(b->nd, top, le, b->ps,
-                                                                                          b->fsort, b->capacity);
+    for (int l = b->nlevels - 1; l >= 0; --l) {  // force sums and dipoles, bottom up
+        const int a = b->level_off[l], e = level_end(b, l);
+        node_force_up_kernel<<<grid_of(ctx, e - a), 256, 0, counted(s)>>>(b->nd, a, e, b->max_nodes, b->ps,
+                                                                          b->fsort, b->capacity);
+    }
     scale_nodes_kernel<<<grid_of(ctx, le), 256, 0, counted(s)>>>(b->nd, le, b->scales, b->geom, 1);
     scale_forces_kernel<<<grid_of(ctx, n), 256, 0, counted(s)>>>(n, b->capacity, b->fsort, b->scales, b->fs32);
     if ((rc = dem_check_cuda(ctx, cudaMemsetAsync(b->counters, 0, 2 * sizeof(unsigned long long), s), "memset")))
