@@ -370,9 +370,12 @@ __global__ void count_pairs_kernel(int n, const double *__restrict__ x, const do
 // neighbour cells, and a bucket of more than 32 droplets, take for_each_contact
 // per droplet.  Counts per droplet do not depend on the order.
 constexpr int CB_WARPS = 4;
-constexpr int CB_LIST = 1024;  // candidate slots staged per warp (more: found by search)
+constexpr int CB_LIST = 256;  // candidate slots staged per warp (more: found by search)
+#ifndef CB_MIN_CTAS
+#define CB_MIN_CTAS 8  // resident CTAs per SM the count pass is compiled for (latency-bound: more warps)
+#endif
 
-__global__ void __launch_bounds__(32 * CB_WARPS)
+__global__ void __launch_bounds__(32 * CB_WARPS, CB_MIN_CTAS)
     count_pairs_bucket_kernel(int n, int table, const double *__restrict__ x, const double *__restrict__ y,
                               const double *__restrict__ z, const double *__restrict__ r,
                               const double2 *__restrict__ P, const float4 *__restrict__ P32,
