@@ -36,6 +36,12 @@ from ..solution.snapshot import SnapshotWriter
 from .solver_base import Solver
 
 
+# Consecutive detections without pairs after which the device loop steps speculatively
+# (detection beside the step, the step discarded if pairs turn up): a discarded step costs a
+# whole step, the overlap saves about the detection's time, so it pays only when merges are rare.
+SPECULATE_AFTER = 8
+
+
 class EulerDropletSolver(Solver):
     def __init__(self, force_calculator, solution, post_processor, collision_detector=None, save_interval: int = 1,
                  pbm_coupling=None, verbose: bool = True, snapshot_depth: int = 4, graphs: bool = True):
@@ -193,17 +199,24 @@ class EulerDropletSolver(Solver):
         graphs = {}  # (n, cur, rc, detect) -> (graph, kernels in it); a key is captured on its second use
         seen = set()
         speculative = det is not None and hasattr(det, "detect_launch") and hasattr(det, "_pairs")
+        side = torch.cuda.Stream(device=dev)  # the speculative step's detection
+        clean = [0]  # consecutive detections without pairs
         pairs_ptr = [det._pairs.data_ptr() if speculative else 0]
 
         def advance(n, cur, rc, detect=False):
             """[detection of pos_bufs[cur] +] forces + convection + Euler from pos_bufs[cur]
             into pos_bufs[1 - cur]."""
             def body():
-                if detect:
-                    det.detect_launch(n, pos_bufs[cur], r_bufs[rc], L, periodic)
+                main = torch.cuda.current_stream(dev)
+                if detect:  # on a side stream, beside the step
+                    side.wait_stream(main)
+                    with torch.cuda.stream(side):
+                        det.detect_launch(n, pos_bufs[cur], r_bufs[rc], L, periodic)
                 F, V = fc.forces_and_convection_soa(n, pos_bufs[cur], r_bufs[rc])
                 ctx.euler_update(n, pos_bufs[cur], r_bufs[rc], F, V, self.stokes_factor, dt, L, periodic,
                                  pos_bufs[1 - cur])
+                if detect:
+                    main.wait_stream(side)
 
             key = (n, cur, rc, detect)
             if not state["graphs"] or key not in seen:
@@ -246,7 +259,9 @@ class EulerDropletSolver(Solver):
                 pos, r = pos_bufs[cur], r_bufs[rc]
                 stepped = False
                 if det is not None and n > 0:
-                    if tree or not speculative:
+                    # a speculative step is discarded when pairs are found, so it pays only while
+                    # collisions are rare: after SPECULATE_AFTER consecutive detections without pairs
+                    if tree or not speculative or clean[0] < SPECULATE_AFTER:
                         k, pairs, counts = det.detect_device(n, pos, r, L, periodic)
                     else:  # detection and the step together; the step is kept when no pair was found
                         advance(n, cur, rc, detect=True)
@@ -257,6 +272,7 @@ class EulerDropletSolver(Solver):
                             graphs.clear()
                             seen.clear()
                         stepped = k == 0
+                    clean[0] = clean[0] + 1 if k == 0 else 0
                     if k > 0:
                         if writer is not None:
                             writer.flush()  # this solution's frames first
