@@ -1080,9 +1080,17 @@ __global__ void prep_sym_kernel(const SymBoxes t, const double *__restrict__ x, 
 // RED_SPLIT consecutive lanes share a droplet: lane q of the group adds the items q, q + RED_SPLIT, ... of both
 // sides, and the groups' sums are combined by a fixed butterfly, so the order depends on K and nbk only.
 constexpr int RED_SPLIT = 4;
+// Build knobs of the reduction: 16-byte loads of the sorted kernel's j records, and the
+// resident CTAs per SM its registers are budgeted for.
+#ifndef DEM_RED_VEC
+#define DEM_RED_VEC 1
+#endif
+#ifndef DEM_RED_MIN_CTAS
+#define DEM_RED_MIN_CTAS 4
+#endif
 
 template <bool FORCE, int JW, bool PLANAR>
-__global__ void __launch_bounds__(256) reduce_sym_kernel(const SymBoxes t, int B, const double *__restrict__ pi,
+__global__ void __launch_bounds__(256, DEM_RED_MIN_CTAS) reduce_sym_kernel(const SymBoxes t, int B, const double *__restrict__ pi,
                                                          const double *__restrict__ pj, const double *__restrict__ r,
                                                          double coeff, double *__restrict__ ox,
                                                          double *__restrict__ oy, double *__restrict__ oz,
@@ -1131,16 +1139,33 @@ __global__ void __launch_bounds__(256) reduce_sym_kernel(const SymBoxes t, int B
                     const long long item = ib + rows_before(Ib, nbk) + K - Ib;
                     const double *P = pj + (size_t)item * JW * wstep + off;
                     double a[JW], b[JW], c[JW];
+                    if (DEM_RED_VEC && !PLANAR && JW % 2 == 0) {  // JW x 3 doubles, 16-byte aligned: vector loads
+                        const double2 *P2 = reinterpret_cast<const double2 *>(P);
+                        double rec[3 * JW];
 #pragma unroll
-                    for (int w = 0; w < JW; ++w) {
-                        if (PLANAR) {
-                            a[w] = P[w * wstep];
-                            b[w] = P[w * wstep + plane];
-                            c[w] = P[w * wstep + 2 * plane];
-                        } else {
-                            a[w] = P[3 * w];
-                            b[w] = P[3 * w + 1];
-                            c[w] = P[3 * w + 2];
+                        for (int h = 0; h < 3 * JW / 2; ++h) {
+                            const double2 v2 = P2[h];
+                            rec[2 * h] = v2.x;
+                            rec[2 * h + 1] = v2.y;
+                        }
+#pragma unroll
+                        for (int w = 0; w < JW; ++w) {
+                            a[w] = rec[3 * w];
+                            b[w] = rec[3 * w + 1];
+                            c[w] = rec[3 * w + 2];
+                        }
+                    } else {
+#pragma unroll
+                        for (int w = 0; w < JW; ++w) {
+                            if (PLANAR) {
+                                a[w] = P[w * wstep];
+                                b[w] = P[w * wstep + plane];
+                                c[w] = P[w * wstep + 2 * plane];
+                            } else {
+                                a[w] = P[3 * w];
+                                b[w] = P[3 * w + 1];
+                                c[w] = P[3 * w + 2];
+                            }
                         }
                     }
 #pragma unroll
