@@ -48,6 +48,7 @@
 // and those of dz^2 |d|^-5 follow from the product rule; contracted with Q they
 // give the closed form of quad_force below.
 #include <algorithm>
+#include <type_traits>
 #include <vector>
 
 #include "corr.cuh"
@@ -966,44 +967,57 @@ __global__ void __launch_bounds__(BH_T, FORCE ? BH_WALK2_CTAS_FORCE : BH_WALK2_C
                                               (float)(bh_mic<PER>(lcy - yi1, w.L, w.halfL) * inv_ell));
                 const float2 lz = make_float2((float)(bh_mic<PER>(lcz - zi0, w.L, w.halfL) * inv_ell),
                                               (float)(bh_mic<PER>(lcz - zi1, w.L, w.halfL) * inv_ell));
-                for (int k = 0; k < cnt; ++k) {
-                    const int sj = s0 + k;
-                    const float4 o = w.loff[sj];
-                    float2 dx = p_add(dup2(o.x), lx), dy = p_add(dup2(o.y), ly), dz = p_add(dup2(o.z), lz);
-                    // within 1e-6 L of the image boundary (or past it: a leaf reaching across L/2 in a
-                    // shallow tree) the image and the separation come from the FP64 positions
-                    if (PER) {
-                        if (fmaxf(fabsf(dx.x), fmaxf(fabsf(dy.x), fabsf(dz.x))) > edge) {
-                            dx.x = (float)(bh_mic<PER>(w.ps[sj] - xi0, w.L, w.halfL) * inv_ell);
-                            dy.x = (float)(bh_mic<PER>(w.ps[cap + sj] - yi0, w.L, w.halfL) * inv_ell);
-                            dz.x = (float)(bh_mic<PER>(w.ps[2 * (size_t)cap + sj] - zi0, w.L, w.halfL) * inv_ell);
+                // every droplet of the leaf lies within `reach` of its centre on each axis, so while
+                // |l| + reach stays below the edge for both targets of every lane, no pair of the leaf
+                // needs the image-boundary test: the warp takes the loop compiled without it
+                const float reach = (FORCE ? rec : w.nd.qr[2 * (size_t)node + 1]).w;
+                const bool near_edge =
+                    PER && (fmaxf(fabsf(lx.x), fmaxf(fabsf(ly.x), fabsf(lz.x))) + reach >= 0.999f * edge ||
+                            fmaxf(fabsf(lx.y), fmaxf(fabsf(ly.y), fabsf(lz.y))) + reach >= 0.999f * edge);
+                auto leaf_pairs = [&](auto edge_tests) {
+                    for (int k = 0; k < cnt; ++k) {
+                        const int sj = s0 + k;
+                        const float4 o = w.loff[sj];
+                        float2 dx = p_add(dup2(o.x), lx), dy = p_add(dup2(o.y), ly), dz = p_add(dup2(o.z), lz);
+                        // within 1e-6 L of the image boundary (or past it: a leaf reaching across L/2 in a
+                        // shallow tree) the image and the separation come from the FP64 positions
+                        if (PER && decltype(edge_tests)::value) {
+                            if (fmaxf(fabsf(dx.x), fmaxf(fabsf(dy.x), fabsf(dz.x))) > edge) {
+                                dx.x = (float)(bh_mic<PER>(w.ps[sj] - xi0, w.L, w.halfL) * inv_ell);
+                                dy.x = (float)(bh_mic<PER>(w.ps[cap + sj] - yi0, w.L, w.halfL) * inv_ell);
+                                dz.x = (float)(bh_mic<PER>(w.ps[2 * (size_t)cap + sj] - zi0, w.L, w.halfL) * inv_ell);
+                            }
+                            if (fmaxf(fabsf(dx.y), fmaxf(fabsf(dy.y), fabsf(dz.y))) > edge) {
+                                dx.y = (float)(bh_mic<PER>(w.ps[sj] - xi1, w.L, w.halfL) * inv_ell);
+                                dy.y = (float)(bh_mic<PER>(w.ps[cap + sj] - yi1, w.L, w.halfL) * inv_ell);
+                                dz.y = (float)(bh_mic<PER>(w.ps[2 * (size_t)cap + sj] - zi1, w.L, w.halfL) * inv_ell);
+                            }
                         }
-                        if (fmaxf(fabsf(dx.y), fmaxf(fabsf(dy.y), fabsf(dz.y))) > edge) {
-                            dx.y = (float)(bh_mic<PER>(w.ps[sj] - xi1, w.L, w.halfL) * inv_ell);
-                            dy.y = (float)(bh_mic<PER>(w.ps[cap + sj] - yi1, w.L, w.halfL) * inv_ell);
-                            dz.y = (float)(bh_mic<PER>(w.ps[2 * (size_t)cap + sj] - zi1, w.L, w.halfL) * inv_ell);
+                        const float2 r2 = p_fma(dx, dx, p_fma(dy, dy, p_mul(dz, dz)));
+                        const float2 rs = p_add(ris, dup2(o.w)), rs2 = p_mul(rs, rs);
+                        // excluded: padding target, the target itself, or closer than r_i + r_j
+                        const bool e0 = !v0 || sj == si0 || r2.x < rs2.x, e1 = !v1 || sj == si1 || r2.y < rs2.y;
+                        if (e0 && e1) continue;
+                        const float2 rinv = p_rsqrt(make_float2(e0 ? 1.f : r2.x, e1 ? 1.f : r2.y));
+                        const float2 rinv2 = p_mul(rinv, rinv);
+                        const float2 keep = make_float2(e0 ? 0.f : 1.f, e1 ? 0.f : 1.f);
+                        if (FORCE) {
+                            const float rj3 = o.w * o.w * o.w;
+                            const float2 r7 = p_mul(p_mul(rinv2, rinv2), p_mul(rinv2, rinv));
+                            mono_force2(dx, dy, dz, p_mul(p_mul(dup2(rj3), keep), r7), ax, ay, az);
+                        } else {  // e = x_i - x_j = -d
+                            const float4 fj = w.fs32[sj];
+                            const float2 ex = p_mul(dup2(-1.f), dx), ey = p_mul(dup2(-1.f), dy),
+                                         ez = p_mul(dup2(-1.f), dz);
+                            stokeslet2(ex, ey, ez, dup2(fj.x), dup2(fj.y), dup2(fj.z), p_mul(rinv, keep), rinv2, ax, ay,
+                                       az);
                         }
                     }
-                    const float2 r2 = p_fma(dx, dx, p_fma(dy, dy, p_mul(dz, dz)));
-                    const float2 rs = p_add(ris, dup2(o.w)), rs2 = p_mul(rs, rs);
-                    // excluded: padding target, the target itself, or closer than r_i + r_j
-                    const bool e0 = !v0 || sj == si0 || r2.x < rs2.x, e1 = !v1 || sj == si1 || r2.y < rs2.y;
-                    if (e0 && e1) continue;
-                    const float2 rinv = p_rsqrt(make_float2(e0 ? 1.f : r2.x, e1 ? 1.f : r2.y));
-                    const float2 rinv2 = p_mul(rinv, rinv);
-                    const float2 keep = make_float2(e0 ? 0.f : 1.f, e1 ? 0.f : 1.f);
-                    if (FORCE) {
-                        const float rj3 = o.w * o.w * o.w;
-                        const float2 r7 = p_mul(p_mul(rinv2, rinv2), p_mul(rinv2, rinv));
-                        mono_force2(dx, dy, dz, p_mul(p_mul(dup2(rj3), keep), r7), ax, ay, az);
-                    } else {  // e = x_i - x_j = -d
-                        const float4 fj = w.fs32[sj];
-                        const float2 ex = p_mul(dup2(-1.f), dx), ey = p_mul(dup2(-1.f), dy),
-                                     ez = p_mul(dup2(-1.f), dz);
-                        stokeslet2(ex, ey, ez, dup2(fj.x), dup2(fj.y), dup2(fj.z), p_mul(rinv, keep), rinv2, ax, ay,
-                                   az);
-                    }
-                }
+                };
+                if (__any_sync(0xffffffffu, near_edge))
+                    leaf_pairs(std::true_type{});
+                else
+                    leaf_pairs(std::false_type{});
                 continue;
             }
             if (sp + nch > BH_STACK) {  // cannot happen for depth <= 10; kept bounded anyway
@@ -1081,10 +1095,15 @@ __global__ void leaf_offsets_kernel(BhNodes nd, int nc, const double *__restrict
         if (nd.nchild[k] != 0) continue;
         const int s0 = nd.start[k], cnt = nd.count[k];
         const double cx = nd.cx[k], cy = nd.cy[k], cz = nd.cz[k];
-        for (int j = s0; j < s0 + cnt; ++j)
-            loff[j] = make_float4((float)((ps[j] - cx) * inv_ell), (float)((ps[cap + j] - cy) * inv_ell),
-                                  (float)((ps[2 * (size_t)cap + j] - cz) * inv_ell),
-                                  (float)(ps[3 * (size_t)cap + j] * inv_ell));
+        float reach = 0.f;
+        for (int j = s0; j < s0 + cnt; ++j) {
+            const float4 o = make_float4((float)((ps[j] - cx) * inv_ell), (float)((ps[cap + j] - cy) * inv_ell),
+                                         (float)((ps[2 * (size_t)cap + j] - cz) * inv_ell),
+                                         (float)(ps[3 * (size_t)cap + j] * inv_ell));
+            loff[j] = o;
+            reach = fmaxf(reach, fmaxf(fabsf(o.x), fmaxf(fabsf(o.y), fabsf(o.z))));
+        }
+        nd.qr[2 * (size_t)k + 1].w = reach;  // the leaf's largest |offset| on any axis (the walks' edge test)
     }
 }
 
