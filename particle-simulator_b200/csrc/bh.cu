@@ -85,8 +85,10 @@ struct BhNodes {
     // walk records, one 16-byte-aligned group per node so that a visit issues vector loads:
     float4 *qr;  // [M][2] second moment Q = sum r^3 (x - c)(x - c)^T and R^3 sum:
                  //        (Qxx, Qxy, Qxz, Qyy), (Qyz, Qzz, R^3, 0)
-    float4 *fd;  // [M][3] force sum and dipole D_ab = sum (x_a - c_a) F_b (row a, column b):
-                 //        (Fx, Fy, Fz, D00), (D01, D02, D10, D11), (D12, D20, D21, D22)
+    float4 *fd;  // [M][3] force sum and dipole D_ab = sum (x_a - c_a) F_b (row a, column b), as its
+                 // symmetric part S = (D + D^T) / 2 and antisymmetric part A = D^T - D:
+                 //        (Fx, Fy, Fz, Sxx), (Syy, Szz, 2 Sxy, 2 Sxz), (2 Syz, A01, A02, A12)
+                 // (the walk's dipole term needs A e, e.S e and tr S only)
 };
 
 }  // namespace dem
@@ -504,9 +506,12 @@ __global__ void node_force_up_kernel(BhNodes nd, int a, int b, int M, const doub
         }
 #pragma unroll
         for (int p = 0; p < 12; ++p) fm[(size_t)p * M + k] = v[p];
-        for (int q = 0; q < 3; ++q)  // v = (F, D row-major): the record's order
-            nd.fd[3 * (size_t)k + q] = make_float4((float)v[4 * q], (float)v[4 * q + 1], (float)v[4 * q + 2],
-                                                   (float)v[4 * q + 3]);
+        // v = (F, D row-major) -> the record: F, S (off-diagonal doubled), A = D^T - D
+        nd.fd[3 * (size_t)k] = make_float4((float)v[0], (float)v[1], (float)v[2], (float)v[3]);
+        nd.fd[3 * (size_t)k + 1] =
+            make_float4((float)v[7], (float)v[11], (float)(v[4] + v[6]), (float)(v[5] + v[9]));
+        nd.fd[3 * (size_t)k + 2] =
+            make_float4((float)(v[8] + v[10]), (float)(v[6] - v[4]), (float)(v[9] - v[5]), (float)(v[10] - v[8]));
     }
 }
 
@@ -662,20 +667,17 @@ __global__ void __launch_bounds__(BH_T, FORCE ? 6 : (CORR ? 5 : 7)) bh_walk_kern
                         ax = fmaf(rinv, fmaf(ex, dot * rinv2, fnx), ax);
                         ay = fmaf(rinv, fmaf(ey, dot * rinv2, fny), ay);
                         az = fmaf(rinv, fmaf(ez, dot * rinv2, fnz), az);
-                        const float4 d1 = rq, d2 = rd;
-                        const float Dm[9] = {rec.w, d1.x, d1.y, d1.z, d1.w, d2.x, d2.y, d2.z, d2.w};  // D_ab
-                        const float Ux = Dm[0] * ex + Dm[3] * ey + Dm[6] * ez;  // D^T e
-                        const float Uy = Dm[1] * ex + Dm[4] * ey + Dm[7] * ez;
-                        const float Uz = Dm[2] * ex + Dm[5] * ey + Dm[8] * ez;
-                        const float Wx = Dm[0] * ex + Dm[1] * ey + Dm[2] * ez;  // D e
-                        const float Wy = Dm[3] * ex + Dm[4] * ey + Dm[5] * ez;
-                        const float Wz = Dm[6] * ex + Dm[7] * ey + Dm[8] * ez;
-                        const float tr = Dm[0] + Dm[4] + Dm[8];
-                        const float q = ex * Wx + ey * Wy + ez * Wz;
+                        // dipole: (D^T e - D e) = A e, e.D e = e.S e, tr D = tr S (records: see BhNodes.fd)
+                        const float sxx = rec.w, syy = rq.x, szz = rq.y, sxy2 = rq.z, sxz2 = rq.w, syz2 = rd.x,
+                                    a01 = rd.y, a02 = rd.z, a12 = rd.w;
+                        const float Aex = a01 * ey + a02 * ez, Aey = a12 * ez - a01 * ex, Aez = -a02 * ex - a12 * ey;
+                        const float tr = sxx + syy + szz;
+                        const float q = ex * (sxx * ex + sxy2 * ey + sxz2 * ez) + ey * (syy * ey + syz2 * ez) +
+                                        ez * (szz * ez);
                         const float rinv3 = rinv * rinv2, rinv5 = rinv3 * rinv2;
-                        ax += rinv3 * (Ux - Wx - tr * ex) + 3.f * ex * q * rinv5;
-                        ay += rinv3 * (Uy - Wy - tr * ey) + 3.f * ey * q * rinv5;
-                        az += rinv3 * (Uz - Wz - tr * ez) + 3.f * ez * q * rinv5;
+                        ax += rinv3 * (Aex - tr * ex) + 3.f * ex * q * rinv5;
+                        ay += rinv3 * (Aey - tr * ey) + 3.f * ey * q * rinv5;
+                        az += rinv3 * (Aez - tr * ez) + 3.f * ez * q * rinv5;
                         if (CORR) corr_pair32(cf, ex, ey, ez, fnx, fny, fnz, cx, cy, cz);
                     }
                 }
@@ -932,21 +934,19 @@ __global__ void __launch_bounds__(BH_T, FORCE ? BH_WALK2_CTAS_FORCE : BH_WALK2_C
                         const float2 fnx = dup2(rec.x), fny = dup2(rec.y), fnz = dup2(rec.z);
                         stokeslet2(dx, dy, dz, fnx, fny, fnz, rinv, rinv2, ax, ay, az);
                         // dipole: D^T e, D e, e.D e, tr D (D_ab from the records, row a, column b)
-                        const float d00 = rec.w, d01 = rq.x, d02 = rq.y, d10 = rq.z, d11 = rq.w, d12 = rd.x,
-                                    d20 = rd.y, d21 = rd.z, d22 = rd.w;
-                        const float2 Ux = p_fma(dup2(d00), dx, p_fma(dup2(d10), dy, p_mul(dup2(d20), dz)));
-                        const float2 Uy = p_fma(dup2(d01), dx, p_fma(dup2(d11), dy, p_mul(dup2(d21), dz)));
-                        const float2 Uz = p_fma(dup2(d02), dx, p_fma(dup2(d12), dy, p_mul(dup2(d22), dz)));
-                        const float2 Wx = p_fma(dup2(d00), dx, p_fma(dup2(d01), dy, p_mul(dup2(d02), dz)));
-                        const float2 Wy = p_fma(dup2(d10), dx, p_fma(dup2(d11), dy, p_mul(dup2(d12), dz)));
-                        const float2 Wz = p_fma(dup2(d20), dx, p_fma(dup2(d21), dy, p_mul(dup2(d22), dz)));
-                        const float2 ntr = dup2(-(d00 + d11 + d22));
-                        const float2 q = p_fma(dx, Wx, p_fma(dy, Wy, p_mul(dz, Wz)));
+                        // dipole: (D^T e - D e) = A e, e.D e = e.S e, tr D = tr S (records: see BhNodes.fd)
+                        const float sxx = rec.w, syy = rq.x, szz = rq.y, sxy2 = rq.z, sxz2 = rq.w, syz2 = rd.x,
+                                    a01 = rd.y, a02 = rd.z, a12 = rd.w;
+                        const float2 ntr = dup2(-(sxx + syy + szz));
+                        const float2 t1 = p_fma(dup2(sxx), dx, p_fma(dup2(sxy2), dy, p_mul(dup2(sxz2), dz)));
+                        const float2 t2 = p_fma(dup2(syy), dy, p_mul(dup2(syz2), dz));
+                        const float2 q = p_fma(dx, t1, p_fma(dy, t2, p_mul(p_mul(dup2(szz), dz), dz)));
                         const float2 rinv3 = p_mul(rinv, rinv2), rinv5 = p_mul(rinv3, rinv2);
                         const float2 q3 = p_mul(p_mul(dup2(3.f), q), rinv5);
-                        const float2 Vx = p_fma(ntr, dx, p_add(Ux, p_mul(dup2(-1.f), Wx)));
-                        const float2 Vy = p_fma(ntr, dy, p_add(Uy, p_mul(dup2(-1.f), Wy)));
-                        const float2 Vz = p_fma(ntr, dz, p_add(Uz, p_mul(dup2(-1.f), Wz)));
+                        // V = A e - tr e
+                        const float2 Vx = p_fma(ntr, dx, p_fma(dup2(a01), dy, p_mul(dup2(a02), dz)));
+                        const float2 Vy = p_fma(ntr, dy, p_fma(dup2(-a01), dx, p_mul(dup2(a12), dz)));
+                        const float2 Vz = p_fma(ntr, dz, p_fma(dup2(-a02), dx, p_mul(dup2(-a12), dy)));
                         ax = p_fma(rinv3, Vx, p_fma(dx, q3, ax));
                         ay = p_fma(rinv3, Vy, p_fma(dy, q3, ay));
                         az = p_fma(rinv3, Vz, p_fma(dz, q3, az));
@@ -1135,7 +1135,7 @@ __global__ void scale_nodes_kernel(BhNodes nd, int nc, const unsigned long long 
             nd.meta[k] = make_int4(cnt, nch, nch ? nd.first_child[k] : nd.start[k],
                                    nd.level[k] | (skip ? BH_SKIP_FORCE : 0) | (cnt == 0 ? BH_SKIP_VEL : 0));
         } else {
-            float *fd = reinterpret_cast<float *>(nd.fd + 3 * (size_t)k);  // F[0..2], D[0..8]
+            float *fd = reinterpret_cast<float *>(nd.fd + 3 * (size_t)k);  // F[0..2], then S and A (linear in D)
             for (int q = 0; q < 3; ++q) fd[q] = (float)((double)fd[q] * fsc);
             for (int q = 3; q < 12; ++q) fd[q] = (float)((double)fd[q] * fsc * inv_ell);
             const double f0 = fd[0], f1 = fd[1], f2 = fd[2];  // force sum in units of 2^q newtons
