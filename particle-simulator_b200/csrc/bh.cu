@@ -803,37 +803,33 @@ __device__ __forceinline__ float2 p_mic(float2 d, float2 invL, float2 nL) {
     return p_fma(nL, u, d);
 }
 
-// quad_force for two targets: x, y, z = D = c - x_i per lane, r7 = |D|^-7, rinv2 = |D|^-2.
+// quad_force for two targets: x, y, z = D = c - x_i per lane, r7 = |D|^-7, rinv2 = |D|^-2.  The same
+// closed form, its terms collected by what they multiply (with the 1/6 folded in):
+//   g += X x + P Qx + C Q e_z + c_z e_z,  P = 2 c_t,  X = c_t tr + c_x,  C = 10 z r^-7,
+//   c_t = 2.5 r^-7 - 17.5 z^2 r^-9,
+//   c_x = -17.5 (x.Qx) r^-9 + 5 Qzz r^-7 - 70 z (Qx)_z r^-9 + 157.5 z^2 (x.Qx) r^-11,
+//   c_z = 10 (Qx)_z r^-7 + 5 z tr r^-7 - 35 z (x.Qx) r^-9
+// (checked against quad_force's form to 1e-14 in FP64 on random separations and moments).
 __device__ __forceinline__ void quad_force2(float2 x, float2 y, float2 z, const float4 qa, const float4 qb, float2 r7,
                                             float2 rinv2, float2 &gx, float2 &gy, float2 &gz) {
-    const float2 r9 = p_mul(r7, rinv2), r11 = p_mul(r9, rinv2);
-    const float2 qxx = dup2(qa.x), qxy = dup2(qa.y), qxz = dup2(qa.z), qyy = dup2(qa.w), qyz = dup2(qb.x),
-                 qzz = dup2(qb.y);
-    const float2 tr = dup2(qa.x + qa.w + qb.y);
-    const float2 Qx = p_fma(qxx, x, p_fma(qxy, y, p_mul(qxz, z)));
-    const float2 Qy = p_fma(qxy, x, p_fma(qyy, y, p_mul(qyz, z)));
-    const float2 Qz = p_fma(qxz, x, p_fma(qyz, y, p_mul(qzz, z)));
+    const float2 r9 = p_mul(r7, rinv2);
+    const float qxx = qa.x, qxy = qa.y, qxz = qa.z, qyy = qa.w, qyz = qb.x, qzz = qb.y;
+    const float tr = qxx + qyy + qzz;
+    const float2 Qx = p_fma(dup2(qxx), x, p_fma(dup2(qxy), y, p_mul(dup2(qxz), z)));
+    const float2 Qy = p_fma(dup2(qxy), x, p_fma(dup2(qyy), y, p_mul(dup2(qyz), z)));
+    const float2 Qz = p_fma(dup2(qxz), x, p_fma(dup2(qyz), y, p_mul(dup2(qzz), z)));
     const float2 xQx = p_fma(x, Qx, p_fma(y, Qy, p_mul(z, Qz)));
-    // from |d|^-3: 15 [(tr x + 2 Q x) r^-7 - 7 (x.Qx) x r^-9]
-    const float2 a1 = p_mul(dup2(15.f), r7), a2 = p_mul(p_mul(dup2(-105.f), xQx), r9);
-    // from dz^2 |d|^-5 (times -3 below)
-    const float2 zz = p_mul(z, z), zr7 = p_mul(z, r7);
-    const float2 b1 = p_mul(p_mul(dup2(35.f), zz), r9);
-    const float2 b2 = p_fma(dup2(-10.f * qb.y), r7,
-                            p_fma(p_mul(dup2(140.f), p_mul(z, Qz)), r9, p_mul(p_mul(dup2(-315.f), p_mul(zz, xQx)), r11)));
-    const float2 tx = p_fma(dup2(2.f), Qx, p_mul(tr, x)), ty = p_fma(dup2(2.f), Qy, p_mul(tr, y)),
-                 tz = p_fma(dup2(2.f), Qz, p_mul(tr, z));
-    const float2 Bx = p_fma(b1, tx, p_fma(b2, x, p_mul(dup2(-20.f * qa.z), zr7)));
-    const float2 By = p_fma(b1, ty, p_fma(b2, y, p_mul(dup2(-20.f * qb.x), zr7)));
-    const float2 Bz = p_fma(
-        b1, tz,
-        p_fma(b2, z,
-              p_fma(dup2(-20.f * qb.y), zr7,
-                    p_fma(dup2(-20.f), p_mul(Qz, r7),
-                          p_mul(p_mul(dup2(-10.f), z), p_fma(tr, r7, p_mul(dup2(-7.f), p_mul(xQx, r9))))))));
-    gx = p_fma(dup2(1.f / 6.f), p_fma(a1, tx, p_fma(a2, x, p_mul(dup2(-3.f), Bx))), gx);
-    gy = p_fma(dup2(1.f / 6.f), p_fma(a1, ty, p_fma(a2, y, p_mul(dup2(-3.f), By))), gy);
-    gz = p_fma(dup2(1.f / 6.f), p_fma(a1, tz, p_fma(a2, z, p_mul(dup2(-3.f), Bz))), gz);
+    const float2 zz = p_mul(z, z), u = p_mul(xQx, r9), zr7 = p_mul(z, r7);
+    const float2 ct = p_fma(dup2(-17.5f), p_mul(zz, r9), p_mul(dup2(2.5f), r7));
+    const float2 cx = p_fma(dup2(-17.5f), u,
+                            p_fma(dup2(5.f * qzz), r7,
+                                  p_fma(dup2(-70.f), p_mul(p_mul(z, Qz), r9),
+                                        p_mul(dup2(157.5f), p_mul(p_mul(zz, u), rinv2)))));
+    const float2 cz = p_fma(dup2(10.f), p_mul(Qz, r7), p_fma(dup2(5.f * tr), zr7, p_mul(dup2(-35.f), p_mul(z, u))));
+    const float2 X = p_fma(ct, dup2(tr), cx), P = p_add(ct, ct), C = p_mul(dup2(10.f), zr7);
+    gx = p_fma(X, x, p_fma(P, Qx, p_fma(C, dup2(qxz), gx)));
+    gy = p_fma(X, y, p_fma(P, Qy, p_fma(C, dup2(qyz), gy)));
+    gz = p_fma(X, z, p_fma(P, Qz, p_fma(C, dup2(qzz), p_add(gz, cz))));
 }
 
 // The pair force r_j^3 P(d) / |d|^7 (b = r_j^3 |d|^-7, per lane) added to (ax, ay, az).
