@@ -883,6 +883,7 @@ __global__ void __launch_bounds__(BH_T, FORCE ? BH_WALK2_CTAS_FORCE : BH_WALK2_C
         const float2 ys = make_float2((float)((yi0 - goy) * inv_ell), (float)((yi1 - goy) * inv_ell));
         const float2 zs = make_float2((float)((zi0 - goz) * inv_ell), (float)((zi1 - goz) * inv_ell));
         const float2 ris = make_float2((float)(ri0 * inv_ell), (float)(ri1 * inv_ell));
+        const float2 nxs = make_float2(-xs.x, -xs.y), nys = make_float2(-ys.x, -ys.y), nzs = make_float2(-zs.x, -zs.y);
         float2 ax = make_float2(0.f, 0.f), ay = ax, az = ax;
         int sp = 1;
         if (lane == 0) stack[wp][0] = 0;
@@ -904,9 +905,9 @@ __global__ void __launch_bounds__(BH_T, FORCE ? BH_WALK2_CTAS_FORCE : BH_WALK2_C
             const int cnt = mt.x;
             if (mt.w & (FORCE ? BH_SKIP_FORCE : BH_SKIP_VEL)) continue;  // empty, or :861 / :1155
             // force walk: D = c - x_i; velocity walk: e = x_i - c (= -D, the minimum image is odd)
-            float2 dx = FORCE ? p_add(dup2(cs.x), p_mul(dup2(-1.f), xs)) : p_add(xs, dup2(-cs.x));
-            float2 dy = FORCE ? p_add(dup2(cs.y), p_mul(dup2(-1.f), ys)) : p_add(ys, dup2(-cs.y));
-            float2 dz = FORCE ? p_add(dup2(cs.z), p_mul(dup2(-1.f), zs)) : p_add(zs, dup2(-cs.z));
+            float2 dx = FORCE ? p_add(dup2(cs.x), nxs) : p_add(xs, dup2(-cs.x));
+            float2 dy = FORCE ? p_add(dup2(cs.y), nys) : p_add(ys, dup2(-cs.y));
+            float2 dz = FORCE ? p_add(dup2(cs.z), nzs) : p_add(zs, dup2(-cs.z));
             dx = p_mic<PER>(dx, invL2, nL2);
             dy = p_mic<PER>(dy, invL2, nL2);
             dz = p_mic<PER>(dz, invL2, nL2);
@@ -1001,11 +1002,9 @@ __global__ void __launch_bounds__(BH_T, FORCE ? BH_WALK2_CTAS_FORCE : BH_WALK2_C
                             const float rj3 = o.w * o.w * o.w;
                             const float2 r7 = p_mul(p_mul(rinv2, rinv2), p_mul(rinv2, rinv));
                             mono_force2(dx, dy, dz, p_mul(p_mul(dup2(rj3), keep), r7), ax, ay, az);
-                        } else {  // e = x_i - x_j = -d
+                        } else {  // G(e) with e = x_i - x_j = -d: G is even, so d serves
                             const float4 fj = w.fs32[sj];
-                            const float2 ex = p_mul(dup2(-1.f), dx), ey = p_mul(dup2(-1.f), dy),
-                                         ez = p_mul(dup2(-1.f), dz);
-                            stokeslet2(ex, ey, ez, dup2(fj.x), dup2(fj.y), dup2(fj.z), p_mul(rinv, keep), rinv2, ax, ay,
+                            stokeslet2(dx, dy, dz, dup2(fj.x), dup2(fj.y), dup2(fj.z), p_mul(rinv, keep), rinv2, ax, ay,
                                        az);
                         }
                     }
