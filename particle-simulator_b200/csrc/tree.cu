@@ -394,7 +394,11 @@ __global__ void __launch_bounds__(128) force_walk_kernel(TreeDev t, double m_con
                                                          double *__restrict__ fz) {
     const int M = t.max_nodes, N = t.cap, n = t.n;
     const double L = t.L, halfL = 0.5 * t.L;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    // targets in leaf-slot order (a permutation of all n particles: every particle ends in a leaf), so
+    // the lanes of a warp walk neighbouring targets along nearly the same path; each target's sums
+    // are its own thread's, in the reference's order, whatever order the targets are taken in
+    for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < n; slot += gridDim.x * blockDim.x) {
+        const int i = t.leaf_idx[slot];
         const double xi = t.p[i], yi = t.p[N + i], zi = t.p[2 * N + i], ri = t.p[3 * N + i];
         const double ri3 = ipow3(ri);
         double Fx = 0, Fy = 0, Fz = 0;
@@ -485,7 +489,9 @@ __global__ void __launch_bounds__(128) velocity_walk_kernel(TreeDev t, const dou
                                                             double *__restrict__ vz) {
     const int M = t.max_nodes, N = t.cap, n = t.n;
     const double L = t.L, halfL = 0.5 * t.L;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    // targets in leaf-slot order, as in force_walk_kernel
+    for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < n; slot += gridDim.x * blockDim.x) {
+        const int i = t.leaf_idx[slot];
         const double xi = t.p[i], yi = t.p[N + i], zi = t.p[2 * N + i], ri = t.p[3 * N + i];
         double ux = 0, uy = 0, uz = 0;
         if (stokes > 0) {
@@ -608,7 +614,9 @@ __global__ void collision_walk_kernel(TreeDev t, const int32_t *__restrict__ bin
                                       unsigned int *__restrict__ matrix) {
     const int M = t.max_nodes, N = t.cap, n = t.n;
     const double L = t.L, halfL = 0.5 * t.L;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    // targets in leaf-slot order, as in force_walk_kernel (the counts are integers: any order)
+    for (int slot = blockIdx.x * blockDim.x + threadIdx.x; slot < n; slot += gridDim.x * blockDim.x) {
+        const int i = t.leaf_idx[slot];
         const double xi = t.p[i], yi = t.p[N + i], zi = t.p[2 * N + i], ri = t.p[3 * N + i];
         const int bi = bins[i];
         int node = 0, steps = 0;
