@@ -73,6 +73,21 @@ __device__ __forceinline__ void decode_item(int q, int nb, int &I, int &J) {
     J = I + (int)(q - rows_before(I, nb));
 }
 
+// Processing order of the sorted pair kernel within a box: the nb diagonal
+// items (I, I) first, then the off-diagonal items (I < J) row by row.  A
+// diagonal item evaluates every ordered pair of a compact block, and most of
+// the box's near-contact pairs, which take the FP64 path, lie there: it runs
+// several times longer than an off-diagonal item.  Started first, these items
+// overlap the rest of the grid instead of forming its tail.
+__device__ __forceinline__ void decode_slot(int s, int nb, int &I, int &J) {
+    if (s < nb) {
+        I = J = s;
+        return;
+    }
+    decode_item(s - nb, nb - 1, I, J);  // upper triangle without the diagonal: rows of nb - 1 - I items
+    ++J;
+}
+
 // The box of work item q: droplet offset o0 and count n, padded offset p0,
 // blocks nbk, side L, scale slots sc; ql = item index within the box.
 struct BoxView {
@@ -411,6 +426,77 @@ __global__ void __launch_bounds__(SYM_T, 4) mixed_sym_kernel(const SymArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// Both FP64 terms of one near pair, sharing the square root and the division:
+// a on droplet i from j, b on j from i (scaled units, the reference formulas).
+// ---------------------------------------------------------------------------
+struct NearTerms {
+    double ax, ay, az, bx, by, bz;
+};
+
+// Force (direct_droplet_force_calculator.py:183-200, 229-249): the term on i is
+// r_j^3 g(d), d = x_j - x_i after the minimum image; g is odd in d, so the term
+// on j is -r_i^3 g(d).  Both are cut at contact, r <= r_i + r_j.
+static __device__ __noinline__ NearTerms near_force_pair_fp64(int i, int j, const MixedArgs a, int periodic,
+                                                              double inv_ell, double L) {
+    NearTerms o = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    double dx = a.x[j] - a.x[i], dy = a.y[j] - a.y[i], dz = a.z[j] - a.z[i];
+    if (periodic) {
+        dx = mic64(dx, L, 0.5 * L);
+        dy = mic64(dy, L, 0.5 * L);
+        dz = mic64(dz, L, 0.5 * L);
+    }
+    const double r_mag = sqrt(dx * dx + dy * dy + dz * dz);
+    const double ri = a.r[i], rj = a.r[j];
+    if (!(r_mag > ri + rj)) return o;  // contact cut, :246
+    const double s = inv_ell;
+    dx *= s;
+    dy *= s;
+    dz *= s;
+    const double inv7 = 1.0 / ipow7(r_mag * s);
+    const double dx2 = dx * dx, dy2 = dy * dy, dz2 = dz * dz;
+    const double fxy = inv7 * (4 * dz2 - dx2 - dy2);
+    const double gx = fxy * dx, gy = fxy * dy, gz = inv7 * (2 * dz2 - 3 * dx2 - 3 * dy2) * dz;
+    const double cj = ipow3(rj * s), ci = ipow3(ri * s);
+    o.ax = cj * gx;
+    o.ay = cj * gy;
+    o.az = cj * gz;
+    o.bx = -ci * gx;
+    o.by = -ci * gy;
+    o.bz = -ci * gz;
+    return o;
+}
+
+// Oseen (:381-411, no contact cut): with X = x_i - x_j, the velocity of i from
+// F_j is F_j / r + X (X . F_j) / r^3; the tensor is even in X, so j gets the same
+// form with F_i.
+static __device__ __noinline__ NearTerms near_oseen_pair_fp64(int i, int j, const MixedArgs a, int periodic,
+                                                              double inv_ell, double fscale_inv, double L) {
+    double X = a.x[i] - a.x[j], Y = a.y[i] - a.y[j], Z = a.z[i] - a.z[j];
+    if (periodic) {
+        X = mic64(X, L, 0.5 * L);
+        Y = mic64(Y, L, 0.5 * L);
+        Z = mic64(Z, L, 0.5 * L);
+    }
+    const double s = inv_ell;
+    X *= s;
+    Y *= s;
+    Z *= s;
+    const double inv_r = 1.0 / sqrt(X * X + Y * Y + Z * Z);
+    const double inv_r3 = inv_r * inv_r * inv_r;
+    const double Fjx = a.fx[j] * fscale_inv, Fjy = a.fy[j] * fscale_inv, Fjz = a.fz[j] * fscale_inv;
+    const double Fix = a.fx[i] * fscale_inv, Fiy = a.fy[i] * fscale_inv, Fiz = a.fz[i] * fscale_inv;
+    const double dj = (X * Fjx + Y * Fjy + Z * Fjz) * inv_r3, di = (X * Fix + Y * Fiy + Z * Fiz) * inv_r3;
+    NearTerms o;
+    o.ax = Fjx * inv_r + X * dj;
+    o.ay = Fjy * inv_r + Y * dj;
+    o.az = Fjz * inv_r + Z * dj;
+    o.bx = Fix * inv_r + X * di;
+    o.by = Fiy * inv_r + Y * di;
+    o.bz = Fiz * inv_r + Z * di;
+    return o;
+}
+
+// ---------------------------------------------------------------------------
 // One box with its droplets in Morton order: lists of far j's without the
 // per-pair tests.
 //
@@ -529,6 +615,90 @@ __device__ __forceinline__ int classify_j(float sc[3], float kj, const float4 &b
 // sub-tile loops: MODE_FAST (no image), MODE_MASKED (image on the axes of a uniform mask), MODE_SLOW
 enum { MODE_FAST = 0, MODE_MASKED = 1, MODE_SLOW = 2 };
 
+// Near pairs of the slow run (near contact, i == j, ambiguous image) are not
+// evaluated where the test finds them: each thread queues the list entry per
+// i row, and the warp evaluates the queues together once one is full and at
+// the end of the item, every lane on its own rows' pairs.  Evaluated where
+// found, a pair ran on one lane with the warp waiting on its FP64 loads,
+// square root and division; a diagonal item holds a few thousand such pairs.
+constexpr int NQ = 8;  // queued pairs per (i row, thread)
+struct NearQueue {
+    uint16_t (*entry)[NQ][SYM_T];  // [IPT][NQ][SYM_T]: list entry of each queued pair
+    uint8_t (*count)[SYM_T];       // [IPT][SYM_T]
+    double (*stage)[3][32];        // [warps][3][32]: j-side terms of one round
+};
+
+// Evaluates every queued pair of the calling warp in FP64.  The i-side term is
+// folded into the owner thread's compensated sums, rows in order and each
+// row's pairs in queue order.  The j-side term goes, for an entry of the
+// current sub-tile (cur_sub), to jnear (added when the sub-tile writes its
+// partial sums), else onto the entry's partial sum already written to PJ; the
+// terms on one entry within a round are added in lane order.  All orders
+// depend only on the inputs.
+template <int IPT, bool PER, bool FORCE>
+__device__ __forceinline__ void near_flush(const SortedArgs &a, const int *CI, int lane, int tid, int warp, int I,
+                                           int J, bool diag, const BoxView &v, double inv_ell, double fscale_inv,
+                                           int cur_sub, const NearQueue &nq, double (*jnear)[3][32], double *PJ,
+                                           float *hx, float *hy, float *hz, float *lx, float *ly, float *lz) {
+    constexpr int B = SYM_T * IPT;
+    constexpr int NW = SYM_T / 32;
+    const double sg = FORCE ? -1.0 : 1.0;  // the force i side is held negated
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+        const int cnt = nq.count[k][tid];
+        const int rounds = (int)__reduce_max_sync(0xffffffffu, (unsigned)cnt);
+        const int il = I * B + k * SYM_T + tid;
+        const int i = il < v.n ? a.perm[v.o0 + il] : -1;
+#pragma unroll 1
+        for (int t = 0; t < rounds; ++t) {
+            int key = -1;
+            NearTerms w = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+            if (t < cnt && i >= 0) {
+                const int jj = nq.entry[k][t][tid];
+                const int jo = CI[jj];
+                const int jl = J * B + jo;
+                if (jo >= 0 && jl < v.n && jl != il) {  // padding entries and i == j add nothing
+                    const int j = a.perm[v.o0 + jl];
+                    w = FORCE ? near_force_pair_fp64(i, j, a.s.m, PER ? 1 : 0, inv_ell, v.L)
+                              : near_oseen_pair_fp64(i, j, a.s.m, PER ? 1 : 0, inv_ell, fscale_inv, v.L);
+                    fold_double(hx[k], lx[k], sg * w.ax);
+                    fold_double(hy[k], ly[k], sg * w.ay);
+                    fold_double(hz[k], lz[k], sg * w.az);
+                    key = jj;
+                }
+            }
+            if (!diag) {  // a diagonal item evaluates both orders of each pair on the i side
+                nq.stage[warp][0][lane] = w.bx;
+                nq.stage[warp][1][lane] = w.by;
+                nq.stage[warp][2][lane] = w.bz;
+                __syncwarp();
+                const unsigned peers = __match_any_sync(0xffffffffu, key);
+                if (key >= 0 && lane == __ffs(peers) - 1) {
+                    double bx = 0.0, by = 0.0, bz = 0.0;
+                    for (unsigned m = peers; m; m &= m - 1) {
+                        const int l = __ffs(m) - 1;
+                        bx += nq.stage[warp][0][l];
+                        by += nq.stage[warp][1][l];
+                        bz += nq.stage[warp][2][l];
+                    }
+                    if ((key >> 5) == cur_sub) {
+                        jnear[warp][0][key & 31] += bx;
+                        jnear[warp][1][key & 31] += by;
+                        jnear[warp][2][key & 31] += bz;
+                    } else {
+                        double *d = PJ + (size_t)CI[key] * NW * 3;
+                        d[0] += bx;
+                        d[1] += by;
+                        d[2] += bz;
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        nq.count[k][tid] = 0;
+    }
+}
+
 // Build knobs of the sorted pair kernel: resident CTAs per SM its registers are
 // budgeted for, and how the force pass forms r^-7 (1: 2^(-3.5 log2 r^2) from the
 // PTX approximate lg2 / ex2, two MUFU operations and one multiply; 0: rsqrt and
@@ -563,8 +733,8 @@ __device__ __forceinline__ void sorted_subtile(const SortedArgs &a, const float4
                                                const float2 *wi, const float2 *fxi, const float2 *fyi,
                                                const float2 *fzi, float2 *ax, float2 *ay, float2 *az, float *hx,
                                                float *hy, float *hz, float *lx, float *ly, float *lz,
-                                               double (*jnear)[3][32], float2 &sx, float2 &sy, float2 &sz,
-                                               bool &had_exact) {
+                                               double (*jnear)[3][32], const NearQueue &nq, double *PJ,
+                                               float2 &sx, float2 &sy, float2 &sz, bool &had_exact) {
     constexpr int B = SYM_T * IPT;
     constexpr int KP = IPT / 2;
     constexpr bool TESTS = MODE == MODE_SLOW;
@@ -653,40 +823,21 @@ __device__ __forceinline__ void sorted_subtile(const SortedArgs &a, const float4
             bool any = false;
 #pragma unroll
             for (int k = 0; k < IPT; ++k) any |= ex[k];
-            if (__any_sync(0xffffffffu, any)) {  // rare: exact FP64 terms
-                had_exact = true;
-                const int jo = CI[jj];
-                const int jl = J * B + jo;  // packed position of j
-                if (any && jo >= 0 && jl < v.n) {
-                    const int j = a.perm[v.o0 + jl];
-                    double ex_ = 0.0, ey_ = 0.0, ez_ = 0.0;
+            if (__any_sync(0xffffffffu, any)) {  // rare: queue the pairs for the FP64 terms
+                bool full_q = false;
 #pragma unroll
-                    for (int k = 0; k < IPT; ++k) {
-                        const int il = I * B + k * SYM_T + tid;
-                        if (ex[k] && il < v.n) {
-                            const int i = a.perm[v.o0 + il];
-                            const double3 w1 = FORCE ? near_force_fp64(i, j, a.s.m, PER ? 1 : 0, inv_ell, v.L)
-                                                     : near_oseen_fp64(i, j, a.s.m, PER ? 1 : 0, inv_ell,
-                                                                       fscale_inv, v.L);
-                            const double sg = FORCE ? -1.0 : 1.0;  // the force i side is held negated
-                            fold_double(hx[k], lx[k], sg * w1.x);
-                            fold_double(hy[k], ly[k], sg * w1.y);
-                            fold_double(hz[k], lz[k], sg * w1.z);
-                            if (!diag) {
-                                const double3 w2 = FORCE ? near_force_fp64(j, i, a.s.m, PER ? 1 : 0, inv_ell, v.L)
-                                                         : near_oseen_fp64(j, i, a.s.m, PER ? 1 : 0, inv_ell,
-                                                                           fscale_inv, v.L);
-                                ex_ += w2.x;
-                                ey_ += w2.y;
-                                ez_ += w2.z;
-                            }
-                        }
+                for (int k = 0; k < IPT; ++k) {
+                    if (ex[k]) {
+                        const int c = nq.count[k][tid];
+                        nq.entry[k][c][tid] = (uint16_t)jj;
+                        nq.count[k][tid] = (uint8_t)(c + 1);
+                        full_q |= c + 1 == NQ;
                     }
-                    if (!diag) {
-                        jnear[warp][0][u] += ex_;
-                        jnear[warp][1][u] += ey_;
-                        jnear[warp][2][u] += ez_;
-                    }
+                }
+                if (__any_sync(0xffffffffu, full_q)) {
+                    had_exact = true;  // jnear may hold terms of this sub-tile
+                    near_flush<IPT, PER, FORCE>(a, CI, lane, tid, warp, I, J, diag, v, inv_ell, fscale_inv, e0 >> 5,
+                                                nq, jnear, PJ, hx, hy, hz, lx, ly, lz);
                 }
             }
         }
@@ -717,6 +868,10 @@ __global__ void __launch_bounds__(SYM_T, DEM_SORTED_MIN_CTAS) mixed_sym_sorted_k
     int *CI = reinterpret_cast<int *>(C3 + CAP);  // list entry -> j within block J (-1: padding entry)
     unsigned char *CM = reinterpret_cast<unsigned char *>(CI + CAP);  // list entry -> class (image mask)
     __shared__ double jnear[NW][3][32];           // exact j-side terms of the current sub-tile, per warp
+    __shared__ uint16_t nq_entry[IPT][NQ][SYM_T];  // queued near pairs (list entries), per i row and thread
+    __shared__ uint8_t nq_count[IPT][SYM_T];
+    __shared__ double nq_stage[NW][3][32];
+    const NearQueue nq = {nq_entry, nq_count, nq_stage};
     __shared__ int wcnt[IPT][NW][NCLS];           // entries per round, warp and class
     __shared__ int wpre[IPT][NW][NCLS];           // entries of the class before (round, warp)
     __shared__ int ctot[NCLS], cbase[NCLS];       // entries per class; first entry of a class in the masked run
@@ -725,13 +880,18 @@ __global__ void __launch_bounds__(SYM_T, DEM_SORTED_MIN_CTAS) mixed_sym_sorted_k
     if ((int)blockIdx.x >= nitems) return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int c = tid; c < NW * 3 * 32; c += SYM_T) (&jnear[0][0][0])[c] = 0.0;
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) nq_count[k][tid] = 0;
     const size_t plane = (size_t)B;
     const unsigned lt = (1u << lane) - 1u;
 
-    for (int q = blockIdx.x; q < nitems; q += gridDim.x) {
-        int ql, I, J;
-        const BoxView v = item_box(a.s.t, B, q, ql);
-        decode_item(ql, v.nbk, I, J);
+    for (int slot = blockIdx.x; slot < nitems; slot += gridDim.x) {
+        // slot: processing order (diagonal items first); q: the item's row-major index, which places its
+        // partial sums, so the order changes nothing in the results
+        int sl, I, J;
+        const BoxView v = item_box(a.s.t, B, slot, sl);
+        decode_slot(sl, v.nbk, I, J);
+        const int q = slot - sl + (int)(rows_before(I, v.nbk) + (J - I));
         const bool diag = (I == J);
         const double inv_ell = pow2_inv_of(v.sc[0]);
         const double fscale_inv = FORCE ? 1.0 : pow2_inv_of(v.sc[1]);
@@ -883,8 +1043,8 @@ __global__ void __launch_bounds__(SYM_T, DEM_SORTED_MIN_CTAS) mixed_sym_sorted_k
 #define DEM_SORTED_SUBTILE(MODE, MASK)                                                                            \
     sorted_subtile<IPT, PER, FORCE, MODE, MASK>(a, C0, C1, C2, C3, CI, 32 * sub, lane, tid, warp, I, J, diag, v,   \
                                                 inv_ell, fscale_inv, invL2, magic2, nmagic2, nL2, hm, xi, yi, zi, ki, \
-                                                wi, fxi, fyi, fzi, ax, ay, az, hx, hy, hz, lx, ly, lz, jnear, sx, sy, \
-                                                sz, had_exact)
+                                                wi, fxi, fyi, fzi, ax, ay, az, hx, hy, hz, lx, ly, lz, jnear, nq, PJ, \
+                                                sx, sy, sz, had_exact)
                 if (sub < nfs) {
                     DEM_SORTED_SUBTILE(MODE_FAST, 0);
                 } else if (sub < nfs + nms) {
@@ -933,6 +1093,14 @@ __global__ void __launch_bounds__(SYM_T, DEM_SORTED_MIN_CTAS) mixed_sym_sorted_k
                     }
                 }
             }
+        }
+        {  // the pairs still queued (their j entries' partial sums are written)
+            bool pending = false;
+#pragma unroll
+            for (int k = 0; k < IPT; ++k) pending |= nq_count[k][tid] != 0;
+            if (__any_sync(0xffffffffu, pending))
+                near_flush<IPT, PER, FORCE>(a, CI, lane, tid, warp, I, J, diag, v, inv_ell, fscale_inv, -1, nq, jnear,
+                                            PJ, hx, hy, hz, lx, ly, lz);
         }
         __syncthreads();  // every warp is done with the lists before the next item rebuilds them
         double *PI = a.s.pi + (size_t)q * 3 * plane;  // interleaved per droplet: [i][3]
