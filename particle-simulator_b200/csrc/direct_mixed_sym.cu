@@ -616,87 +616,105 @@ __device__ __forceinline__ int classify_j(float sc[3], float kj, const float4 &b
 enum { MODE_FAST = 0, MODE_MASKED = 1, MODE_SLOW = 2 };
 
 // Near pairs of the slow run (near contact, i == j, ambiguous image) are not
-// evaluated where the test finds them: each thread queues the list entry per
-// i row, and the warp evaluates the queues together once one is full and at
-// the end of the item, every lane on its own rows' pairs.  Evaluated where
-// found, a pair ran on one lane with the warp waiting on its FP64 loads,
-// square root and division; a diagonal item holds a few thousand such pairs.
-constexpr int NQ = 8;  // queued pairs per (i row, thread)
+// evaluated where the test finds them.  Each warp queues them (entry code:
+// list entry jj | i row k << 10 | owner lane << 12, rows then lanes in order)
+// and evaluates the queue 32 pairs at a time, every lane on one pair, once it
+// holds more than one sub-tile step can add and at the end of the item.
+// Evaluated where found, a pair ran on one lane with the warp waiting on its
+// FP64 loads, square root and division; at N = 65,536 a force pass meets
+// ~5e5 such pairs (k = 5), a few thousand in every diagonal item.
+constexpr int NQ_CAP = 256;  // queued pairs per warp
 struct NearQueue {
-    uint16_t (*entry)[NQ][SYM_T];  // [IPT][NQ][SYM_T]: list entry of each queued pair
-    uint8_t (*count)[SYM_T];       // [IPT][SYM_T]
-    double (*stage)[3][32];        // [warps][3][32]: j-side terms of one round
+    uint32_t (*entry)[NQ_CAP];  // [warps][NQ_CAP]
+    int *count;                 // [warps]
+    double (*mbox)[3][32];      // [warps][3][lane]: the i-side terms of one row and round, per owner lane
 };
 
-// Evaluates every queued pair of the calling warp in FP64.  The i-side term is
-// folded into the owner thread's compensated sums, rows in order and each
-// row's pairs in queue order.  The j-side term goes, for an entry of the
-// current sub-tile (cur_sub), to jnear (added when the sub-tile writes its
-// partial sums), else onto the entry's partial sum already written to PJ; the
-// terms on one entry within a round are added in lane order.  All orders
-// depend only on the inputs.
+// Evaluates every queued pair of the calling warp in FP64 (whole warp, uniform
+// call).  Terms go to their targets in queue order: within a round the terms
+// on one target are added one rank at a time (the pairs' queue order), and
+// rounds follow each other.
+//   i side: per row k, the sum for each owner lane is handed over in mbox and
+//           folded into the owner's compensated sums;
+//   j side: an entry of the current sub-tile (cur_sub) collects in jnear
+//           (added when the sub-tile writes its partial sums); an earlier
+//           entry is added onto its partial sum already written to PJ.
 template <int IPT, bool PER, bool FORCE>
-__device__ __forceinline__ void near_flush(const SortedArgs &a, const int *CI, int lane, int tid, int warp, int I,
-                                           int J, bool diag, const BoxView &v, double inv_ell, double fscale_inv,
+__device__ __forceinline__ void near_flush(const SortedArgs &a, const int *CI, int lane, int warp, int I, int J,
+                                           bool diag, const BoxView &v, double inv_ell, double fscale_inv,
                                            int cur_sub, const NearQueue &nq, double (*jnear)[3][32], double *PJ,
                                            float *hx, float *hy, float *hz, float *lx, float *ly, float *lz) {
     constexpr int B = SYM_T * IPT;
     constexpr int NW = SYM_T / 32;
     const double sg = FORCE ? -1.0 : 1.0;  // the force i side is held negated
-#pragma unroll
-    for (int k = 0; k < IPT; ++k) {
-        const int cnt = nq.count[k][tid];
-        const int rounds = (int)__reduce_max_sync(0xffffffffu, (unsigned)cnt);
-        const int il = I * B + k * SYM_T + tid;
-        const int i = il < v.n ? a.perm[v.o0 + il] : -1;
+    const unsigned lt = (1u << lane) - 1u;
+    const int qn = nq.count[warp];
 #pragma unroll 1
-        for (int t = 0; t < rounds; ++t) {
-            int key = -1;
-            NearTerms w = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-            if (t < cnt && i >= 0) {
-                const int jj = nq.entry[k][t][tid];
-                const int jo = CI[jj];
-                const int jl = J * B + jo;
-                if (jo >= 0 && jl < v.n && jl != il) {  // padding entries and i == j add nothing
-                    const int j = a.perm[v.o0 + jl];
-                    w = FORCE ? near_force_pair_fp64(i, j, a.s.m, PER ? 1 : 0, inv_ell, v.L)
-                              : near_oseen_pair_fp64(i, j, a.s.m, PER ? 1 : 0, inv_ell, fscale_inv, v.L);
-                    fold_double(hx[k], lx[k], sg * w.ax);
-                    fold_double(hy[k], ly[k], sg * w.ay);
-                    fold_double(hz[k], lz[k], sg * w.az);
-                    key = jj;
-                }
+    for (int base = 0; base < qn; base += 32) {
+        const int s = base + lane;
+        int code = -1;
+        NearTerms w = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        if (s < qn) {
+            const int c = (int)nq.entry[warp][s];
+            const int jj = c & 1023, k = (c >> 10) & 3, ol = c >> 12;
+            const int il = I * B + k * SYM_T + warp * 32 + ol;
+            const int jo = CI[jj];
+            const int jl = J * B + jo;
+            if (jo >= 0 && jl < v.n && il < v.n && jl != il) {  // padding entries and i == j add nothing
+                const int i = a.perm[v.o0 + il], j = a.perm[v.o0 + jl];
+                w = FORCE ? near_force_pair_fp64(i, j, a.s.m, PER ? 1 : 0, inv_ell, v.L)
+                          : near_oseen_pair_fp64(i, j, a.s.m, PER ? 1 : 0, inv_ell, fscale_inv, v.L);
+                code = c;
             }
-            if (!diag) {  // a diagonal item evaluates both orders of each pair on the i side
-                nq.stage[warp][0][lane] = w.bx;
-                nq.stage[warp][1][lane] = w.by;
-                nq.stage[warp][2][lane] = w.bz;
+        }
+        // i side, row by row (static rows: the sums live in registers)
+#pragma unroll
+        for (int k = 0; k < IPT; ++k) {
+            const int key = (code >= 0 && ((code >> 10) & 3) == k) ? (code >> 12) : -1;  // owner lane
+            const unsigned owners = __reduce_or_sync(0xffffffffu, key >= 0 ? 1u << key : 0u);
+            if (owners == 0u) continue;
+            const unsigned peers = __match_any_sync(0xffffffffu, key);
+            const int rank = __popc(peers & lt);
+            const int ranks = (int)__reduce_max_sync(0xffffffffu, key >= 0 ? (unsigned)__popc(peers) : 0u);
+            for (int r = 0; r < ranks; ++r) {
+                if (key >= 0 && rank == r) {
+                    nq.mbox[warp][0][key] = r ? nq.mbox[warp][0][key] + w.ax : w.ax;
+                    nq.mbox[warp][1][key] = r ? nq.mbox[warp][1][key] + w.ay : w.ay;
+                    nq.mbox[warp][2][key] = r ? nq.mbox[warp][2][key] + w.az : w.az;
+                }
                 __syncwarp();
-                const unsigned peers = __match_any_sync(0xffffffffu, key);
-                if (key >= 0 && lane == __ffs(peers) - 1) {
-                    double bx = 0.0, by = 0.0, bz = 0.0;
-                    for (unsigned m = peers; m; m &= m - 1) {
-                        const int l = __ffs(m) - 1;
-                        bx += nq.stage[warp][0][l];
-                        by += nq.stage[warp][1][l];
-                        bz += nq.stage[warp][2][l];
-                    }
+            }
+            if ((owners >> lane) & 1u) {
+                fold_double(hx[k], lx[k], sg * nq.mbox[warp][0][lane]);
+                fold_double(hy[k], ly[k], sg * nq.mbox[warp][1][lane]);
+                fold_double(hz[k], lz[k], sg * nq.mbox[warp][2][lane]);
+            }
+            __syncwarp();
+        }
+        if (!diag) {  // j side (a diagonal item evaluates both orders of each pair on the i side)
+            const int key = code >= 0 ? (code & 1023) : -1;  // list entry
+            const unsigned peers = __match_any_sync(0xffffffffu, key);
+            const int rank = __popc(peers & lt);
+            const int ranks = (int)__reduce_max_sync(0xffffffffu, key >= 0 ? (unsigned)__popc(peers) : 0u);
+            for (int r = 0; r < ranks; ++r) {
+                if (key >= 0 && rank == r) {
                     if ((key >> 5) == cur_sub) {
-                        jnear[warp][0][key & 31] += bx;
-                        jnear[warp][1][key & 31] += by;
-                        jnear[warp][2][key & 31] += bz;
+                        jnear[warp][0][key & 31] += w.bx;
+                        jnear[warp][1][key & 31] += w.by;
+                        jnear[warp][2][key & 31] += w.bz;
                     } else {
                         double *d = PJ + (size_t)CI[key] * NW * 3;
-                        d[0] += bx;
-                        d[1] += by;
-                        d[2] += bz;
+                        d[0] += w.bx;
+                        d[1] += w.by;
+                        d[2] += w.bz;
                     }
                 }
                 __syncwarp();
             }
         }
-        nq.count[k][tid] = 0;
     }
+    if (lane == 0) nq.count[warp] = 0;
+    __syncwarp();
 }
 
 // Build knobs of the sorted pair kernel: resident CTAs per SM its registers are
@@ -824,20 +842,21 @@ __device__ __forceinline__ void sorted_subtile(const SortedArgs &a, const float4
 #pragma unroll
             for (int k = 0; k < IPT; ++k) any |= ex[k];
             if (__any_sync(0xffffffffu, any)) {  // rare: queue the pairs for the FP64 terms
-                bool full_q = false;
+                const unsigned lt = (1u << lane) - 1u;
+                int qn = nq.count[warp];
 #pragma unroll
                 for (int k = 0; k < IPT; ++k) {
-                    if (ex[k]) {
-                        const int c = nq.count[k][tid];
-                        nq.entry[k][c][tid] = (uint16_t)jj;
-                        nq.count[k][tid] = (uint8_t)(c + 1);
-                        full_q |= c + 1 == NQ;
-                    }
+                    const unsigned b = __ballot_sync(0xffffffffu, ex[k]);
+                    if (ex[k]) nq.entry[warp][qn + __popc(b & lt)] = (uint32_t)(jj | (k << 10) | (lane << 12));
+                    qn += __popc(b);
                 }
-                if (__any_sync(0xffffffffu, full_q)) {
-                    had_exact = true;  // jnear may hold terms of this sub-tile
-                    near_flush<IPT, PER, FORCE>(a, CI, lane, tid, warp, I, J, diag, v, inv_ell, fscale_inv, e0 >> 5,
-                                                nq, jnear, PJ, hx, hy, hz, lx, ly, lz);
+                __syncwarp();
+                if (lane == 0) nq.count[warp] = qn;
+                __syncwarp();
+                if (qn > NQ_CAP - 32 * IPT) {  // the next step could overflow the queue
+                    had_exact = true;          // jnear may hold terms of this sub-tile
+                    near_flush<IPT, PER, FORCE>(a, CI, lane, warp, I, J, diag, v, inv_ell, fscale_inv, e0 >> 5, nq,
+                                                jnear, PJ, hx, hy, hz, lx, ly, lz);
                 }
             }
         }
@@ -868,10 +887,10 @@ __global__ void __launch_bounds__(SYM_T, DEM_SORTED_MIN_CTAS) mixed_sym_sorted_k
     int *CI = reinterpret_cast<int *>(C3 + CAP);  // list entry -> j within block J (-1: padding entry)
     unsigned char *CM = reinterpret_cast<unsigned char *>(CI + CAP);  // list entry -> class (image mask)
     __shared__ double jnear[NW][3][32];           // exact j-side terms of the current sub-tile, per warp
-    __shared__ uint16_t nq_entry[IPT][NQ][SYM_T];  // queued near pairs (list entries), per i row and thread
-    __shared__ uint8_t nq_count[IPT][SYM_T];
-    __shared__ double nq_stage[NW][3][32];
-    const NearQueue nq = {nq_entry, nq_count, nq_stage};
+    __shared__ uint32_t nq_entry[NW][NQ_CAP];     // queued near pairs, per warp
+    __shared__ int nq_count[NW];
+    __shared__ double nq_mbox[NW][3][32];
+    const NearQueue nq = {nq_entry, nq_count, nq_mbox};
     __shared__ int wcnt[IPT][NW][NCLS];           // entries per round, warp and class
     __shared__ int wpre[IPT][NW][NCLS];           // entries of the class before (round, warp)
     __shared__ int ctot[NCLS], cbase[NCLS];       // entries per class; first entry of a class in the masked run
@@ -880,8 +899,7 @@ __global__ void __launch_bounds__(SYM_T, DEM_SORTED_MIN_CTAS) mixed_sym_sorted_k
     if ((int)blockIdx.x >= nitems) return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int c = tid; c < NW * 3 * 32; c += SYM_T) (&jnear[0][0][0])[c] = 0.0;
-#pragma unroll
-    for (int k = 0; k < IPT; ++k) nq_count[k][tid] = 0;
+    if (lane == 0) nq_count[warp] = 0;
     const size_t plane = (size_t)B;
     const unsigned lt = (1u << lane) - 1u;
 
@@ -1094,14 +1112,10 @@ __global__ void __launch_bounds__(SYM_T, DEM_SORTED_MIN_CTAS) mixed_sym_sorted_k
                 }
             }
         }
-        {  // the pairs still queued (their j entries' partial sums are written)
-            bool pending = false;
-#pragma unroll
-            for (int k = 0; k < IPT; ++k) pending |= nq_count[k][tid] != 0;
-            if (__any_sync(0xffffffffu, pending))
-                near_flush<IPT, PER, FORCE>(a, CI, lane, tid, warp, I, J, diag, v, inv_ell, fscale_inv, -1, nq, jnear,
-                                            PJ, hx, hy, hz, lx, ly, lz);
-        }
+        __syncwarp();
+        if (nq_count[warp] != 0)  // the pairs still queued (their j entries' partial sums are written)
+            near_flush<IPT, PER, FORCE>(a, CI, lane, warp, I, J, diag, v, inv_ell, fscale_inv, -1, nq, jnear, PJ, hx,
+                                        hy, hz, lx, ly, lz);
         __syncthreads();  // every warp is done with the lists before the next item rebuilds them
         double *PI = a.s.pi + (size_t)q * 3 * plane;  // interleaved per droplet: [i][3]
         const double sg = FORCE ? -1.0 : 1.0;
