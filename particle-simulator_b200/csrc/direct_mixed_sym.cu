@@ -879,6 +879,8 @@ __global__ void __launch_bounds__(SYM_T, DEM_SORTED_MIN_CTAS) mixed_sym_sorted_k
     constexpr int KP = IPT / 2;
     constexpr int CAP = B + SORTED_PAD;
     constexpr int NW = SYM_T / 32;
+    static_assert(CAP <= 1024 && IPT <= 4 && NQ_CAP >= 2 * 32 * IPT,
+                  "near-pair queue codes: list entry in 10 bits, row in 2; room for one step beyond the threshold");
     extern __shared__ __align__(128) unsigned char sorted_smem[];
     float4 *C0 = reinterpret_cast<float4 *>(sorted_smem);
     float4 *C1 = C0 + CAP;
