@@ -550,7 +550,7 @@ constexpr int NCLS = 9;
 
 template <bool FORCE>
 constexpr int sorted_entry_bytes() {
-    return FORCE ? 16 + 16 + 8 + 4 + 1 : 16 + 16 + 16 + 8 + 4 + 1;
+    return FORCE ? 16 + 16 + 8 + 4 + 4 + 1 : 16 + 16 + 16 + 8 + 4 + 4 + 1;
 }
 template <int IPT, bool FORCE>
 constexpr int sorted_smem_bytes() {
@@ -640,11 +640,10 @@ struct NearQueue {
 //           (added when the sub-tile writes its partial sums); an earlier
 //           entry is added onto its partial sum already written to PJ.
 template <int IPT, bool PER, bool FORCE>
-__device__ __forceinline__ void near_flush(const SortedArgs &a, const int *CI, int lane, int warp, int I, int J,
-                                           bool diag, const BoxView &v, double inv_ell, double fscale_inv,
+__device__ __forceinline__ void near_flush(const SortedArgs &a, const int *CI, const int *CJ, const int *IP, int lane,
+                                           int warp, bool diag, const BoxView &v, double inv_ell, double fscale_inv,
                                            int cur_sub, const NearQueue &nq, double (*jnear)[3][32], double *PJ,
                                            float *hx, float *hy, float *hz, float *lx, float *ly, float *lz) {
-    constexpr int B = SYM_T * IPT;
     constexpr int NW = SYM_T / 32;
     const double sg = FORCE ? -1.0 : 1.0;  // the force i side is held negated
     const unsigned lt = (1u << lane) - 1u;
@@ -656,12 +655,8 @@ __device__ __forceinline__ void near_flush(const SortedArgs &a, const int *CI, i
         NearTerms w = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         if (s < qn) {
             const int c = (int)nq.entry[warp][s];
-            const int jj = c & 1023, k = (c >> 10) & 3, ol = c >> 12;
-            const int il = I * B + k * SYM_T + warp * 32 + ol;
-            const int jo = CI[jj];
-            const int jl = J * B + jo;
-            if (jo >= 0 && jl < v.n && il < v.n && jl != il) {  // padding entries and i == j add nothing
-                const int i = a.perm[v.o0 + il], j = a.perm[v.o0 + jl];
+            const int i = IP[((c >> 10) & 3) * SYM_T + warp * 32 + (c >> 12)], j = CJ[c & 1023];
+            if (i >= 0 && j >= 0 && i != j) {  // padding rows and entries (-1) and i == j add nothing
                 w = FORCE ? near_force_pair_fp64(i, j, a.s.m, PER ? 1 : 0, inv_ell, v.L)
                           : near_oseen_pair_fp64(i, j, a.s.m, PER ? 1 : 0, inv_ell, fscale_inv, v.L);
                 code = c;
@@ -743,7 +738,8 @@ __device__ __forceinline__ float ex2_approx(float x) {
 // pays only for its own axes).
 template <int IPT, bool PER, bool FORCE, int MODE, int MASK>
 __device__ __forceinline__ void sorted_subtile(const SortedArgs &a, const float4 *C0, const float4 *C1,
-                                               const float4 *C2, const float2 *C3, const int *CI, int e0, int lane,
+                                               const float4 *C2, const float2 *C3, const int *CI, const int *CJ,
+                                               const int *IP, int e0, int lane,
                                                int tid, int warp, int I, int J, bool diag, const BoxView &v,
                                                double inv_ell, double fscale_inv, float2 invL2, float2 magic2,
                                                float2 nmagic2, float2 nL2, float hm, const float2 *xi,
@@ -855,7 +851,7 @@ __device__ __forceinline__ void sorted_subtile(const SortedArgs &a, const float4
                 __syncwarp();
                 if (qn > NQ_CAP - 32 * IPT) {  // the next step could overflow the queue
                     had_exact = true;          // jnear may hold terms of this sub-tile
-                    near_flush<IPT, PER, FORCE>(a, CI, lane, warp, I, J, diag, v, inv_ell, fscale_inv, e0 >> 5, nq,
+                    near_flush<IPT, PER, FORCE>(a, CI, CJ, IP, lane, warp, diag, v, inv_ell, fscale_inv, e0 >> 5, nq,
                                                 jnear, PJ, hx, hy, hz, lx, ly, lz);
                 }
             }
@@ -887,11 +883,13 @@ __global__ void __launch_bounds__(SYM_T, DEM_SORTED_MIN_CTAS) mixed_sym_sorted_k
     float4 *C2 = C1 + CAP;  // convection only
     float2 *C3 = reinterpret_cast<float2 *>(C2 + (FORCE ? 0 : CAP));
     int *CI = reinterpret_cast<int *>(C3 + CAP);  // list entry -> j within block J (-1: padding entry)
-    unsigned char *CM = reinterpret_cast<unsigned char *>(CI + CAP);  // list entry -> class (image mask)
+    int *CJ = CI + CAP;  // slow-run entry -> its droplet (-1: padding entry or beyond the box)
+    unsigned char *CM = reinterpret_cast<unsigned char *>(CJ + CAP);  // list entry -> class (image mask)
     __shared__ double jnear[NW][3][32];           // exact j-side terms of the current sub-tile, per warp
     __shared__ uint32_t nq_entry[NW][NQ_CAP];     // queued near pairs, per warp
     __shared__ int nq_count[NW];
     __shared__ double nq_mbox[NW][3][32];
+    __shared__ int IP[B];  // row of block I -> its droplet (-1: beyond the box)
     const NearQueue nq = {nq_entry, nq_count, nq_mbox};
     __shared__ int wcnt[IPT][NW][NCLS];           // entries per round, warp and class
     __shared__ int wpre[IPT][NW][NCLS];           // entries of the class before (round, warp)
@@ -1008,6 +1006,7 @@ __global__ void __launch_bounds__(SYM_T, DEM_SORTED_MIN_CTAS) mixed_sym_sorted_k
             if (!FORCE) C2[e] = Q;
             C3[e] = S3;
             CI[e] = jb;
+            if (e >= C0e) CJ[e] = J * B + jb < v.n ? a.perm[v.o0 + J * B + jb] : -1;  // near pairs: slow run only
             CM[e] = (unsigned char)cls;
         }
         // padding: the fast run's lies far from every droplet, the slow run's at the centre; zero weight
@@ -1021,6 +1020,7 @@ __global__ void __launch_bounds__(SYM_T, DEM_SORTED_MIN_CTAS) mixed_sym_sorted_k
                 if (!FORCE) C2[e] = make_float4(0.f, 0.f, 0.f, 0.f);
                 C3[e] = make_float2(0.f, 0.f);
                 CI[e] = -1;
+                CJ[e] = -1;
                 CM[e] = 0;
             }
         }
@@ -1050,7 +1050,11 @@ __global__ void __launch_bounds__(SYM_T, DEM_SORTED_MIN_CTAS) mixed_sym_sorted_k
             ax[kp] = ay[kp] = az[kp] = make_float2(0.f, 0.f);
         }
 #pragma unroll
-        for (int k = 0; k < IPT; ++k) hx[k] = hy[k] = hz[k] = lx[k] = ly[k] = lz[k] = 0.f;
+        for (int k = 0; k < IPT; ++k) {
+            hx[k] = hy[k] = hz[k] = lx[k] = ly[k] = lz[k] = 0.f;
+            const int il = I * B + k * SYM_T + tid;
+            IP[k * SYM_T + tid] = il < v.n ? a.perm[v.o0 + il] : -1;  // for the near pairs
+        }
         __syncthreads();  // the lists are complete (and wcnt may be rewritten by the next item)
 
         const int nfs = A_pad >> 5, nms = B_used >> 5, nsub = nfs + nms + (C_pad >> 5);
@@ -1061,7 +1065,8 @@ __global__ void __launch_bounds__(SYM_T, DEM_SORTED_MIN_CTAS) mixed_sym_sorted_k
                 float2 sx = make_float2(0.f, 0.f), sy = sx, sz = sx;
                 bool had_exact = false;
 #define DEM_SORTED_SUBTILE(MODE, MASK)                                                                            \
-    sorted_subtile<IPT, PER, FORCE, MODE, MASK>(a, C0, C1, C2, C3, CI, 32 * sub, lane, tid, warp, I, J, diag, v,   \
+    sorted_subtile<IPT, PER, FORCE, MODE, MASK>(a, C0, C1, C2, C3, CI, CJ, IP, 32 * sub, lane, tid, warp, I, J,    \
+                                                diag, v,                                                           \
                                                 inv_ell, fscale_inv, invL2, magic2, nmagic2, nL2, hm, xi, yi, zi, ki, \
                                                 wi, fxi, fyi, fzi, ax, ay, az, hx, hy, hz, lx, ly, lz, jnear, nq, PJ, \
                                                 sx, sy, sz, had_exact)
@@ -1116,8 +1121,8 @@ __global__ void __launch_bounds__(SYM_T, DEM_SORTED_MIN_CTAS) mixed_sym_sorted_k
         }
         __syncwarp();
         if (nq_count[warp] != 0)  // the pairs still queued (their j entries' partial sums are written)
-            near_flush<IPT, PER, FORCE>(a, CI, lane, warp, I, J, diag, v, inv_ell, fscale_inv, -1, nq, jnear, PJ, hx,
-                                        hy, hz, lx, ly, lz);
+            near_flush<IPT, PER, FORCE>(a, CI, CJ, IP, lane, warp, diag, v, inv_ell, fscale_inv, -1, nq, jnear, PJ,
+                                        hx, hy, hz, lx, ly, lz);
         __syncthreads();  // every warp is done with the lists before the next item rebuilds them
         double *PI = a.s.pi + (size_t)q * 3 * plane;  // interleaved per droplet: [i][3]
         const double sg = FORCE ? -1.0 : 1.0;
