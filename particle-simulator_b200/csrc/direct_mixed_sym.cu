@@ -739,8 +739,8 @@ __device__ __forceinline__ float ex2_approx(float x) {
 template <int IPT, bool PER, bool FORCE, int MODE, int MASK>
 __device__ __forceinline__ void sorted_subtile(const SortedArgs &a, const float4 *C0, const float4 *C1,
                                                const float4 *C2, const float2 *C3, const int *CI, const int *CJ,
-                                               const int *IP, int e0, int lane,
-                                               int tid, int warp, int I, int J, bool diag, const BoxView &v,
+                                               const int *IP, int e0, int lane, int warp, bool diag,
+                                               const BoxView &v,
                                                double inv_ell, double fscale_inv, float2 invL2, float2 magic2,
                                                float2 nmagic2, float2 nL2, float hm, const float2 *xi,
                                                const float2 *yi, const float2 *zi, const float2 *ki,
@@ -1065,8 +1065,7 @@ __global__ void __launch_bounds__(SYM_T, DEM_SORTED_MIN_CTAS) mixed_sym_sorted_k
                 float2 sx = make_float2(0.f, 0.f), sy = sx, sz = sx;
                 bool had_exact = false;
 #define DEM_SORTED_SUBTILE(MODE, MASK)                                                                            \
-    sorted_subtile<IPT, PER, FORCE, MODE, MASK>(a, C0, C1, C2, C3, CI, CJ, IP, 32 * sub, lane, tid, warp, I, J,    \
-                                                diag, v,                                                           \
+    sorted_subtile<IPT, PER, FORCE, MODE, MASK>(a, C0, C1, C2, C3, CI, CJ, IP, 32 * sub, lane, warp, diag, v,     \
                                                 inv_ell, fscale_inv, invL2, magic2, nmagic2, nL2, hm, xi, yi, zi, ki, \
                                                 wi, fxi, fyi, fzi, ax, ay, az, hx, hy, hz, lx, ly, lz, jnear, nq, PJ, \
                                                 sx, sy, sz, had_exact)
