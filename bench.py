@@ -291,9 +291,11 @@ def hbm_entry(name, ms, nbytes, peak, src, formula):
             "frac": gbs / peak if gbs else None}
 
 
-def time_steps(st, steps, flush, stream):
+def time_steps(st, steps, flush, stream, sizes=None):
     """CUDA-event time of each of ``steps`` steps, L2 flushed before each one
-    (outside the events); returns (per-step ms, merges inside the window)."""
+    (outside the events); returns (per-step ms, merges inside the window).
+    ``sizes`` (a list) receives each step's droplet count after its merges: the
+    N of that step's pair passes."""
     import torch
 
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
@@ -304,6 +306,8 @@ def time_steps(st, steps, flush, stream):
         ev[k][0].record(stream)
         st.step()
         ev[k][1].record(stream)
+        if sizes is not None:
+            sizes.append(st.n)
     torch.cuda.synchronize()
     return [a.elapsed_time(b) for a, b in ev], st.merges - m0
 
@@ -366,7 +370,8 @@ def run_ours(args, rank, world, device):
     stream = torch.cuda.current_stream()
     torch.cuda.synchronize()
     launches0 = launch_count()
-    step_ms, merges_timed = time_steps(st, args.steps, flush, stream)
+    n_timed = []
+    step_ms, merges_timed = time_steps(st, args.steps, flush, stream, n_timed)
     launches = launch_count() - launches0
     total_ms = float(sum(step_ms))
     kern = {}
@@ -385,7 +390,7 @@ def run_ours(args, rank, world, device):
     job_ms = job_time_ms(total_ms, device)
     if world > 1:
         torch.distributed.barrier()
-    res = dict(n=n, n_final=st.n, L=L, total_ms=job_ms, step_ms=step_ms, kern=kern, clocks=clocks,
+    res = dict(n=n, n_timed=n_timed, n_final=st.n, L=L, total_ms=job_ms, step_ms=step_ms, kern=kern, clocks=clocks,
                merges=st.merges, merges_advance=merges_advance, merges_timed=merges_timed, pos=pos, r=r,
                launches=launches, schedule=schedule)
     if args.precision == "mixed" and not args.no_fp64 and rank == 0:
@@ -1398,7 +1403,10 @@ def main():
     from dem.replicas import whole_job_rate
 
     steps_per_s = whole_job_rate(K, world, res["total_ms"])
-    pairs = n * (n - 1)
+    # ordered pairs per step: the timed steps' own droplet counts (merges during the untimed advance and the
+    # window itself leave fewer than the seeded n)
+    nt = res["n_timed"] or [n]
+    pairs = sum(m * (m - 1) for m in nt) / len(nt)
     clocks = res["clocks"] or {}
     # roofline of the dominant kernel
     prec = args.precision
@@ -1455,7 +1463,8 @@ def main():
             "peak_source": f"{SM_COUNT_B200} SMs x {lanes} lanes x 2 flop x {max_mhz:.0f} MHz (max SM clock); "
                            "MEASURED_PEAKS.json holds no CUDA-core figure",
             "flops_per_pair": FLOPS_FORCE_PAIR if dom == fname else FLOPS_OSEEN_PAIR,
-            "units_per_launch": f"N(N-1) = {pairs} ordered pairs (the reference's pair evaluations)",
+            "units_per_launch": f"N(N-1) averaged over the timed steps = {pairs:.0f} ordered pairs (the reference's "
+                                f"pair evaluations; N = {min(nt)}..{max(nt)} after merges)",
             "schedule": schedule,
         },
         "clocks": clocks,
@@ -1473,8 +1482,9 @@ def main():
     if "hash_detect" in kern:
         peak_b, src_b = hbm_peak()
         table = 1 << max(int(2 * n - 1).bit_length(), 0)
+        n_det = int(round(sum(nt) / len(nt)))  # droplets per detection in the timed window
         line["memory_bound"] = [hbm_entry("hash detection (assign, scans, scatter, bucket records, count, write)",
-                                          kern["hash_detect"][0] / kern["hash_detect"][1], hash_bytes(n, table, 0),
+                                          kern["hash_detect"][0] / kern["hash_detect"][1], hash_bytes(n_det, table, 0),
                                           peak_b, src_b, "48 N + 8 table + 8 pairs")]
     if "fp64" in res:
         f64 = res["fp64"]
